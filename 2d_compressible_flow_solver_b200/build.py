@@ -1,0 +1,80 @@
+"""Builds the stage engine's shared library, libcfs.so, in this folder.
+
+Kernels are compiled by nvcc for sm_100a only (``-gencode
+arch=compute_100a,code=sm_100a``); kernels_exact.cu with ``-fmad=false`` so the
+CFS_FP64_EXACT path keeps the reference's rounding sequence.  Host C++ is
+compiled by g++ with ``-ffp-contract=off`` (the immersed-boundary set-up must
+reproduce the reference's doubles).  Objects go to ``_build/``; a file is
+rebuilt when it or a header it may include is newer than its object.
+
+Usage: ``python build.py [--force]``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+INCLUDE = HERE.parent / "include"
+OUT_DIR = HERE / "_build"
+LIB = HERE / "libcfs.so"
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = {
+    "kernels_exact.cu": ["-fmad=false"],
+    "kernels_fast.cu": [],
+}
+CPP_SOURCES = ["cfs_api.cpp", "ib_setup.cpp"]
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _stale(src: Path, obj: Path, deps: list[Path]) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return src.stat().st_mtime > t or any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
+    """Compiles what is stale and links libcfs.so; returns its path."""
+    OUT_DIR.mkdir(exist_ok=True)
+    deps = _headers()
+    objs = []
+    relink = force or not LIB.exists()
+    for name, extra in CU_SOURCES.items():
+        src, obj = CSRC / name, OUT_DIR / (name + ".o")
+        objs.append(obj)
+        if force or _stale(src, obj, deps):
+            cmd = [NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC",
+                   f"-I{CSRC}", f"-I{INCLUDE}", *extra, "-c", str(src), "-o", str(obj)]
+            if verbose_ptxas:
+                cmd.insert(1, "-Xptxas=-v")
+            _run(cmd)
+            relink = True
+    for name in CPP_SOURCES:
+        src, obj = CSRC / name, OUT_DIR / (name + ".o")
+        objs.append(obj)
+        if force or _stale(src, obj, deps):
+            _run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra",
+                  f"-I{CSRC}", f"-I{INCLUDE}", f"-I{CUDA_HOME / 'include'}", "-c", str(src), "-o", str(obj)])
+            relink = True
+    if relink:
+        _run([NVCC, "-shared", *ARCH, "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(LIB)])
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="--ptxas" in sys.argv)

@@ -1,0 +1,659 @@
+// C ABI of the stage engine (include/cfs.h): context, device memory, stage
+// sequencing, CUDA-graph replay of whole steps, immersed-boundary upload.
+#include "cfs.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cfs_launch.h"
+#include "cfs_layout.h"
+#include "ib_setup.h"
+
+using cfs::kGhost;
+using cfs::kVars;
+
+struct cfs_ctx {
+    cfs_config cfg{};
+    cfs::Prec prec = cfs::kF64;
+    cfs::Layout L{};
+    cfs::BcSides sides{};
+    double dx = 0, dy = 0;
+    cudaStream_t stream = nullptr;
+    void* S[3] = {nullptr, nullptr, nullptr};
+    int cur = 0;          // buffer holding the current state
+    int u0_idx = -1;      // buffer holding the stage-0 input of the running step
+    int u1_idx = -1;      // buffer holding the stage-1 input (TVD3)
+    int next_stage = 0;   // stage the RK sequence expects next
+    double* rhs = nullptr;
+    double* staging = nullptr;
+    uint8_t* types_d = nullptr;
+    bool has_types = false;
+    std::vector<uint8_t> types_h;
+    // immersed ghosts
+    int ib_n = 0, ib_mode = 0;
+    int* ib_cell = nullptr;
+    int* ib_donor = nullptr;
+    int* ib_perm = nullptr;
+    double* ib_img = nullptr;
+    double* ib_fac = nullptr;
+    std::vector<int32_t> ib_cell_h, ib_donor_h;
+    std::vector<double> ib_img_h;
+    // reductions / graph-mode parameters
+    cfs::DevParams* P = nullptr;
+    unsigned long long* wmax = nullptr;
+    double* totals = nullptr;
+    cudaGraphExec_t graph2 = nullptr;  // two full steps (parity 0 then 1)
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(cfs_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CFS_CUDA(ctx, call)                                                                          \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) return fail((ctx), CFS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int stages_per_step(int rk) { return rk == CFS_RK_TVD2 ? 2 : 3; }
+
+// Stage index from the loop counter: TVD2rdRK.cpp:11, TVD3rdRK.cpp:15.
+int stage_of_counter(int rk, int counter) {
+    if (rk == CFS_RK_TVD2) return (counter % 2 == 0) ? 1 : 0;
+    return (counter % 3 == 0) ? 2 : (counter % 3 == 1) ? 0 : 1;
+}
+
+void release_graph(cfs_ctx* c) {
+    if (c->graph2) {
+        cudaGraphExecDestroy(c->graph2);
+        c->graph2 = nullptr;
+    }
+}
+
+int validate(const cfs_config* g, std::string& msg) {
+    if (!g) { msg = "null config"; return CFS_ERR_INVALID; }
+    if (g->nx < 3 || g->ny < 3) { msg = "nx and ny must be at least 3"; return CFS_ERR_INVALID; }
+    if (static_cast<long long>(g->nx) * g->ny > (1LL << 31) - 1) { msg = "nx*ny must fit in 31 bits"; return CFS_ERR_INVALID; }
+    if (!(g->lx > 0) || !(g->ly > 0)) { msg = "lx and ly must be positive"; return CFS_ERR_INVALID; }
+    if (!(g->gamma > 1.0)) { msg = "gamma must exceed 1"; return CFS_ERR_INVALID; }
+    if (!(g->weno_eps > 0)) { msg = "weno_eps must be positive"; return CFS_ERR_INVALID; }
+    if (g->precision < 0 || g->precision > 2) { msg = "unknown precision"; return CFS_ERR_INVALID; }
+    if (g->rk < 0 || g->rk > 2) { msg = "unknown rk variant"; return CFS_ERR_INVALID; }
+    if (g->hll < 0 || g->hll > 1) { msg = "unknown hll variant"; return CFS_ERR_INVALID; }
+    for (int s = 0; s < 4; ++s)
+        if (g->bc[s] < 0 || g->bc[s] > 2) { msg = "unknown boundary kind on side " + std::to_string(s); return CFS_ERR_INVALID; }
+    if ((g->bc[0] == CFS_BC_PERIODIC) != (g->bc[1] == CFS_BC_PERIODIC) ||
+        (g->bc[2] == CFS_BC_PERIODIC) != (g->bc[3] == CFS_BC_PERIODIC)) {
+        msg = "periodic sides come in pairs (left/right, bottom/top)";
+        return CFS_ERR_INVALID;
+    }
+    for (int s = 0; s < 4; ++s)
+        if (g->bc[s] == CFS_BC_DIRICHLET && !(g->bc_prim[s][0] > 0)) {
+            msg = "Dirichlet density must be positive on side " + std::to_string(s);
+            return CFS_ERR_INVALID;
+        }
+    if (g->viscous != CFS_VISCOUS_OFF && g->viscous != CFS_VISCOUS_NS) { msg = "unknown viscous mode"; return CFS_ERR_INVALID; }
+    if (g->viscous == CFS_VISCOUS_NS) { msg = "viscous terms are not available in this build"; return CFS_ERR_INVALID; }
+    return CFS_OK;
+}
+
+cfs::StageArgs base_args(const cfs_ctx* c) {
+    cfs::StageArgs a{};
+    a.L = c->L;
+    for (int s = 0; s < 4; ++s) a.bc[s] = c->sides.bc[s];
+    a.gamma = c->cfg.gamma;
+    a.eps = c->cfg.weno_eps;
+    a.dx = c->dx;
+    a.dy = c->dy;
+    a.rk = c->cfg.rk;
+    a.hll = c->cfg.hll;
+    a.viscous = c->cfg.viscous;
+    a.mu = c->cfg.mu;
+    a.prandtl = c->cfg.prandtl;
+    a.mach = c->cfg.mach;
+    a.types = c->has_types ? c->types_d : nullptr;
+    return a;
+}
+
+cfs::IbArgs ib_args(const cfs_ctx* c, void* U) {
+    cfs::IbArgs a{};
+    a.U = U;
+    a.L = c->L;
+    a.n = c->ib_n;
+    a.mode = c->ib_mode;
+    a.cell = c->ib_cell;
+    a.donor = c->ib_donor;
+    a.image = c->ib_img;
+    a.fac = c->ib_fac;
+    a.perm = c->ib_perm;
+    return a;
+}
+
+// Buffer roles of one stage: reads `in` (+ u0, u1 pointwise), writes `out`.
+struct Roles {
+    int in, out, u0, u1;
+};
+
+Roles roles_for(const cfs_ctx* c, int stage, int cur, int u0_idx, int u1_idx) {
+    Roles r{cur, -1, u0_idx, u1_idx};
+    if (stage == 0) {
+        r.u0 = cur;
+        r.out = (cur + 1) % 3;
+    } else if (stage == 1) {
+        r.u1 = cur;
+        if (c->cfg.rk == CFS_RK_TVD2) r.out = u0_idx;
+        else r.out = 3 - u0_idx - cur;  // the buffer that is neither
+    } else {
+        r.out = u0_idx;
+    }
+    return r;
+}
+
+// Enqueues one stage (immersed-ghost fill + stage kernel).  P/parity/flags
+// select graph mode.
+int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_mode, int parity, bool first,
+                  bool last) {
+    if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[r.in]), c->stream));
+    cfs::StageArgs a = base_args(c);
+    a.in = c->S[r.in];
+    a.u0 = r.u0 >= 0 ? c->S[r.u0] : nullptr;
+    a.u1 = r.u1 >= 0 ? c->S[r.u1] : nullptr;
+    a.out = c->S[r.out];
+    a.rhs = c->cfg.keep_rhs ? c->rhs : nullptr;
+    a.stage = stage;
+    a.dt = dt;
+    if (graph_mode) {
+        a.P = c->P;
+        a.parity = parity;
+        a.first_stage = first ? 1 : 0;
+        a.last_stage = last ? 1 : 0;
+    }
+    CFS_CUDA(c, cfs::launch_stage(c->prec, a, c->stream));
+    return CFS_OK;
+}
+
+int run_stage(cfs_ctx* c, int stage, double dt) {
+    if (stage > 0 && stage != c->next_stage)
+        return fail(c, CFS_ERR_STATE, "stage " + std::to_string(stage) + " requested but the RK sequence expects stage " +
+                                          std::to_string(c->next_stage));
+    const Roles r = roles_for(c, stage, c->cur, c->u0_idx, c->u1_idx);
+    const int rc = enqueue_stage(c, stage, r, dt, false, 0, false, false);
+    if (rc != CFS_OK) return rc;
+    if (stage == 0) c->u0_idx = r.u0;
+    if (stage == 1) c->u1_idx = r.u1;
+    c->cur = r.out;
+    c->next_stage = (stage + 1) % stages_per_step(c->cfg.rk);
+    return CFS_OK;
+}
+
+// Upload of per-ghost data for the device fill.
+int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* donor4, const double* image,
+              const double* normal) {
+    release_graph(c);
+    cudaFree(c->ib_cell);
+    cudaFree(c->ib_donor);
+    cudaFree(c->ib_perm);
+    cudaFree(c->ib_img);
+    cudaFree(c->ib_fac);
+    c->ib_cell = c->ib_donor = c->ib_perm = nullptr;
+    c->ib_img = c->ib_fac = nullptr;
+    c->ib_n = 0;
+    c->ib_cell_h.assign(cell, cell + n);
+    c->ib_donor_h.assign(donor4, donor4 + 4 * static_cast<size_t>(n));
+    c->ib_img_h.assign(image, image + 2 * static_cast<size_t>(n));
+    if (n == 0) return CFS_OK;
+    std::vector<double> fac(16 * static_cast<size_t>(n), 0.0);
+    std::vector<int> perm(4 * static_cast<size_t>(n), 0);
+    for (int g = 0; g < n; ++g) {
+        double M[4][4];
+        for (int k = 0; k < 4; ++k) {
+            const int d = donor4[4 * g + k];
+            const int i = d / c->cfg.ny, j = d % c->cfg.ny;
+            const double x = (i + 0.5) * c->dx, y = (j + 0.5) * c->dy;  // CartesianMesh.cpp:92
+            M[k][0] = x * y;
+            M[k][1] = x;
+            M[k][2] = y;
+            M[k][3] = 1.0;
+        }
+        if (mode == CFS_IB_REFERENCE) {
+            cfs::ldlt4_lower(M, &fac[16 * g], &perm[4 * g]);
+        } else {
+            double w[4];
+            if (!cfs::bilinear_weights(M, image[2 * g], image[2 * g + 1], w))
+                return fail(c, CFS_ERR_INVALID, "singular donor matrix for immersed-ghost " + std::to_string(g));
+            for (int k = 0; k < 4; ++k) fac[16 * g + k] = w[k];
+            fac[16 * g + 4] = normal[2 * g];
+            fac[16 * g + 5] = normal[2 * g + 1];
+        }
+    }
+    CFS_CUDA(c, cudaMalloc(&c->ib_cell, sizeof(int) * n));
+    CFS_CUDA(c, cudaMalloc(&c->ib_donor, sizeof(int) * 4 * n));
+    CFS_CUDA(c, cudaMalloc(&c->ib_perm, sizeof(int) * 4 * n));
+    CFS_CUDA(c, cudaMalloc(&c->ib_img, sizeof(double) * 2 * n));
+    CFS_CUDA(c, cudaMalloc(&c->ib_fac, sizeof(double) * 16 * n));
+    CFS_CUDA(c, cudaMemcpy(c->ib_cell, cell, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CFS_CUDA(c, cudaMemcpy(c->ib_donor, donor4, sizeof(int) * 4 * n, cudaMemcpyHostToDevice));
+    CFS_CUDA(c, cudaMemcpy(c->ib_perm, perm.data(), sizeof(int) * 4 * n, cudaMemcpyHostToDevice));
+    CFS_CUDA(c, cudaMemcpy(c->ib_img, image, sizeof(double) * 2 * n, cudaMemcpyHostToDevice));
+    CFS_CUDA(c, cudaMemcpy(c->ib_fac, fac.data(), sizeof(double) * 16 * n, cudaMemcpyHostToDevice));
+    c->ib_n = n;
+    c->ib_mode = mode;
+    return CFS_OK;
+}
+
+}  // namespace
+
+namespace cfs {
+cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s) {
+    if (p == kF64Exact) return launch_stage_exact(a, s);
+    if (p == kF32Mixed) return launch_stage_f32(a, s);
+    return launch_stage_f64(a, s);
+}
+cudaError_t launch_weno_faces(Prec p, int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s) {
+    if (p == kF64Exact) return launch_weno_faces_exact(n, st, l, r, g, eps, s);
+    if (p == kF32Mixed) return launch_weno_faces_f32(n, st, l, r, g, eps, s);
+    return launch_weno_faces_f64(n, st, l, r, g, eps, s);
+}
+cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const double* R, double* F, double g, int v,
+                             cudaStream_t s) {
+    if (p == kF64Exact) return launch_hll_faces_exact(n, dir, L, R, F, g, v, s);
+    if (p == kF32Mixed) return launch_hll_faces_f32(n, dir, L, R, F, g, v, s);
+    return launch_hll_faces_f64(n, dir, L, R, F, g, v, s);
+}
+}  // namespace cfs
+
+extern "C" {
+
+int cfs_abi_version(void) { return CFS_ABI_VERSION; }
+
+void cfs_config_default(cfs_config* g) {
+    if (!g) return;
+    std::memset(g, 0, sizeof(*g));
+    g->nx = g->ny = 64;
+    g->lx = g->ly = 1.0;
+    g->gamma = 1.4;
+    g->weno_eps = 1e-2;
+    g->precision = CFS_FP64;
+    g->rk = CFS_RK_TVD3_REFERENCE;
+    g->hll = CFS_HLL_REFERENCE;
+    for (int s = 0; s < 4; ++s) g->bc[s] = CFS_BC_NEUMANN;
+    g->viscous = CFS_VISCOUS_OFF;
+    g->mu = 1e-3;
+    g->prandtl = 0.72;
+    g->mach = 1.0;
+}
+
+const char* cfs_last_error(const cfs_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
+    if (!out) return fail(nullptr, CFS_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    std::string msg;
+    const int v = validate(cfg, msg);
+    if (v != CFS_OK) return fail(nullptr, v, msg);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, CFS_ERR_CUDA, "no CUDA device available (the engine has no CPU path)");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, CFS_ERR_INVALID, "device ordinal out of range");
+    cfs_ctx* c = new (std::nothrow) cfs_ctx();
+    if (!c) return fail(nullptr, CFS_ERR_NOMEM, "host allocation failed");
+    c->cfg = *cfg;
+    c->prec = cfg->precision == CFS_FP32_MIXED ? cfs::kF32Mixed : (cfg->precision == CFS_FP64_EXACT ? cfs::kF64Exact : cfs::kF64);
+    c->L = cfs::Layout::make(cfg->nx, cfg->ny, c->prec == cfs::kF32Mixed ? 4 : 8);
+    c->dx = cfg->lx / cfg->nx;  // CartesianMesh::CalCellsize (CartesianMesh.cpp:150-154)
+    c->dy = cfg->ly / cfg->ny;
+    for (int s = 0; s < 4; ++s) {
+        c->sides.bc[s] = cfg->bc[s];
+        // DirichletBoundary ghost: rho, rho u, rho v, E from p (Cylinder.cpp:22-32,
+        // EulerPhase::computeEnergyfromOther, EulerPhase.cpp:124-128).
+        const double rho = cfg->bc_prim[s][0], u = cfg->bc_prim[s][1], vv = cfg->bc_prim[s][2], p = cfg->bc_prim[s][3];
+        const double mx = rho * u, my = rho * vv;
+        const double e = p / (cfg->gamma - 1);
+        c->sides.U[s][0] = rho;
+        c->sides.U[s][1] = mx;
+        c->sides.U[s][2] = my;
+        c->sides.U[s][3] = e + 0.5 * (mx * mx + my * my) / rho;
+    }
+    auto bail = [&](int code) {
+        const std::string m = c->err;
+        cfs_destroy(c);
+        return fail(nullptr, code, m);
+    };
+    if (cudaSetDevice(cfg->device) != cudaSuccess) { c->err = "cudaSetDevice failed"; return bail(CFS_ERR_CUDA); }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { c->err = "stream creation failed"; return bail(CFS_ERR_CUDA); }
+    const size_t sb = static_cast<size_t>(c->L.bytes());
+    for (int b = 0; b < 3; ++b) {
+        if (cudaMalloc(&c->S[b], sb) != cudaSuccess) { c->err = "device allocation of the state failed"; return bail(CFS_ERR_NOMEM); }
+        cudaMemsetAsync(c->S[b], 0, sb, c->stream);
+    }
+    const size_t hb = sizeof(double) * kVars * static_cast<size_t>(cfg->nx) * cfg->ny;
+    if (cudaMalloc(&c->staging, hb) != cudaSuccess) { c->err = "device allocation of the staging buffer failed"; return bail(CFS_ERR_NOMEM); }
+    if (cfg->keep_rhs) {
+        if (cudaMalloc(&c->rhs, hb) != cudaSuccess) { c->err = "device allocation of the RHS buffer failed"; return bail(CFS_ERR_NOMEM); }
+        cudaMemsetAsync(c->rhs, 0, hb, c->stream);
+    }
+    if (cudaMalloc(&c->P, sizeof(cfs::DevParams)) != cudaSuccess || cudaMalloc(&c->wmax, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&c->totals, 4 * sizeof(double)) != cudaSuccess) {
+        c->err = "device allocation of the reduction slots failed";
+        return bail(CFS_ERR_NOMEM);
+    }
+    cudaMemsetAsync(c->P, 0, sizeof(cfs::DevParams), c->stream);
+    for (int b = 0; b < 3; ++b) cfs::launch_ghost_fill(c->L.elem_bytes, c->S[b], c->L, c->sides, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { c->err = std::string("initialisation failed: ") + cudaGetErrorString(cudaGetLastError()); return bail(CFS_ERR_CUDA); }
+    *out = c;
+    return CFS_OK;
+}
+
+int cfs_destroy(cfs_ctx* c) {
+    if (!c) return CFS_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    release_graph(c);
+    for (void* p : c->S) cudaFree(p);
+    cudaFree(c->rhs);
+    cudaFree(c->staging);
+    cudaFree(c->types_d);
+    cudaFree(c->ib_cell);
+    cudaFree(c->ib_donor);
+    cudaFree(c->ib_perm);
+    cudaFree(c->ib_img);
+    cudaFree(c->ib_fac);
+    cudaFree(c->P);
+    cudaFree(c->wmax);
+    cudaFree(c->totals);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CFS_OK;
+}
+
+int cfs_set_state(cfs_ctx* c, const double* U) {
+    if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
+    CFS_CUDA(c, cfs::launch_pack(c->L.elem_bytes, c->staging, c->S[0], c->L, c->stream));
+    CFS_CUDA(c, cfs::launch_ghost_fill(c->L.elem_bytes, c->S[0], c->L, c->sides, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->cur = 0;
+    c->u0_idx = c->u1_idx = -1;
+    c->next_stage = 0;
+    return CFS_OK;
+}
+
+int cfs_get_state(cfs_ctx* c, double* U) {
+    if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    CFS_CUDA(c, cfs::launch_unpack(c->L.elem_bytes, c->S[c->cur], c->staging, c->L, c->stream));
+    CFS_CUDA(c, cudaMemcpyAsync(U, c->staging, hb, cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return CFS_OK;
+}
+
+int cfs_get_rhs(cfs_ctx* c, double* R) {
+    if (!c || !R) return fail(c, CFS_ERR_INVALID, "null argument");
+    if (!c->cfg.keep_rhs) return fail(c, CFS_ERR_STATE, "context created without keep_rhs");
+    const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    CFS_CUDA(c, cudaMemcpyAsync(R, c->rhs, hb, cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return CFS_OK;
+}
+
+int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
+    if (!c || !types) return fail(c, CFS_ERR_INVALID, "null argument");
+    const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    for (size_t k = 0; k < n; ++k)
+        if (types[k] > 2) return fail(c, CFS_ERR_INVALID, "cell type out of range at " + std::to_string(k));
+    release_graph(c);
+    if (!c->types_d) CFS_CUDA(c, cudaMalloc(&c->types_d, n));
+    CFS_CUDA(c, cudaMemcpy(c->types_d, types, n, cudaMemcpyHostToDevice));
+    c->types_h.assign(types, types + n);
+    c->has_types = true;
+    return CFS_OK;
+}
+
+int cfs_set_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* donor4, const double* image_xy,
+               const double* normal_xy) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (mode != CFS_IB_REFERENCE && mode != CFS_IB_BILINEAR_SLIP) return fail(c, CFS_ERR_INVALID, "unknown IB mode");
+    if (n < 0 || (n > 0 && (!cell || !donor4 || !image_xy))) return fail(c, CFS_ERR_INVALID, "bad IB list");
+    if (n > 0 && mode == CFS_IB_BILINEAR_SLIP && !normal_xy) return fail(c, CFS_ERR_INVALID, "slip mode needs wall normals");
+    const long long ncell = static_cast<long long>(c->cfg.nx) * c->cfg.ny;
+    for (int g = 0; g < n; ++g) {
+        if (cell[g] < 0 || cell[g] >= ncell) return fail(c, CFS_ERR_INVALID, "IB cell index out of range");
+        for (int k = 0; k < 4; ++k)
+            if (donor4[4 * g + k] < 0 || donor4[4 * g + k] >= ncell) return fail(c, CFS_ERR_INVALID, "IB donor index out of range");
+    }
+    return upload_ib(c, mode, n, cell, donor4, image_xy, normal_xy);
+}
+
+int cfs_ib_build_circle(cfs_ctx* c, double radius, double cx, double cy, int npoints, int mode) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_circle(c->cfg.nx, c->cfg.ny, c->cfg.lx, c->cfg.ly, radius, cx, cy, npoints, ib, err))
+        return fail(c, CFS_ERR_INVALID, err);
+    const int rc = cfs_set_cell_types(c, ib.types.data());
+    if (rc != CFS_OK) return rc;
+    return cfs_set_ib(c, mode, static_cast<int>(ib.cell.size()), ib.cell.data(), ib.donor.data(), ib.image.data(),
+                      ib.normal.data());
+}
+
+int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
+                     uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy,
+                     double* normal_xy) {
+    if (nx < 1 || ny < 1 || !(lx > 0) || !(ly > 0)) return fail(nullptr, CFS_ERR_INVALID, "bad grid");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_circle(nx, ny, lx, ly, radius, cx, cy, npoints, ib, err)) return fail(nullptr, CFS_ERR_INVALID, err);
+    if (types) std::memcpy(types, ib.types.data(), ib.types.size());
+    const int total = static_cast<int>(ib.cell.size());
+    if (n) *n = total;
+    const int m = total < max_n ? total : max_n;
+    for (int g = 0; g < m; ++g) {
+        if (cell) cell[g] = ib.cell[g];
+        for (int k = 0; k < 4; ++k)
+            if (donor4) donor4[4 * g + k] = ib.donor[4 * g + k];
+        for (int k = 0; k < 2; ++k) {
+            if (image_xy) image_xy[2 * g + k] = ib.image[2 * g + k];
+            if (normal_xy) normal_xy[2 * g + k] = ib.normal[2 * g + k];
+        }
+    }
+    return CFS_OK;
+}
+
+int cfs_get_ib(cfs_ctx* c, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    const size_t nc = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    if (types) {
+        if (c->has_types) std::memcpy(types, c->types_h.data(), nc);
+        else std::memset(types, 0, nc);
+    }
+    const int total = static_cast<int>(c->ib_cell_h.size());
+    if (n) *n = total;
+    const int m = total < max_n ? total : max_n;
+    for (int g = 0; g < m; ++g) {
+        if (cell) cell[g] = c->ib_cell_h[g];
+        for (int k = 0; k < 4; ++k)
+            if (donor4) donor4[4 * g + k] = c->ib_donor_h[4 * g + k];
+        if (image_xy) {
+            image_xy[2 * g] = c->ib_img_h[2 * g];
+            image_xy[2 * g + 1] = c->ib_img_h[2 * g + 1];
+        }
+    }
+    return CFS_OK;
+}
+
+int cfs_ib_fill(cfs_ctx* c) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (c->ib_n == 0) return CFS_OK;
+    CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[c->cur]), c->stream));
+    return CFS_OK;
+}
+
+int cfs_compute_dt(cfs_ctx* c, double cfl, double* dt) {
+    if (!c || !dt) return fail(c, CFS_ERR_INVALID, "null argument");
+    if (!(cfl > 0)) return fail(c, CFS_ERR_INVALID, "cfl must be positive");
+    CFS_CUDA(c, cudaMemsetAsync(c->wmax, 0, sizeof(unsigned long long), c->stream));
+    CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
+                                 c->dx, c->dy, c->wmax, c->stream));
+    unsigned long long bits = 0;
+    CFS_CUDA(c, cudaMemcpyAsync(&bits, c->wmax, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    double m;
+    std::memcpy(&m, &bits, sizeof(m));
+    if (!(m > 0) || !std::isfinite(m)) return fail(c, CFS_ERR_NUMERIC, "CFL reduction found no finite positive wave speed");
+    *dt = cfl / m;
+    return CFS_OK;
+}
+
+int cfs_stage(cfs_ctx* c, int counter, double dt) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (counter < 1) return fail(c, CFS_ERR_INVALID, "loop counter starts at 1 (Run.cpp:153)");
+    return run_stage(c, stage_of_counter(c->cfg.rk, counter), dt);
+}
+
+int cfs_step(cfs_ctx* c, double dt) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (c->next_stage != 0) return fail(c, CFS_ERR_STATE, "a step is in progress (stage sequence not at stage 0)");
+    for (int s = 0; s < stages_per_step(c->cfg.rk); ++s) {
+        const int rc = run_stage(c, s, dt);
+        if (rc != CFS_OK) return rc;
+    }
+    return CFS_OK;
+}
+
+int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed, double* dt_last) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (nsteps < 0) return fail(c, CFS_ERR_INVALID, "nsteps must be non-negative");
+    if (c->next_stage != 0) return fail(c, CFS_ERR_STATE, "a step is in progress (stage sequence not at stage 0)");
+    if (!(cfl > 0) && !(dt > 0)) return fail(c, CFS_ERR_INVALID, "give cfl > 0 or dt > 0");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    if (c->cur != 0) {
+        CFS_CUDA(c, cudaMemcpyAsync(c->S[0], c->S[c->cur], static_cast<size_t>(c->L.bytes()), cudaMemcpyDeviceToDevice, c->stream));
+        c->cur = 0;
+    }
+    cfs::DevParams hp{};
+    hp.use_cfl = cfl > 0 ? 1 : 0;
+    hp.cfl = cfl;
+    hp.dt_fixed = dt;
+    CFS_CUDA(c, cudaMemcpyAsync(c->P, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+    if (hp.use_cfl) {
+        if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[0]), c->stream));
+        CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[0], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
+                                     c->dx, c->dy, reinterpret_cast<unsigned long long*>(c->P), c->stream));
+    }
+    const int S = stages_per_step(c->cfg.rk);
+    auto enqueue_step = [&](int parity) -> int {
+        int cur = 0, u0 = -1, u1 = -1;
+        for (int s = 0; s < S; ++s) {
+            const Roles r = roles_for(c, s, cur, u0, u1);
+            const int rc = enqueue_stage(c, s, r, dt, true, parity, s == 0, s == S - 1);
+            if (rc != CFS_OK) return rc;
+            if (s == 0) u0 = r.u0;
+            if (s == 1) u1 = r.u1;
+            cur = r.out;
+        }
+        return CFS_OK;
+    };
+    if (nsteps >= 2 && !c->graph2) {
+        cudaGraph_t g = nullptr;
+        CFS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(0);
+        if (rc == CFS_OK) rc = enqueue_step(1);
+        const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+        if (rc != CFS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&c->graph2, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            c->graph2 = nullptr;
+            return fail(c, CFS_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(ei));
+        }
+    }
+    for (int k = 0; k + 1 < nsteps; k += 2) CFS_CUDA(c, cudaGraphLaunch(c->graph2, c->stream));
+    if (nsteps % 2 == 1) {
+        const int rc = enqueue_step(0);
+        if (rc != CFS_OK) return rc;
+    }
+    cfs::DevParams out{};
+    CFS_CUDA(c, cudaMemcpyAsync(&out, c->P, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (t_elapsed) *t_elapsed = out.t;
+    if (dt_last) *dt_last = out.dt_last;
+    if (nsteps > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
+        return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
+    return CFS_OK;
+}
+
+int cfs_synchronize(cfs_ctx* c) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return CFS_OK;
+}
+
+void* cfs_get_stream(cfs_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int cfs_conserved_totals(cfs_ctx* c, double totals[4]) {
+    if (!c || !totals) return fail(c, CFS_ERR_INVALID, "null argument");
+    CFS_CUDA(c, cudaMemsetAsync(c->totals, 0, 4 * sizeof(double), c->stream));
+    CFS_CUDA(c, cfs::launch_totals(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->totals, c->stream));
+    CFS_CUDA(c, cudaMemcpyAsync(totals, c->totals, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < 4; ++v) totals[v] *= c->dx * c->dy;
+    return CFS_OK;
+}
+
+int cfs_weno5_faces(cfs_ctx* c, int n, const double* st, double* left, double* right) {
+    if (!c || n < 0 || (n > 0 && (!st || !left || !right))) return fail(c, CFS_ERR_INVALID, "bad argument");
+    if (n == 0) return CFS_OK;
+    double *d_st = nullptr, *d_l = nullptr, *d_r = nullptr;
+    CFS_CUDA(c, cudaMalloc(&d_st, sizeof(double) * 24 * n));
+    CFS_CUDA(c, cudaMalloc(&d_l, sizeof(double) * 5 * n));
+    CFS_CUDA(c, cudaMalloc(&d_r, sizeof(double) * 5 * n));
+    cudaMemcpyAsync(d_st, st, sizeof(double) * 24 * n, cudaMemcpyHostToDevice, c->stream);
+    cudaError_t e = cfs::launch_weno_faces(c->prec, n, d_st, d_l, d_r, c->cfg.gamma, c->cfg.weno_eps, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(left, d_l, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(right, d_r, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_st);
+    cudaFree(d_l);
+    cudaFree(d_r);
+    if (e != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("weno5 faces: ") + cudaGetErrorString(e));
+    return CFS_OK;
+}
+
+int cfs_hll_faces(cfs_ctx* c, int n, int dir, const double* L, const double* R, double* F) {
+    if (!c || n < 0 || (dir != 0 && dir != 1) || (n > 0 && (!L || !R || !F))) return fail(c, CFS_ERR_INVALID, "bad argument");
+    if (n == 0) return CFS_OK;
+    double *d_l = nullptr, *d_r = nullptr, *d_f = nullptr;
+    CFS_CUDA(c, cudaMalloc(&d_l, sizeof(double) * 4 * n));
+    CFS_CUDA(c, cudaMalloc(&d_r, sizeof(double) * 4 * n));
+    CFS_CUDA(c, cudaMalloc(&d_f, sizeof(double) * 4 * n));
+    cudaMemcpyAsync(d_l, L, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d_r, R, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
+    cudaError_t e = cfs::launch_hll_faces(c->prec, n, dir, d_l, d_r, d_f, c->cfg.gamma, c->cfg.hll, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F, d_f, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_l);
+    cudaFree(d_r);
+    cudaFree(d_f);
+    if (e != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("hll faces: ") + cudaGetErrorString(e));
+    return CFS_OK;
+}
+
+}  // extern "C"

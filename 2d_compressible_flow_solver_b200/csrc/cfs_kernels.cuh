@@ -1,0 +1,657 @@
+// Stage, immersed-boundary, reduction and layout kernels, templated over an
+// arithmetic policy.  Included by kernels_exact.cu (built with -fmad=false, so
+// PolExact keeps the reference's rounding sequence) and kernels_fast.cu (FMA
+// contraction on: PolF64, PolF32).
+#pragma once
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <cstdint>
+
+#include "cfs_layout.h"
+
+namespace cfs {
+
+// ---------------------------------------------------------------- policies
+// T = storage type of the state, C = type of the WENO/HLL arithmetic.
+struct PolExact { using T = double; using C = double; static constexpr bool kExact = true;  static constexpr bool kMixed = false; };
+struct PolF64   { using T = double; using C = double; static constexpr bool kExact = false; static constexpr bool kMixed = false; };
+struct PolF32   { using T = float;  using C = float;  static constexpr bool kExact = false; static constexpr bool kMixed = true;  };
+
+enum { kRkTvd2 = 0, kRkTvd3Ref = 1, kRkSsp3 = 2 };
+enum { kHllReference = 0, kHllDavis = 1 };
+
+template <class C> struct Face5 { C r, mx, my, E, p, a; };
+
+__device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
+__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrtf(x); }
+__device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
+
+// std::min / std::max as the reference uses them (RiemmanSolverHLL.cpp:41-42):
+// the first argument is returned unless the second compares smaller (larger),
+// so a NaN second argument is dropped.
+template <class C> __device__ __forceinline__ C min_ref(C a, C b) { return (b < a) ? b : a; }
+template <class C> __device__ __forceinline__ C max_ref(C a, C b) { return (a < b) ? b : a; }
+
+// ------------------------------------------------------------------- WENO5
+// Weno5th::weno5Interpolation (Weno5th.cpp:4-28) in its own operation order.
+__device__ __forceinline__ double weno5_ref(double v0, double v1, double v2, double v3, double v4, double eps) {
+    double beta0 = (13.0 / 12.0) * ((v0 - 2 * v1 + v2) * (v0 - 2 * v1 + v2))
+                 + 0.25 * ((v0 - 4 * v1 + 3 * v2) * (v0 - 4 * v1 + 3 * v2));
+    double beta1 = (13.0 / 12.0) * ((v1 - 2 * v2 + v3) * (v1 - 2 * v2 + v3))
+                 + 0.25 * ((v1 - v3) * (v1 - v3));
+    double beta2 = (13.0 / 12.0) * ((v2 - 2 * v3 + v4) * (v2 - 2 * v3 + v4))
+                 + 0.25 * ((3 * v2 - 4 * v3 + v4) * (3 * v2 - 4 * v3 + v4));
+    double alpha0 = 0.1 / ((eps + beta0) * (eps + beta0));
+    double alpha1 = 0.6 / ((eps + beta1) * (eps + beta1));
+    double alpha2 = 0.3 / ((eps + beta2) * (eps + beta2));
+    double sum_alpha = alpha0 + alpha1 + alpha2;
+    double omega0 = alpha0 / sum_alpha;
+    double omega1 = alpha1 / sum_alpha;
+    double omega2 = alpha2 / sum_alpha;
+    return omega0 * (v0 / 3.0 - 7.0 * v1 / 6.0 + 11.0 * v2 / 6.0)
+         + omega1 * (-v1 / 6.0 + 5.0 * v2 / 6.0 + v3 / 3.0)
+         + omega2 * (v2 / 3.0 + 5.0 * v3 / 6.0 - v4 / 6.0);
+}
+
+// The same reconstruction with one division: alpha_k = d_k / q_k with
+// q_k = (eps + beta_k)^2 is scaled by q0 q1 q2, so
+// result = (sum d_k q_l q_m P_k) / (6 sum d_k q_l q_m), P_k = 6 x candidate k.
+// In FP32 beta is capped at 1e9 so that the q products stay finite.
+template <class C>
+__device__ __forceinline__ C weno5_fast(C v0, C v1, C v2, C v3, C v4, C eps) {
+    const C k13 = C(13.0 / 12.0), k14 = C(0.25);
+    const C d0 = v0 - C(2) * v1 + v2, e0 = v0 - C(4) * v1 + C(3) * v2;
+    const C d1 = v1 - C(2) * v2 + v3, e1 = v1 - v3;
+    const C d2 = v2 - C(2) * v3 + v4, e2 = C(3) * v2 - C(4) * v3 + v4;
+    C b0 = k13 * d0 * d0 + k14 * e0 * e0;
+    C b1 = k13 * d1 * d1 + k14 * e1 * e1;
+    C b2 = k13 * d2 * d2 + k14 * e2 * e2;
+    if (sizeof(C) == 4) {
+        b0 = fmin(b0, C(1e9));
+        b1 = fmin(b1, C(1e9));
+        b2 = fmin(b2, C(1e9));
+    }
+    C q0 = eps + b0, q1 = eps + b1, q2 = eps + b2;
+    q0 *= q0;
+    q1 *= q1;
+    q2 *= q2;
+    const C a0 = C(0.1) * q1 * q2, a1 = C(0.6) * q0 * q2, a2 = C(0.3) * q0 * q1;
+    const C p0 = C(2) * v0 - C(7) * v1 + C(11) * v2;
+    const C p1 = -v1 + C(5) * v2 + C(2) * v3;
+    const C p2 = C(2) * v2 + C(5) * v3 - v4;
+    return (a0 * p0 + a1 * p1 + a2 * p2) * rcp_fast(C(6) * (a0 + a1 + a2));
+}
+
+template <class Pol>
+__device__ __forceinline__ typename Pol::C weno5(typename Pol::C v0, typename Pol::C v1, typename Pol::C v2,
+                                                 typename Pol::C v3, typename Pol::C v4, typename Pol::C eps) {
+    if constexpr (Pol::kExact) return weno5_ref(v0, v1, v2, v3, v4, eps);
+    else return weno5_fast(v0, v1, v2, v3, v4, eps);
+}
+
+// ------------------------------------------------- pressure / sound speed
+// EulerPhase::computePressurefromOther (EulerPhase.cpp:130-133) and
+// a = sqrt(gamma p / rho) (RiemmanSolverHLL.cpp:18,24).  FP32-mixed: p and a are
+// recovered in FP64 where the kinetic energy exceeds 90% of E.
+template <class Pol>
+__device__ __forceinline__ void finish_state(Face5<typename Pol::C>& s, double g) {
+    using C = typename Pol::C;
+    if constexpr (Pol::kExact) {
+        s.p = (g - 1) * (s.E - 0.5 * (s.mx * s.mx + s.my * s.my) / s.r);
+        s.a = sqrt(g * s.p / s.r);
+    } else if constexpr (Pol::kMixed) {
+        const C rinv = rcp_fast(s.r);
+        const C ke = C(0.5) * (s.mx * s.mx + s.my * s.my) * rinv;
+        if (ke > C(0.9) * s.E) {
+            const double r = s.r, mx = s.mx, my = s.my, E = s.E;
+            const double p = (g - 1) * (E - 0.5 * (mx * mx + my * my) / r);
+            s.p = C(p);
+            s.a = C(sqrt(g * p / r));
+        } else {
+            s.p = C(g - 1) * (s.E - ke);
+            s.a = sqrt_fast(C(g) * s.p * rinv);
+        }
+    } else {
+        const C rinv = rcp_fast(s.r);
+        s.p = C(g - 1) * (s.E - C(0.5) * (s.mx * s.mx + s.my * s.my) * rinv);
+        s.a = sqrt(C(g) * s.p * rinv);
+    }
+}
+
+// EulerMod::comFlux (EulerMod.cpp:33-54); dir 0 = X, 1 = Y.
+template <class Pol>
+__device__ __forceinline__ void phys_flux(const Face5<typename Pol::C>& s, int dir, typename Pol::C F[4]) {
+    using C = typename Pol::C;
+    if constexpr (Pol::kExact) {
+        const double rho = s.r, u = s.mx, v = s.my, E = s.E, p = s.p;
+        if (dir == 0) {
+            F[0] = u;
+            F[1] = u * u / rho + p;
+            F[2] = u * v / rho;
+            F[3] = (E + p) * (u / rho);
+        } else {
+            F[0] = v;
+            F[1] = u * v / rho;
+            F[2] = v * v / rho + p;
+            F[3] = (E + p) * (v / rho);
+        }
+    } else {
+        const C q = dir == 0 ? s.mx : s.my;
+        const C un = q * rcp_fast(s.r);
+        F[0] = q;
+        F[1] = s.mx * un + (dir == 0 ? s.p : C(0));
+        F[2] = s.my * un + (dir == 0 ? C(0) : s.p);
+        F[3] = (s.E + s.p) * un;
+    }
+}
+
+// RiemmanSolverHLL::Solver (RiemmanSolverHLL.cpp:5-75): PVRS star state, wave
+// bounds SL = min(m_nL - aL, u* - a*L), SR = max(m_nL + aL, u* + a*R) (left
+// momentum in both, as written), HLL average.  kHllDavis: bounds from the
+// velocities of both sides (no reference counterpart).
+template <class Pol>
+__device__ __forceinline__ void hll_flux(const Face5<typename Pol::C>& L, const Face5<typename Pol::C>& R, int dir,
+                                         int variant, double g, typename Pol::C F[4]) {
+    using C = typename Pol::C;
+    C FL[4], FR[4];
+    phys_flux<Pol>(L, dir, FL);
+    phys_flux<Pol>(R, dir, FR);
+    const C qL = dir == 0 ? L.mx : L.my, qR = dir == 0 ? R.mx : R.my;
+    const C aL = L.a, aR = R.a;
+    C SL, SR;
+    if constexpr (Pol::kExact) {
+        const double rhoL = L.r, rhoR = R.r, pL = L.p, pR = R.p;
+        if (variant == kHllReference) {
+            double a_ave = 0.5 * (aL + aR);
+            double rho_ave = 0.5 * (rhoL + rhoR);
+            double p_star = 0.5 * (pL + pR) - 0.5 * (qR / rhoR - qL / rhoL) * rho_ave * a_ave;
+            double u_star = 0.5 * (qR / rhoR + qL / rhoL) - 0.5 * (pR - pL) / (rho_ave * a_ave);
+            double rho_star_L = rhoL + (qL / rhoL - u_star) * rho_ave / a_ave;
+            double rho_star_R = rhoR - (qR / rhoR - u_star) * rho_ave / a_ave;
+            double a_star_L = sqrt(g * p_star / rho_star_L);
+            double a_star_R = sqrt(g * p_star / rho_star_R);
+            SL = min_ref(qL - aL, u_star - a_star_L);
+            SR = max_ref(qL + aL, u_star + a_star_R);
+        } else {
+            const double uL = qL / rhoL, uR = qR / rhoR;
+            SL = min_ref(uL - aL, uR - aR);
+            SR = max_ref(uL + aL, uR + aR);
+        }
+    } else {
+        const C rinvL = rcp_fast(L.r), rinvR = rcp_fast(R.r);
+        const C uL = qL * rinvL, uR = qR * rinvR;
+        if (variant == kHllReference) {
+            const C a_ave = C(0.5) * (aL + aR);
+            const C rho_ave = C(0.5) * (L.r + R.r);
+            const C ra = rho_ave * a_ave;
+            const C p_star = C(0.5) * (L.p + R.p) - C(0.5) * (uR - uL) * ra;
+            const C u_star = C(0.5) * (uR + uL) - C(0.5) * (R.p - L.p) * rcp_fast(ra);
+            const C ratio = rho_ave * rcp_fast(a_ave);
+            const C rho_star_L = L.r + (uL - u_star) * ratio;
+            const C rho_star_R = R.r - (uR - u_star) * ratio;
+            const C gp = C(g) * p_star;
+            const C a_star_L = sqrt_fast(gp * rcp_fast(rho_star_L));
+            const C a_star_R = sqrt_fast(gp * rcp_fast(rho_star_R));
+            SL = min_ref(qL - aL, u_star - a_star_L);
+            SR = max_ref(qL + aL, u_star + a_star_R);
+        } else {
+            SL = min_ref(uL - aL, uR - aR);
+            SR = max_ref(uL + aL, uR + aR);
+        }
+    }
+    if (SL >= 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) F[q] = FL[q];
+    } else if (SR <= 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) F[q] = FR[q];
+    } else {
+        const C inv_SR_SL = Pol::kExact ? C(1.0) / (SR - SL) : rcp_fast(SR - SL);
+        const C dU[4] = {R.r - L.r, R.mx - L.mx, R.my - L.my, R.E - L.E};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) F[q] = (SR * FL[q] - SL * FR[q] + SL * SR * dU[q]) * inv_SR_SL;
+    }
+}
+
+// Left state from s[0..4], right state from the reversed s[5..1]
+// (Weno5th::comLeftPhase / comRightPhase, Weno5th.cpp:57-81), then HLL.
+template <class Pol>
+__device__ __forceinline__ void face_flux(const typename Pol::C s[6][kVars], int dir, double g, typename Pol::C eps,
+                                          int variant, typename Pol::C F[4]) {
+    using C = typename Pol::C;
+    Face5<C> L, R;
+    L.r = weno5<Pol>(s[0][0], s[1][0], s[2][0], s[3][0], s[4][0], eps);
+    L.mx = weno5<Pol>(s[0][1], s[1][1], s[2][1], s[3][1], s[4][1], eps);
+    L.my = weno5<Pol>(s[0][2], s[1][2], s[2][2], s[3][2], s[4][2], eps);
+    L.E = weno5<Pol>(s[0][3], s[1][3], s[2][3], s[3][3], s[4][3], eps);
+    R.r = weno5<Pol>(s[5][0], s[4][0], s[3][0], s[2][0], s[1][0], eps);
+    R.mx = weno5<Pol>(s[5][1], s[4][1], s[3][1], s[2][1], s[1][1], eps);
+    R.my = weno5<Pol>(s[5][2], s[4][2], s[3][2], s[2][2], s[1][2], eps);
+    R.E = weno5<Pol>(s[5][3], s[4][3], s[3][3], s[2][3], s[1][3], eps);
+    finish_state<Pol>(L, g);
+    finish_state<Pol>(R, g);
+    hll_flux<Pol>(L, R, dir, variant, g, F);
+}
+
+// ----------------------------------------------------------- RK update
+// TVD2rdRK::advance (TVD2rdRK.cpp:3-31), TVD3rdRK::advance (TVD3rdRK.cpp:3-48),
+// coefficient tables TVD2rdRK.h:16-19 / TVD3rdRK.h:14-18, each product taken in
+// the reference's order (coef * dt) * R.  Evaluated in FP64 for every policy.
+__device__ __forceinline__ double rk_update(int rk, int stage, double dt, double cur, double u0v, double u1v, double r) {
+    if (stage == 0) return 1.0 * cur + 1.0 * dt * r;
+    if (rk == kRkTvd2) return 0.5 * u0v + 0.5 * cur + 0.5 * dt * r;
+    if (stage == 1) return 0.75 * u0v + 0.25 * cur + 0.25 * dt * r;
+    if (rk == kRkTvd3Ref) return (1.0 / 3.0) * u0v + (2.0 / 3.0) * u1v + (2.0 / 3.0) * dt * r;
+    return (1.0 / 3.0) * u0v + (2.0 / 3.0) * cur + (2.0 / 3.0) * dt * r;
+}
+
+// (|u| + a)/dx + (|v| + a)/dy of one cell, FP64, in the order of the CFL
+// reduction every caller shares.
+__device__ __forceinline__ double wave_sum(double rho, double mx, double my, double E, double g, double dx, double dy) {
+    const double p = (g - 1) * (E - 0.5 * (mx * mx + my * my) / rho);
+    const double a = sqrt(g * p / rho);
+    const double u = mx / rho, v = my / rho;
+    return (fabs(u) + a) / dx + (fabs(v) + a) / dy;
+}
+
+// Writes one cell of the new state and the ghost copies it feeds: Neumann
+// ghosts copy the adjacent cell into all three layers (NeummanBoundary.cpp:31-45;
+// one ghost repeated three times in the stencil, CellInterface.cpp:147-179),
+// periodic ghosts wrap.  Dirichlet ghosts are constant and set at upload.
+template <class T>
+__device__ __forceinline__ void store_cell(T* out, const Layout& L, const int bc[4], int v, int i, int j, T val) {
+    T* p = out + v * L.plane;
+    p[L.offset(i, j)] = val;
+    if (i == 0 && bc[0] == kNeumann) { p[L.offset(-1, j)] = val; p[L.offset(-2, j)] = val; p[L.offset(-3, j)] = val; }
+    if (i == L.nx - 1 && bc[1] == kNeumann) { p[L.offset(L.nx, j)] = val; p[L.offset(L.nx + 1, j)] = val; p[L.offset(L.nx + 2, j)] = val; }
+    if (bc[0] == kPeriodic && i >= L.nx - kGhost) p[L.offset(i - L.nx, j)] = val;
+    if (bc[1] == kPeriodic && i < kGhost) p[L.offset(i + L.nx, j)] = val;
+    if (j == 0 && bc[2] == kNeumann) { p[L.offset(i, -1)] = val; p[L.offset(i, -2)] = val; p[L.offset(i, -3)] = val; }
+    if (j == L.ny - 1 && bc[3] == kNeumann) { p[L.offset(i, L.ny)] = val; p[L.offset(i, L.ny + 1)] = val; p[L.offset(i, L.ny + 2)] = val; }
+    if (bc[2] == kPeriodic && j >= L.ny - kGhost) p[L.offset(i, j - L.ny)] = val;
+    if (bc[3] == kPeriodic && j < kGhost) p[L.offset(i, j + L.ny)] = val;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_max(double m, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        m = (l < NT / 32) ? red[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    return m;
+}
+
+__device__ __forceinline__ double stage_dt(const StageArgs& a) {
+    if (!a.P) return a.dt;
+    if (a.P->use_cfl) return a.P->cfl / __longlong_as_double(static_cast<long long>(a.P->wmax[a.parity]));
+    return a.P->dt_fixed;
+}
+
+// ------------------------------------------------------------ stage kernel
+// One RK stage on a TI x TJ tile: the tile and its 3-cell halo are staged in
+// shared memory; every x- and y-face of the tile gets its WENO5 states and HLL
+// flux (kept in shared memory, never in DRAM); each cell then forms its RHS
+// (Cell::comRHS, Cell.cpp:110-126) and, if fluid, its RK update.
+template <class Pol, int TI, int TJ>
+__global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
+    using T = typename Pol::T;
+    using C = typename Pol::C;
+    constexpr int NT = TI * TJ;
+    constexpr int HI = TI + 2 * kGhost, HJ = TJ + 2 * kGhost;
+    __shared__ C sU[kVars][HI][HJ];
+    __shared__ C sFX[kVars][TI + 1][TJ];
+    __shared__ C sFY[kVars][TI][TJ + 1];
+    __shared__ double red[NT / 32];
+
+    const Layout& L = a.L;
+    const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+    const T* in = static_cast<const T*>(a.in);
+    const int t = threadIdx.x;
+
+    for (int e = t; e < HI * HJ; e += NT) {
+        const int r = e / HJ, c = e - r * HJ;
+        const int i = i0 - kGhost + r, j = j0 - kGhost + c;
+        const bool corner = (r < kGhost || r >= TI + kGhost) && (c < kGhost || c >= TJ + kGhost);
+        const bool ok = !corner && i < L.nx + kGhost && j < L.ny + kGhost;
+        if (ok) {
+            const long long off = L.offset(i, j);
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) sU[v][r][c] = C(in[v * L.plane + off]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) sU[v][r][c] = C(0);
+        }
+    }
+    __syncthreads();
+
+    const C eps = C(a.eps);
+    const bool lo_x = a.bc[0] == kNeumann || a.bc[0] == kDirichlet;
+    const bool hi_x = a.bc[1] == kNeumann || a.bc[1] == kDirichlet;
+    const bool lo_y = a.bc[2] == kNeumann || a.bc[2] == kDirichlet;
+    const bool hi_y = a.bc[3] == kNeumann || a.bc[3] == kDirichlet;
+
+    // x-normal faces: face fi (0..TI) of tile column fj lies between cells
+    // i0+fi-1 and i0+fi.  On a physical boundary face the interior slots repeat
+    // the first interior cell (CellInterface.cpp:172-178 stop both walkers).
+    for (int f = t; f < (TI + 1) * TJ; f += NT) {
+        const int fi = f / TJ, fj = f - fi * TJ;
+        const int fa = i0 + fi, j = j0 + fj;
+        if (fa > L.nx || j >= L.ny) continue;
+        C s[6][kVars];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            int r = fi + k;
+            if (fa == 0 && lo_x && k >= 3) r = fi + 3;
+            if (fa == L.nx && hi_x && k <= 2) r = fi + 2;
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) s[k][v] = sU[v][r][fj + kGhost];
+        }
+        C F[4];
+        face_flux<Pol>(s, 0, a.gamma, eps, a.hll, F);
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) sFX[v][fi][fj] = F[v];
+    }
+    // y-normal faces: face fj (0..TJ) of tile row fi between cells j0+fj-1, j0+fj.
+    for (int f = t; f < TI * (TJ + 1); f += NT) {
+        const int fi = f / (TJ + 1), fj = f - fi * (TJ + 1);
+        const int i = i0 + fi, fb = j0 + fj;
+        if (i >= L.nx || fb > L.ny) continue;
+        C s[6][kVars];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            int c = fj + k;
+            if (fb == 0 && lo_y && k >= 3) c = fj + 3;
+            if (fb == L.ny && hi_y && k <= 2) c = fj + 2;
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) s[k][v] = sU[v][fi + kGhost][c];
+        }
+        C F[4];
+        face_flux<Pol>(s, 1, a.gamma, eps, a.hll, F);
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) sFY[v][fi][fj] = F[v];
+    }
+    __syncthreads();
+
+    const double dt = stage_dt(a);
+    if (a.P && a.first_stage && blockIdx.x == 0 && blockIdx.y == 0 && t == 0) {
+        a.P->wmax[1 - a.parity] = 0ull;
+        a.P->t += dt;
+        a.P->dt_last = dt;
+    }
+
+    const int ti = t / TJ, tj = t - (t / TJ) * TJ;
+    const int i = i0 + ti, j = j0 + tj;
+    double wloc = 0.0;
+    if (i < L.nx && j < L.ny) {
+        const bool fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+        const long long off = L.offset(i, j);
+        const T* u0 = static_cast<const T*>(a.u0);
+        const T* u1 = static_cast<const T*>(a.u1);
+        T* out = static_cast<T*>(a.out);
+        double nv[kVars];
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) {
+            double rv;
+            if constexpr (Pol::kExact) {
+                rv = -(sFX[v][ti + 1][tj] - sFX[v][ti][tj]) / a.dx - (sFY[v][ti][tj + 1] - sFY[v][ti][tj]) / a.dy;
+            } else {
+                rv = -double(sFX[v][ti + 1][tj] - sFX[v][ti][tj]) / a.dx - double(sFY[v][ti][tj + 1] - sFY[v][ti][tj]) / a.dy;
+            }
+            const double cur = double(sU[v][ti + kGhost][tj + kGhost]);
+            double val = cur;
+            if (fluid) {
+                const double u0v = a.stage >= 1 ? double(u0[v * L.plane + off]) : 0.0;
+                const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? double(u1[v * L.plane + off]) : 0.0;
+                val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
+            }
+            const T stored = T(val);
+            nv[v] = double(stored);
+            store_cell<T>(out, L, a.bc, v, i, j, stored);
+            if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
+        }
+        if (a.P && a.last_stage && a.P->use_cfl && fluid) {
+            const double w = wave_sum(nv[0], nv[1], nv[2], nv[3], a.gamma, a.dx, a.dy);
+            if (w > wloc) wloc = w;
+        }
+    }
+    if (a.P && a.last_stage && a.P->use_cfl) {
+        const double m = block_max<NT>(wloc, red);
+        if (t == 0 && m > 0.0) atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// -------------------------------------------------- immersed-ghost fill
+// Cell::comImmersedGhostPhase -> ImagePoint::InterpolatePhase
+// (Cell.cpp:172-181, ImagePoint.cpp:20-82).  Mode 0 replays the solve of the
+// donor matrix's pivoted LDL^T (factor computed once on the host from the
+// lower triangle, as Eigen's ldlt() reads it): permute, unit-lower forward
+// substitution, pseudo-inverse of D, back substitution, un-permute; then
+// W0 X Y + W1 X + W2 Y + W3 and both momenta negated.  Mode 1: bilinear
+// weights and reflection of the wall-normal momentum only.  FP64 arithmetic.
+template <class T>
+__global__ void ib_fill_kernel(const IbArgs a) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.n) return;
+    const Layout& L = a.L;
+    T* U = static_cast<T*>(a.U);
+    double f[kVars][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int d = a.donor[4 * g + k];
+        const int i = d / L.ny, j = d - (d / L.ny) * L.ny;
+        const long long off = L.offset(i, j);
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) f[v][k] = double(U[v * L.plane + off]);
+    }
+    const double* fac = a.fac + 16 * g;
+    double val[kVars];
+    if (a.mode == 0) {
+        const double X = a.image[2 * g], Y = a.image[2 * g + 1];
+        const double l10 = fac[0], l20 = fac[1], l21 = fac[2], l30 = fac[3], l31 = fac[4], l32 = fac[5];
+        const double dd[4] = {fac[6], fac[7], fac[8], fac[9]};
+        const int* pm = a.perm + 4 * g;
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) {
+            double y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) y[k] = f[v][pm[k]];
+            y[1] -= l10 * y[0];
+            y[2] -= l20 * y[0];
+            y[2] -= l21 * y[1];
+            y[3] -= l30 * y[0];
+            y[3] -= l31 * y[1];
+            y[3] -= l32 * y[2];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) y[k] = (fabs(dd[k]) > DBL_MIN) ? y[k] / dd[k] : 0.0;
+            y[2] -= l32 * y[3];
+            y[1] -= l21 * y[2];
+            y[1] -= l31 * y[3];
+            y[0] -= l10 * y[1];
+            y[0] -= l20 * y[2];
+            y[0] -= l30 * y[3];
+            double W[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) W[pm[k]] = y[k];
+            val[v] = W[0] * X * Y + W[1] * X + W[2] * Y + W[3];
+        }
+        val[1] = -val[1];
+        val[2] = -val[2];
+    } else {
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) val[v] = fac[0] * f[v][0] + fac[1] * f[v][1] + fac[2] * f[v][2] + fac[3] * f[v][3];
+        const double nx_ = fac[4], ny_ = fac[5];
+        const double mn = val[1] * nx_ + val[2] * ny_;
+        val[1] = val[1] - 2.0 * mn * nx_;
+        val[2] = val[2] - 2.0 * mn * ny_;
+    }
+    const int c = a.cell[g];
+    const long long off = L.offset(c / L.ny, c - (c / L.ny) * L.ny);
+#pragma unroll
+    for (int v = 0; v < kVars; ++v) U[v * L.plane + off] = T(val[v]);
+}
+
+// ------------------------------------------------------ CFL reduction
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) wmax_kernel(const T* U, const Layout L, const uint8_t* types, double g,
+                                                  double dx, double dy, unsigned long long* out) {
+    __shared__ double red[NT / 32];
+    double m = 0.0;
+    const long long n = static_cast<long long>(L.nx) * L.ny;
+    for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
+        if (types && types[k] != 0) continue;
+        const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
+        const long long off = L.offset(i, j);
+        const double w = wave_sum(double(U[off]), double(U[L.plane + off]), double(U[2 * L.plane + off]),
+                                  double(U[3 * L.plane + off]), g, dx, dy);
+        if (w > m) m = w;
+    }
+    m = block_max<NT>(m, red);
+    if (threadIdx.x == 0 && m > 0.0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+
+// Sums of rho, m_x, m_y, E over fluid cells (FP64 accumulation).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) totals_kernel(const T* U, const Layout L, const uint8_t* types, double* out) {
+    double s[kVars] = {0, 0, 0, 0};
+    const long long n = static_cast<long long>(L.nx) * L.ny;
+    for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
+        if (types && types[k] != 0) continue;
+        const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
+        const long long off = L.offset(i, j);
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) s[v] += double(U[v * L.plane + off]);
+    }
+#pragma unroll
+    for (int v = 0; v < kVars; ++v) {
+        double x = s[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&out[v], x);
+    }
+}
+
+// --------------------------------------------- layout conversion / ghosts
+// Host order [4][nx][ny] doubles <-> padded device planes.
+template <class T>
+__global__ void pack_kernel(const double* src, T* dst, const Layout L) {
+    const long long n = static_cast<long long>(L.nx) * L.ny;
+    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < kVars * n;
+         k += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int v = static_cast<int>(k / n);
+        const long long c = k - v * n;
+        const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
+        dst[v * L.plane + L.offset(i, j)] = T(src[k]);
+    }
+}
+
+template <class T>
+__global__ void unpack_kernel(const T* src, double* dst, const Layout L) {
+    const long long n = static_cast<long long>(L.nx) * L.ny;
+    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < kVars * n;
+         k += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int v = static_cast<int>(k / n);
+        const long long c = k - v * n;
+        const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
+        dst[k] = double(src[v * L.plane + L.offset(i, j)]);
+    }
+}
+
+// Fills all ghost layers of a state from its interior: Neumann copies of the
+// adjacent cell, periodic wraps, Dirichlet constants (bcU, conserved), as
+// CartesianMesh::ApplyBoundaryCondition does once before the loop (Run.cpp:128).
+template <class T>
+__global__ void ghost_fill_kernel(T* U, const Layout L, BcSides sides) {
+    const int per = (L.nx > L.ny ? L.nx : L.ny);
+    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < 4LL * kGhost * per * kVars;
+         k += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int v = static_cast<int>(k % kVars);
+        long long rest = k / kVars;
+        const int pos = static_cast<int>(rest % per);
+        rest /= per;
+        const int layer = static_cast<int>(rest % kGhost) + 1;
+        const int side = static_cast<int>(rest / kGhost);
+        T* p = U + v * L.plane;
+        const int bc = sides.bc[side];
+        if (side < 2) {
+            const int j = pos;
+            if (j >= L.ny) continue;
+            const int gi = side == 0 ? -layer : L.nx - 1 + layer;
+            T val;
+            if (bc == kDirichlet) val = T(sides.U[side][v]);
+            else if (bc == kNeumann) val = p[L.offset(side == 0 ? 0 : L.nx - 1, j)];
+            else if (bc == kPeriodic) val = p[L.offset(side == 0 ? gi + L.nx : gi - L.nx, j)];
+            else continue;
+            p[L.offset(gi, j)] = val;
+        } else {
+            const int i = pos;
+            if (i >= L.nx) continue;
+            const int gj = side == 2 ? -layer : L.ny - 1 + layer;
+            T val;
+            if (bc == kDirichlet) val = T(sides.U[side][v]);
+            else if (bc == kNeumann) val = p[L.offset(i, side == 2 ? 0 : L.ny - 1)];
+            else if (bc == kPeriodic) val = p[L.offset(i, side == 2 ? gj + L.ny : gj - L.ny)];
+            else continue;
+            p[L.offset(i, gj)] = val;
+        }
+    }
+}
+
+// ------------------------------------------------- unit-level batches
+template <class Pol>
+__global__ void weno_faces_kernel(int n, const double* st, double* left, double* right, double g, double eps) {
+    using C = typename Pol::C;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    C s[6][kVars];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) s[k][v] = C(st[(f * 6 + k) * kVars + v]);
+    Face5<C> L, R;
+    const C e = C(eps);
+    L.r = weno5<Pol>(s[0][0], s[1][0], s[2][0], s[3][0], s[4][0], e);
+    L.mx = weno5<Pol>(s[0][1], s[1][1], s[2][1], s[3][1], s[4][1], e);
+    L.my = weno5<Pol>(s[0][2], s[1][2], s[2][2], s[3][2], s[4][2], e);
+    L.E = weno5<Pol>(s[0][3], s[1][3], s[2][3], s[3][3], s[4][3], e);
+    R.r = weno5<Pol>(s[5][0], s[4][0], s[3][0], s[2][0], s[1][0], e);
+    R.mx = weno5<Pol>(s[5][1], s[4][1], s[3][1], s[2][1], s[1][1], e);
+    R.my = weno5<Pol>(s[5][2], s[4][2], s[3][2], s[2][2], s[1][2], e);
+    R.E = weno5<Pol>(s[5][3], s[4][3], s[3][3], s[2][3], s[1][3], e);
+    finish_state<Pol>(L, g);
+    finish_state<Pol>(R, g);
+    const Face5<C>* st2[2] = {&L, &R};
+    double* o[2] = {left + 5 * f, right + 5 * f};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        o[q][0] = st2[q]->r;
+        o[q][1] = st2[q]->mx;
+        o[q][2] = st2[q]->my;
+        o[q][3] = st2[q]->E;
+        o[q][4] = st2[q]->p;
+    }
+}
+
+template <class Pol>
+__global__ void hll_faces_kernel(int n, int dir, const double* Lh, const double* Rh, double* F, double g, int variant) {
+    using C = typename Pol::C;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    Face5<C> L, R;
+    L.r = C(Lh[4 * f]); L.mx = C(Lh[4 * f + 1]); L.my = C(Lh[4 * f + 2]); L.E = C(Lh[4 * f + 3]);
+    R.r = C(Rh[4 * f]); R.mx = C(Rh[4 * f + 1]); R.my = C(Rh[4 * f + 2]); R.E = C(Rh[4 * f + 3]);
+    finish_state<Pol>(L, g);
+    finish_state<Pol>(R, g);
+    C out[4];
+    hll_flux<Pol>(L, R, dir, variant, g, out);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) F[4 * f + q] = out[q];
+}
+
+}  // namespace cfs

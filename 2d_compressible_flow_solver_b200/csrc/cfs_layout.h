@@ -1,0 +1,100 @@
+// Device grid layout and kernel argument blocks shared by the host code and the
+// kernels.  Plain C++ (no CUDA syntax) so that g++-compiled host files can use it.
+//
+// State: four planes (rho, rho u, rho v, E), each (nx + 6) rows of `pitch`
+// elements.  Row r = i + 3 holds x index i (i = -3 .. nx+2); element j of a
+// row (j = -3 .. ny+2) sits at column joff + j, where joff is one 128-byte block
+// so that every interior row starts 128-byte aligned.  The three ghost layers
+// per side are maintained by the kernels (Neumann copies, periodic wraps) or set
+// once (Dirichlet states), so a stage kernel reads a tile plus its 3-cell halo
+// with no boundary logic in the load path.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define CFS_HD __host__ __device__ __forceinline__
+#else
+#define CFS_HD inline
+#endif
+
+namespace cfs {
+
+constexpr int kGhost = 3;
+constexpr int kVars = 4;
+
+enum BcKind : int { kNeumann = 0, kDirichlet = 1, kPeriodic = 2, kHalo = 3 };
+
+struct Layout {
+    int nx, ny;
+    int pitch;           // elements per row
+    int joff;            // column of j = 0
+    long long plane;     // elements per variable plane
+    int elem_bytes;      // 8 (FP64) or 4 (FP32)
+
+    static Layout make(int nx, int ny, int elem_bytes) {
+        Layout L;
+        L.nx = nx;
+        L.ny = ny;
+        L.elem_bytes = elem_bytes;
+        const int blk = 128 / elem_bytes;
+        L.joff = blk;
+        const int need = L.joff + ny + kGhost;
+        L.pitch = ((need + blk - 1) / blk) * blk;
+        L.plane = static_cast<long long>(nx + 2 * kGhost) * L.pitch;
+        return L;
+    }
+    CFS_HD long long offset(int i, int j) const { return static_cast<long long>(i + kGhost) * pitch + joff + j; }
+    long long bytes() const { return plane * kVars * elem_bytes; }
+};
+
+// Boundary kinds of the four sides (left, right, bottom, top) and the
+// conserved ghost state of each Dirichlet side.
+struct BcSides {
+    int bc[4];
+    double U[4][4];
+};
+
+// Device-resident step parameters used by graph-replayed steps.
+struct DevParams {
+    unsigned long long wmax[2];   // max wave-speed sums (FP64 bit patterns), ping-pong per step
+    double dt_fixed;
+    double cfl;
+    double t;                     // simulated time advanced
+    double dt_last;
+    int use_cfl;
+    int pad;
+};
+
+struct StageArgs {
+    const void* in;        // state differentiated this stage (tile + halo reads)
+    const void* u0;        // RK stage-0 copy (pointwise reads), stage >= 1
+    const void* u1;        // RK stage-1 copy, TVD3-as-written stage 2
+    void* out;             // new state (interior + ghost copies)
+    double* rhs;           // optional RHS, [4][nx][ny]
+    const uint8_t* types;  // optional cell types [nx][ny]; null = all fluid
+    Layout L;
+    int bc[4];
+    double gamma, eps, dx, dy;
+    int stage, rk, hll;
+    int viscous;
+    double mu, prandtl, mach;
+    double dt;             // used when P is null
+    DevParams* P;          // graph mode: dt from P (fixed or CFL), t accounting
+    int parity;            // graph mode: which wmax slot holds this step's max
+    int last_stage;        // 1: accumulate the CFL max of the new state into P->wmax[1-parity]
+    int first_stage;       // 1: reset P->wmax[1-parity], advance P->t
+};
+
+struct IbArgs {
+    void* U;               // state to fill in place
+    Layout L;
+    int n;
+    int mode;              // 0 reference LDLT replay, 1 bilinear + slip
+    const int* cell;       // [n] linear index i*ny + j
+    const int* donor;      // [4n] linear index i*ny + j
+    const double* image;   // [2n]
+    const double* fac;     // [16n] reference: l10 l20 l21 l30 l31 l32 d0..d3 (10); bilinear: w0..w3 nx ny
+    const int* perm;       // [4n] reference pivot order
+};
+
+}  // namespace cfs

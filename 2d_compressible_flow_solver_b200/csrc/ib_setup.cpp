@@ -1,0 +1,210 @@
+// Host-side immersed-boundary set-up.  Built with -ffp-contract=off so that
+// the classification, image points and donor lists reproduce the reference's
+// doubles exactly (Circle.cpp uses only + - * / sqrt, cos and sin).
+#include "ib_setup.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <limits>
+#include <utility>
+
+namespace cfs {
+
+namespace {
+
+struct P2 {
+    double x, y;
+};
+
+// v / sqrt(v.v) when v.v > 0, else v (Eigen's normalized()).
+inline P2 normalized(P2 v) {
+    const double z = v.x * v.x + v.y * v.y;
+    if (z > 0.0) {
+        const double n = std::sqrt(z);
+        return {v.x / n, v.y / n};
+    }
+    return v;
+}
+
+inline double norm(P2 v) { return std::sqrt(v.x * v.x + v.y * v.y); }
+
+}  // namespace
+
+bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
+                  IbList& out, std::string& err) {
+    if (npoints < 3) {
+        err = "circle needs at least 3 polygon points";
+        return false;
+    }
+    const double dx = lx / nx, dy = ly / ny;  // CartesianMesh::CalCellsize (CartesianMesh.cpp:150-154)
+    auto centre = [&](int i, int j) { return P2{(i + 0.5) * dx, (j + 0.5) * dy}; };  // CartesianMesh.cpp:92
+
+    // Circle::Initialize (Circle.cpp:12-41): polygon vertices and unit segment
+    // directions (segment k runs from vertex k to vertex k+1).
+    std::vector<P2> pts(npoints), dir(npoints);
+    for (int k = 0; k < npoints; ++k) {
+        const double angle = 2.0 * M_PI * static_cast<double>(k) / static_cast<double>(npoints);
+        pts[k] = {cx + radius * std::cos(angle), cy + radius * std::sin(angle)};
+    }
+    for (int k = 0; k < npoints; ++k) {
+        const P2 a = pts[k], b = pts[(k + 1) % npoints];
+        dir[k] = normalized({b.x - a.x, b.y - a.y});
+    }
+
+    // DistinguishWallandFluid (Circle.cpp:43-51): solid iff |x_c - c| <= r.
+    std::vector<uint8_t>& t = out.types;
+    t.assign(static_cast<size_t>(nx) * ny, 0);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const P2 p = centre(i, j);
+            if (norm({p.x - cx, p.y - cy}) <= radius) t[static_cast<size_t>(i) * ny + j] = 1;
+        }
+
+    // SetGhostcell(cells, 3) (Circle.cpp:53-103): from every fluid cell, walk
+    // each axis direction into solid/ghost cells and mark up to 3 as ghosts.
+    const int dirs[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+    auto at = [&](int i, int j) -> uint8_t& { return t[static_cast<size_t>(i) * ny + j]; };
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (at(i, j) != 0) continue;
+            for (const auto& d : dirs) {
+                const int ni = i + d[0], nj = j + d[1];
+                if (ni >= 0 && ni < nx && nj >= 0 && nj < ny && at(ni, nj) != 0) {
+                    for (int k = 1; k <= 3; ++k) {
+                        const int gi = i + k * d[0], gj = j + k * d[1];
+                        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny && at(gi, gj) != 0) at(gi, gj) = 2;
+                        else break;
+                    }
+                }
+            }
+        }
+
+    out.cell.clear();
+    out.donor.clear();
+    out.image.clear();
+    out.normal.clear();
+    const P2 origin = centre(0, 0);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (at(i, j) != 2) continue;
+            // SetImagepoint (Circle.cpp:105-138): nearest segment line by
+            // orthogonal projection (strictly smaller distance wins), mirror.
+            const P2 pos = centre(i, j);
+            double minDistance = std::numeric_limits<double>::max();
+            P2 intercept{0.0, 0.0};
+            for (int k = 0; k < npoints; ++k) {
+                const P2 s = dir[k], a = pts[k];
+                const double dd = s.x * (pos.x - a.x) + s.y * (pos.y - a.y);
+                const P2 proj{dd * s.x + a.x, dd * s.y + a.y};
+                const double dist = norm({proj.x - pos.x, proj.y - pos.y});
+                if (dist < minDistance) {
+                    minDistance = dist;
+                    intercept = proj;
+                }
+            }
+            const P2 n = normalized({intercept.x - pos.x, intercept.y - pos.y});
+            const P2 img{pos.x + 2 * (minDistance * n.x), pos.y + 2 * (minDistance * n.y)};
+
+            // FindNearest4FluidCellsIndexed (Circle.cpp:160-215): fluid cells of
+            // the 11 x 11 window around the image point's cell, visited i outer /
+            // j inner, sorted by squared distance with the same comparator.
+            const int ic = static_cast<int>((img.x - origin.x) / dx);
+            const int jc = static_cast<int>((img.y - origin.y) / dy);
+            std::vector<std::pair<double, int>> cand;
+            for (int a = ic - 5; a <= ic + 5; ++a)
+                for (int b = jc - 5; b <= jc + 5; ++b) {
+                    if (a >= 0 && a < nx && b >= 0 && b < ny && at(a, b) == 0) {
+                        const P2 c = centre(a, b);
+                        const double ddx = c.x - img.x, ddy = c.y - img.y;
+                        cand.emplace_back(ddx * ddx + ddy * ddy, a * ny + b);
+                    }
+                }
+            std::sort(cand.begin(), cand.end(),
+                      [](const std::pair<double, int>& p, const std::pair<double, int>& q) { return p.first < q.first; });
+            if (cand.size() < 4) {
+                err = "immersed-ghost cell (" + std::to_string(i) + ", " + std::to_string(j) + ") has " +
+                      std::to_string(cand.size()) + " fluid donors, 4 needed";
+                return false;
+            }
+            out.cell.push_back(i * ny + j);
+            for (int k = 0; k < 4; ++k) out.donor.push_back(cand[k].second);
+            out.image.push_back(img.x);
+            out.image.push_back(img.y);
+            out.normal.push_back(n.x);
+            out.normal.push_back(n.y);
+        }
+    return true;
+}
+
+// Outer-product LDL^T with symmetric diagonal pivoting (largest remaining
+// |diagonal| first; Golub & Van Loan 4.1/4.4, Higham ch. 10-11), reading the
+// lower triangle only, as Eigen documents for ldlt().
+void ldlt4_lower(const double M[4][4], double fac[10], int perm[4]) {
+    double w[4][4], l[4][4], d[4];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            w[r][c] = (r >= c) ? M[r][c] : M[c][r];
+            l[r][c] = 0.0;
+        }
+    for (int k = 0; k < 4; ++k) perm[k] = k;
+    for (int k = 0; k < 4; ++k) {
+        int p = k;
+        double best = std::fabs(w[k][k]);
+        for (int i = k + 1; i < 4; ++i) {
+            const double v = std::fabs(w[i][i]);
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (p != k) {
+            for (int c = 0; c < 4; ++c) std::swap(w[k][c], w[p][c]);
+            for (int r = 0; r < 4; ++r) std::swap(w[r][k], w[r][p]);
+            for (int c = 0; c < k; ++c) std::swap(l[k][c], l[p][c]);
+            std::swap(perm[k], perm[p]);
+        }
+        const double dk = w[k][k];
+        d[k] = dk;
+        const bool usable = std::fabs(dk) > DBL_MIN;
+        for (int i = k + 1; i < 4; ++i) l[i][k] = usable ? w[i][k] / dk : 0.0;
+        for (int i = k + 1; i < 4; ++i)
+            for (int j = k + 1; j < 4; ++j) w[i][j] = w[i][j] - l[i][k] * dk * l[j][k];
+    }
+    fac[0] = l[1][0];
+    fac[1] = l[2][0];
+    fac[2] = l[2][1];
+    fac[3] = l[3][0];
+    fac[4] = l[3][1];
+    fac[5] = l[3][2];
+    for (int k = 0; k < 4; ++k) fac[6 + k] = d[k];
+}
+
+bool bilinear_weights(const double M[4][4], double X, double Y, double w[4]) {
+    double A[4][5];
+    const double rhs[4] = {X * Y, X, Y, 1.0};
+    for (int r = 0; r < 4; ++r) {
+        for (int c = 0; c < 4; ++c) A[r][c] = M[c][r];
+        A[r][4] = rhs[r];
+    }
+    for (int k = 0; k < 4; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < 4; ++r)
+            if (std::fabs(A[r][k]) > std::fabs(A[piv][k])) piv = r;
+        if (A[piv][k] == 0.0) return false;
+        if (piv != k)
+            for (int c = 0; c < 5; ++c) std::swap(A[k][c], A[piv][c]);
+        for (int r = k + 1; r < 4; ++r) {
+            const double m = A[r][k] / A[k][k];
+            for (int c = k; c < 5; ++c) A[r][c] -= m * A[k][c];
+        }
+    }
+    for (int r = 3; r >= 0; --r) {
+        double s = A[r][4];
+        for (int c = r + 1; c < 4; ++c) s -= A[r][c] * w[c];
+        w[r] = s / A[r][r];
+    }
+    return true;
+}
+
+}  // namespace cfs

@@ -1,0 +1,88 @@
+// Kernels whose FP64 rounding must follow the reference's operation order:
+// built with -fmad=false so no multiply-add is contracted, IEEE division and
+// square root (nvcc defaults).  Holds the CFS_FP64_EXACT stage, the immersed-
+// ghost fill, the CFL reduction and the layout helpers for both storage types.
+#include "cfs_kernels.cuh"
+#include "cfs_launch.h"
+
+namespace cfs {
+
+namespace {
+inline dim3 stage_grid(const Layout& L) {
+    return dim3((L.ny + kTileJ - 1) / kTileJ, (L.nx + kTileI - 1) / kTileI);
+}
+inline int flat_blocks(long long work, int nt) {
+    long long b = (work + nt - 1) / nt;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return static_cast<int>(b);
+}
+}  // namespace
+
+cudaError_t launch_stage_exact(const StageArgs& a, cudaStream_t s) {
+    stage_kernel<PolExact, kTileI, kTileJ><<<stage_grid(a.L), kTileI * kTileJ, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ib_fill(int elem_bytes, const IbArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    const int nt = 128, nb = (a.n + nt - 1) / nt;
+    if (elem_bytes == 8) ib_fill_kernel<double><<<nb, nt, 0, s>>>(a);
+    else ib_fill_kernel<float><<<nb, nt, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wmax(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double g, double dx,
+                        double dy, unsigned long long* out, cudaStream_t s) {
+    constexpr int nt = 256;
+    const int nb = flat_blocks(static_cast<long long>(L.nx) * L.ny, nt);
+    if (elem_bytes == 8) wmax_kernel<double, nt><<<nb, nt, 0, s>>>(static_cast<const double*>(U), L, types, g, dx, dy, out);
+    else wmax_kernel<float, nt><<<nb, nt, 0, s>>>(static_cast<const float*>(U), L, types, g, dx, dy, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
+                          cudaStream_t s) {
+    constexpr int nt = 256;
+    const int nb = flat_blocks(static_cast<long long>(L.nx) * L.ny, nt);
+    if (elem_bytes == 8) totals_kernel<double, nt><<<nb, nt, 0, s>>>(static_cast<const double*>(U), L, types, out);
+    else totals_kernel<float, nt><<<nb, nt, 0, s>>>(static_cast<const float*>(U), L, types, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(int elem_bytes, const double* src, void* dst, const Layout& L, cudaStream_t s) {
+    const int nt = 256, nb = flat_blocks(4LL * L.nx * L.ny, nt);
+    if (elem_bytes == 8) pack_kernel<double><<<nb, nt, 0, s>>>(src, static_cast<double*>(dst), L);
+    else pack_kernel<float><<<nb, nt, 0, s>>>(src, static_cast<float*>(dst), L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(int elem_bytes, const void* src, double* dst, const Layout& L, cudaStream_t s) {
+    const int nt = 256, nb = flat_blocks(4LL * L.nx * L.ny, nt);
+    if (elem_bytes == 8) unpack_kernel<double><<<nb, nt, 0, s>>>(static_cast<const double*>(src), dst, L);
+    else unpack_kernel<float><<<nb, nt, 0, s>>>(static_cast<const float*>(src), dst, L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_fill(int elem_bytes, void* U, const Layout& L, const BcSides& sides, cudaStream_t s) {
+    const int per = L.nx > L.ny ? L.nx : L.ny;
+    const int nt = 256, nb = flat_blocks(4LL * kGhost * per * kVars, nt);
+    if (elem_bytes == 8) ghost_fill_kernel<double><<<nb, nt, 0, s>>>(static_cast<double*>(U), L, sides);
+    else ghost_fill_kernel<float><<<nb, nt, 0, s>>>(static_cast<float*>(U), L, sides);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_weno_faces_exact(int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    weno_faces_kernel<PolExact><<<(n + 127) / 128, 128, 0, s>>>(n, st, l, r, g, eps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hll_faces_exact(int n, int dir, const double* L, const double* R, double* F, double g, int v,
+                                   cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    hll_faces_kernel<PolExact><<<(n + 127) / 128, 128, 0, s>>>(n, dir, L, R, F, g, v);
+    return cudaGetLastError();
+}
+
+}  // namespace cfs

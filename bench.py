@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the stage engine: Mcell-steps/s on the smooth
+periodic advection workload (rho = 1 + 0.2 sin(2 pi (x+y)), u = v = 1, p = 1 on
+[0,1]^2, CFL 0.4, SSP-RK3, WENO5 eps 1e-2, Davis HLL) at 4096^2 cells, the
+bandwidth-roofline configuration.  A step is one full RK3 step (3 fused stage
+launches) over every cell; inputs are resident in HBM when timing starts.
+
+Arms:
+  default            the engine: FP32-mixed form (headline ``value``), with the
+                     FP64 form, the FP32-vs-FP64 accuracy check at t = 0.5 on a
+                     1024^2 grid, the end-to-end number through the C ABI with
+                     pinned host buffers, the roofline and a CPU baseline (the
+                     reference's own classes, timed on the host cores).
+  --impl reference   the reference's own CPU implementation (oracle/_ref, built
+                     with the reference Makefile's optimisation flags) on all host
+                     cores, on bounded samples of the same workload.
+
+Multi-GPU (torchrun, one rank per GPU): every rank advances its own 4096^2
+periodic domain (weak scaling); there is no exchange between ranks, so no
+collective is on the data path; timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+PKG = "2d_compressible_flow_solver_b200"
+METRIC = "Mcell-steps/s FP32-mixed vs FP64 on 1 B200 at ρ L1 err ≤1e-5; % HBM roofline"
+UNIT = "Mcell-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+# Algorithmic DRAM bytes per cell-step of SSP-RK3: stage 1 reads and writes U,
+# stages 2 and 3 read U_s and U^n and write U -> 32 state words.
+WORDS_PER_CELL_STEP = 32
+# DRAM traffic of one stage launch per cell, from the ncu capture summarised in
+# profiles/ (dram__bytes_read.sum + dram__bytes_write.sum of stage_kernel,
+# scaled by cells); None until a capture exists for the current kernel.
+MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": None, "f64": None}
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) of the GPU's clocks and throttle reasons."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------- CPU reference timing
+def _ref_sample_worker(args):
+    """One bounded sample of the reference's own classes (perf build): one RK3
+    step (3 Run::solver iterations) of the smooth workload on an n x n grid with
+    transmissive sides (the reference has no periodic sides).  Returns
+    (cells, seconds of the stage loop)."""
+    n, root = args
+    sys.path.insert(0, str(root))
+    sys.path.insert(0, str(root / "tests"))
+    import oracle_bind as ob
+    wl = importlib.import_module(f"{PKG}.workloads")
+    lib = ob.ref_lib(perf=True)
+    w = wl.smooth_advection(n)
+    c = ob.make_ref_config(n, n, integrator=3, dt=1e-4)
+    U = np.ascontiguousarray(w.U0)
+    secs = lib.ref_time_stages(ctypes.byref(c), ob.P(U), 3)
+    return n * n, secs
+
+
+def cpu_reference_rate(nproc: int, n: int, rounds: int, warm: int = 0):
+    """Aggregate Mcell-steps/s of nproc concurrent reference processes, each on
+    its own n x n sample (the MPI build's per-rank work without its halo
+    exchange).  Returns (rate per round list, seconds per round list)."""
+    ctx = mp.get_context("spawn")
+    rates, walls = [], []
+    with ctx.Pool(nproc) as pool:
+        for r in range(warm + rounds):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_sample_worker, [(n, ROOT)] * nproc)
+            wall = time.perf_counter() - t0
+            if r >= warm:
+                rates.append(sum(cells / secs for cells, secs in res) / 1e6)
+                walls.append(wall)
+    return rates, walls
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------- engine arm
+def engine_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = env_rank()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    cfsb = importlib.import_module(PKG)
+    wl = importlib.import_module(f"{PKG}.workloads")
+    n, K, W = args.n, args.steps, args.warmup
+    w = wl.smooth_advection(n)
+    kw = dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=(cfsb.BC_PERIODIC,) * 4, device=local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed_advance(prec, steps, warm):
+        s = cfsb.Solver(n, n, precision=prec, **kw)
+        s.set_state(w.U0)
+        stream = torch.cuda.ExternalStream(s.stream, device=local)
+        if warm:
+            s.advance(warm, cfl=w.cfl)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t_sim, dt_last = s.advance(steps, cfl=w.cfl)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        totals = s.totals()
+        s.close()
+        return ms, t_sim, dt_last, totals
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms32, t32, dt32, _ = timed_advance(cfsb.FP32_MIXED, K, W)
+    clocks = sampler.stop()
+    ms64, _, _, _ = timed_advance(cfsb.FP64, K, W)
+    if world > 1:
+        t = torch.tensor([ms32, ms64], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms32, ms64 = float(t[0]), float(t[1])
+    cells = n * n
+    v32 = cells * K * world / (ms32 / 1e3) / 1e6
+    v64 = cells * K * world / (ms64 / 1e3) / 1e6
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        bytes32 = WORDS_PER_CELL_STEP * 4 * cells * K
+        achieved = bytes32 / (ms32 / 1e3) / 1e9
+        launches = 3 * K + 1
+        per_launch_ms = ms32 / launches
+        trf = MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH["f32"]
+        result = {
+            "metric": METRIC, "value": round(v32, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": round(ms32 / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"smooth periodic advection {n}x{n} (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1), "
+                                   "SSP-RK3, WENO5 eps 1e-2, Davis HLL, CFL 0.4 on-device dt",
+                       "precision": "fp32-mixed", "grid": [n, n], "cells_per_gpu": cells,
+                       "l2": "inputs larger than L2 (3 state buffers of "
+                             f"{4 * 4 * cells / 1e6:.0f} MB each)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": None if trf is None else trf * cells,
+                         "algorithmic_bytes_per_cell_step": WORDS_PER_CELL_STEP * 4,
+                         "avg_stage_launch_ms": round(per_launch_ms, 4)},
+            "fp64": {"value": round(v64, 1), "ms_per_step": round(ms64 / K, 4),
+                     "roofline_frac": round(WORDS_PER_CELL_STEP * 8 * cells * K / (ms64 / 1e3) / 1e9 / peak, 4),
+                     "fp32_over_fp64": round(v32 / v64, 3)},
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+    # accuracy of FP32-mixed against FP64 at t_end (fixed dt so both forms sit
+    # on the same time levels), and conservation drift
+    if rank == 0 and args.accuracy_n > 0:
+        ne = args.accuracy_n
+        we = wl.smooth_advection(ne)
+        with cfsb.Solver(ne, ne, precision=cfsb.FP64, **kw) as s:
+            s.set_state(we.U0)
+            dt0 = s.compute_dt(we.cfl)
+        nsteps = int(math.ceil(we.t_end / dt0))
+        dt = we.t_end / nsteps
+        states = {}
+        for prec in (cfsb.FP64, cfsb.FP32_MIXED):
+            with cfsb.Solver(ne, ne, precision=prec, **kw) as s:
+                s.set_state(we.U0)
+                m0 = s.totals()
+                s.advance(nsteps, dt=dt)
+                states[prec] = (s.get_state(), m0, s.totals())
+        U64, U32 = states[cfsb.FP64][0], states[cfsb.FP32_MIXED][0]
+        m0, m1 = states[cfsb.FP32_MIXED][1], states[cfsb.FP32_MIXED][2]
+        exact = wl.smooth_advection_exact(ne, we.t_end)
+        result["accuracy"] = {
+            "grid": [ne, ne], "t_end": we.t_end, "steps": nsteps,
+            "rho_L1_fp32_vs_fp64": float(np.abs(U32[0] - U64[0]).mean()),
+            "rho_Linf_fp32_vs_fp64": float(np.abs(U32[0] - U64[0]).max()),
+            "E_L1_fp32_vs_fp64": float(np.abs(U32[3] - U64[3]).mean()),
+            "E_Linf_fp32_vs_fp64": float(np.abs(U32[3] - U64[3]).max()),
+            "mass_drift": float(abs(m1[0] - m0[0]) / abs(m0[0])),
+            "energy_drift": float(abs(m1[3] - m0[3]) / abs(m0[3])),
+            "rho_L1_fp64_vs_exact": float(np.abs(U64[0] - exact).mean()),
+        }
+    # end to end through the C ABI with pinned host buffers: initial state up,
+    # K steps each reading back its dt and time, final state down
+    if rank == 0:
+        pin = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
+        pin.numpy()[:] = w.U0
+        out = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
+        with cfsb.Solver(n, n, precision=cfsb.FP32_MIXED, **kw) as s:
+            s.set_state(pin.numpy())
+            s.advance(2, cfl=w.cfl)
+            s.synchronize()
+            t0 = time.perf_counter()
+            s.set_state(pin.numpy())
+            for _ in range(K):
+                s.advance(1, cfl=w.cfl)
+            s.get_state(out.numpy())
+            wall = time.perf_counter() - t0
+        state_bytes = 4 * cells * 8
+        result["e2e"] = {"value": round(cells * K / wall / 1e6, 1), "unit": UNIT,
+                         "h2d_bytes_per_step": int(state_bytes / K + 40),
+                         "d2h_bytes_per_step": int(state_bytes / K + 48),
+                         "how": "cfs_set_state from pinned host, K x cfs_advance(1) with dt/t read back, "
+                                "cfs_get_state to pinned host; host wall clock"}
+    # CPU baseline: the reference's own classes on the host cores (rank 0, N=1)
+    if rank == 0:
+        if world == 1 and args.cpu_sample > 0:
+            cores = host_cores()
+            try:
+                rates, walls = cpu_reference_rate(cores, args.cpu_sample, 1)
+                result["cpu_baseline"] = {
+                    "value": round(rates[0], 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                    "sample": f"{cores} concurrent single-rank processes of the reference's classes "
+                              f"(-O3 -ffast-math build), each one RK3 step on a {args.cpu_sample}^2 grid of the "
+                              f"same workload (transmissive sides); {walls[0]:.1f} s wall",
+                }
+            except Exception as e:  # noqa: BLE001
+                result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                          "sample": f"unavailable: {e}"}
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------- reference arm
+def reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    cores = host_cores()
+    lib = ROOT / "oracle" / "_ref" / "libref_perf.so"
+    if not lib.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_perf.so not built "
+                          "(needs the reference tree; run __graft_entry__.build())"}), flush=True)
+        return
+    n = args.cpu_sample
+    rates, walls = cpu_reference_rate(cores, n, args.steps, warm=args.warmup)
+    v = statistics.median(rates)
+    ms_per_step = 4096 * 4096 / (v * 1e6) * 1e3
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"smooth periodic advection {args.n}x{args.n} (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1), "
+                               "SSP-RK3, WENO5 eps 1e-2, Davis HLL, CFL 0.4 on-device dt",
+                   "precision": "reference FP64 (-O3 -ffast-math)", "grid": [args.n, args.n]},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"each step: {cores} concurrent single-rank processes of the reference's classes, "
+                                   f"one RK3 step (TVD3rdRK) on a {n}^2 grid of the workload with transmissive sides "
+                                   "(no periodic sides in the reference); ms_per_step extrapolated to the full grid"},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--n", type=int, default=4096, help="grid edge (cells) per GPU")
+    ap.add_argument("--accuracy-n", type=int, default=1024, help="grid of the FP32-vs-FP64 check (0 = skip)")
+    ap.add_argument("--cpu-sample", type=int, default=384, help="grid edge of one CPU-baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+/* cfs.h - C ABI of the B200 (sm_100a) compressible-flow stage engine.
+ *
+ * One context owns one device-resident Cartesian grid (nx by ny cells on
+ * [0,lx] x [0,ly]) with three ghost layers per side, and runs the per-RK-stage
+ * hot path of the reference solver (xinxiangsama/2d_Compressible_Flow_Solver)
+ * as fused CUDA kernels: immersed-ghost fill, WENO5 reconstruction of the
+ * conserved variables, HLL interface flux, flux difference, TVD Runge-Kutta
+ * update of fluid cells, physical-boundary ghost refresh and the CFL step.
+ *
+ * Host arrays use the reference's cell order: U[v][i][j], v = (rho, rho u,
+ * rho v, E), i = x index (outer), j = y index (inner), as cells[i][j]
+ * (CartesianMesh.cpp:3-9) and the HDF5 datasets (Output.cpp:60).
+ *
+ * Every call returns CFS_OK (0) or a positive error code; the message of the
+ * last failure of a context is cfs_last_error(ctx) (cfs_last_error(NULL) after
+ * a failed cfs_create).  Calls on one context come from one host thread; all
+ * work of a context is ordered on the context's CUDA stream.  There is no CPU
+ * fallback: without a usable CUDA device cfs_create fails with CFS_ERR_CUDA.
+ */
+#ifndef CFS_H
+#define CFS_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFS_ABI_VERSION 1
+
+enum cfs_status {
+    CFS_OK = 0,
+    CFS_ERR_INVALID = 1,    /* bad argument or configuration */
+    CFS_ERR_CUDA = 2,       /* a CUDA call failed (message has the CUDA error) */
+    CFS_ERR_NOMEM = 3,      /* device or host allocation failed */
+    CFS_ERR_STATE = 4,      /* call not valid in the context's current state */
+    CFS_ERR_NUMERIC = 5     /* non-finite or non-positive dt from the CFL reduction */
+};
+
+enum cfs_precision {
+    CFS_FP64 = 0,        /* FP64 state and arithmetic, FMA-contracted kernels */
+    CFS_FP32_MIXED = 1,  /* FP32 state/WENO/HLL; FP64 p and c where kinetic energy
+                            exceeds 90% of E, FP64 dt and conservation sums */
+    CFS_FP64_EXACT = 2   /* FP64 in the reference's operation order, no FMA:
+                            bit-identical to the reference built without fast-math */
+};
+
+enum cfs_rk {
+    CFS_RK_TVD2 = 0,            /* TVD2rdRK (TVD2rdRK.cpp:3-31), the driver's choice (Run.cpp:47) */
+    CFS_RK_TVD3_REFERENCE = 1,  /* TVD3rdRK as written (TVD3rdRK.cpp:3-48): stage 3 uses U1 */
+    CFS_RK_SSP3 = 2             /* Shu-Osher SSP-RK3 (no reference counterpart) */
+};
+
+enum cfs_hll {
+    CFS_HLL_REFERENCE = 0,  /* RiemmanSolverHLL::Solver (RiemmanSolverHLL.cpp:5-75), wave bounds as written */
+    CFS_HLL_DAVIS = 1       /* Davis bounds min/max(u_L -+ a_L, u_R -+ a_R) (no reference counterpart) */
+};
+
+enum cfs_bc {
+    CFS_BC_NEUMANN = 0,    /* NeummanBoundary (NeummanBoundary.cpp:31-45): ghost = adjacent cell */
+    CFS_BC_DIRICHLET = 1,  /* DirichletBoundary (DirichletBoundary.cpp:32-46): fixed state */
+    CFS_BC_PERIODIC = 2    /* no reference counterpart */
+};
+
+enum cfs_cell_type { CFS_CELL_FLUID = 0, CFS_CELL_SOLID = 1, CFS_CELL_IMMERSED_GHOST = 2 };
+
+enum cfs_ib_mode {
+    CFS_IB_REFERENCE = 0,      /* ImagePoint::InterpolatePhase (ImagePoint.cpp:20-82): LDLT of the
+                                  donor matrix's lower triangle, both momenta negated (Cell.cpp:172-181) */
+    CFS_IB_BILINEAR_SLIP = 1   /* true bilinear weights, only the wall-normal momentum reflected */
+};
+
+enum cfs_viscous { CFS_VISCOUS_OFF = 0, CFS_VISCOUS_NS = 1 };
+
+typedef struct cfs_config {
+    int nx, ny;              /* cells; CartesianMesh::setnumberCellsX/YGlobal (Run.cpp:17-18) */
+    double lx, ly;           /* domain lengths; setGlobalLengthX/Y (Run.cpp:19-20) */
+    double gamma;            /* Gamma, param.h:5 (1.4) */
+    double weno_eps;         /* Weno5th.cpp:5 (1e-2) */
+    int precision;           /* enum cfs_precision */
+    int rk;                  /* enum cfs_rk */
+    int hll;                 /* enum cfs_hll */
+    int bc[4];               /* enum cfs_bc for left, right, bottom, top (Cylinder.cpp:19-40 order) */
+    double bc_prim[4][4];    /* Dirichlet (rho, u, v, p) per side, applied as Cylinder.cpp:22-32 */
+    int viscous;             /* enum cfs_viscous */
+    double mu, prandtl, mach;/* Navier-Stokes constants (constant viscosity, T = gamma Ma^2 p / rho) */
+    int keep_rhs;            /* 1: keep the last stage's RHS for cfs_get_rhs (Cell::comRHS m_flux) */
+    int device;              /* CUDA device ordinal */
+} cfs_config;
+
+typedef struct cfs_ctx cfs_ctx;
+
+/* Fills a config with the reference's defaults: gamma 1.4, eps 1e-2, FP64,
+ * TVD3 as written, reference HLL, Neumann sides, inviscid. */
+void cfs_config_default(cfs_config* cfg);
+
+/* Creates a context and allocates the device grid.
+ * Replaces Run::initialize's mesh/plugin set-up (Run.cpp:10-90): the plugin
+ * selection point Run.cpp:41-48 maps to cfg->{rk,hll,weno_eps,bc}. */
+int cfs_create(const cfs_config* cfg, cfs_ctx** out);
+int cfs_destroy(cfs_ctx* ctx);
+const char* cfs_last_error(const cfs_ctx* ctx);
+int cfs_abi_version(void);
+
+/* Conserved state in and out (host U[4][nx][ny]).
+ * set: Initialcondition::fillIn (Initialcondition.h:11) over all cells, then
+ *      the physical-boundary ghost fill (CartesianMesh::ApplyBoundaryCondition,
+ *      CartesianMesh.cpp:280-305, called at Run.cpp:128).
+ * get: the cell phases Output::WriteToHDF5 reads (Output.cpp:58-75). */
+int cfs_set_state(cfs_ctx* ctx, const double* U);
+int cfs_get_state(cfs_ctx* ctx, double* U);
+
+/* RHS R = -(dF/dx + dG/dy) of the last stage (Cell::comRHS, Cell.cpp:110-162,
+ * stored in Cell::m_flux and written as FluxRho/FluxMu/FluxMv/FluxEnergy by
+ * Output.cpp:38-41).  Requires cfg.keep_rhs = 1.  Host R[4][nx][ny]. */
+int cfs_get_rhs(cfs_ctx* ctx, double* R);
+
+/* Cell types (enum cfs_cell_type), host types[nx][ny]; default all fluid.
+ * Only fluid cells are advanced (Run.cpp:193-200). */
+int cfs_set_cell_types(cfs_ctx* ctx, const uint8_t* types);
+
+/* Immersed-ghost list: n cells (i*ny + j), 4 fluid donors each (i*ny + j, in
+ * the reference's nearest-first order), the image point (x, y) of each, and
+ * for CFS_IB_BILINEAR_SLIP the unit wall normal.  Replaces the ImagePoint
+ * objects Circle::SetImagepoint builds (Circle.cpp:105-138). */
+int cfs_set_ib(cfs_ctx* ctx, int mode, int n, const int32_t* cell, const int32_t* donor4,
+               const double* image_xy, const double* normal_xy);
+
+/* Circle immersed boundary built on the host exactly as the reference does it:
+ * Circle::Initialize (Circle.cpp:12-41) with npoints vertices,
+ * DistinguishWallandFluid (:43-51), SetGhostcell(cells, 3) (:53-103),
+ * SetImagepoint (:105-138) and FindNearest4FluidCellsIndexed (:160-215);
+ * then cfs_set_cell_types + cfs_set_ib.  Fails with CFS_ERR_INVALID when an
+ * immersed-ghost cell finds fewer than 4 fluid donors (the reference then reads
+ * past its donor list, ImagePoint.cpp:25). */
+int cfs_ib_build_circle(cfs_ctx* ctx, double radius, double cx, double cy, int npoints, int mode);
+
+/* The same circle set-up as cfs_ib_build_circle, host only (no context, no
+ * device): writes types[nx][ny] and, for the first min(n, max_n) immersed-ghost
+ * cells (i outer, j inner order), cell index, 4 donors, image point and unit
+ * normal (from the ghost centre to its image point).  *n receives the total. */
+int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
+                     uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy,
+                     double* normal_xy);
+
+/* Read-back of the immersed-boundary set-up: types[nx][ny], and for the first
+ * min(n, max_n) immersed-ghost cells (i outer, j inner order) their cell
+ * index, donors and image point.  *n receives the total count. */
+int cfs_get_ib(cfs_ctx* ctx, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy);
+
+/* Fills immersed-ghost cells from their image points now
+ * (Cell::comImmersedGhostPhase over IG cells, Run.cpp:107-113,156-162). */
+int cfs_ib_fill(cfs_ctx* ctx);
+
+/* CFL step on the current state: dt = cfl / max over fluid cells of
+ * (|u|+a)/dx + (|v|+a)/dy.  No reference counterpart (the reference fixes dt,
+ * param.h:20, set by Explicit::setTimeStep at Run.cpp:95).  Warp-shuffle max
+ * reduction; the max is exact, so dt is the same on every launch. */
+int cfs_compute_dt(cfs_ctx* ctx, double cfl, double* dt);
+
+/* One iteration of Run::solver's loop (Run.cpp:153-203) with loop counter
+ * `counter` (1, 2, 3, ...), whose stage is derived as TVD2rdRK.cpp:11 /
+ * TVD3rdRK.cpp:15 do: immersed-ghost fill, reconstruction + HLL on every face
+ * (Interpolation::comLeftPhase/comRightPhase, Interpolation.h:14-15;
+ * RiemmanSolver::Solver, RiemmanSolver.h:12), Explicit::advance of every fluid
+ * cell (Explicit.h:10) with time step dt, physical-boundary ghost refresh
+ * (Boundary::EnforceBoundary, Boundary.h:11). */
+int cfs_stage(cfs_ctx* ctx, int counter, double dt);
+
+/* One full RK step (2 or 3 cfs_stage calls) with time step dt. */
+int cfs_step(cfs_ctx* ctx, double dt);
+
+/* nsteps full RK steps, the stage launches replayed from a CUDA graph.
+ * cfl > 0: dt of every step comes from the CFL reduction of the step's
+ * initial state, computed on the device inside the previous step's last stage
+ * (no host round trip); cfl <= 0: fixed dt.  *t_elapsed (optional) receives
+ * the simulated time advanced, *dt_last the last dt. */
+int cfs_advance(cfs_ctx* ctx, int nsteps, double cfl, double dt, double* t_elapsed, double* dt_last);
+
+/* Waits for the context's stream. */
+int cfs_synchronize(cfs_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work (events, copies, collectives) against the engine's. */
+void* cfs_get_stream(cfs_ctx* ctx);
+
+/* Sums over fluid cells of rho, rho u, rho v and E times the cell area,
+ * accumulated in FP64 (conservation check). */
+int cfs_conserved_totals(cfs_ctx* ctx, double totals[4]);
+
+/* Unit-level entry points (device batch, host buffers), mirroring one plugin
+ * call each, for parity tests:
+ * cfs_weno5_faces: Weno5th::comLeftPhase + comRightPhase (Weno5th.cpp:57-81) on
+ *   n six-cell stencils st[n][6][4] -> left[n][5], right[n][5] = (rho, mx, my, E, p).
+ * cfs_hll_faces: EulerMod::comFlux + RiemmanSolverHLL::Solver
+ *   (CellInterface.cpp:68-89) on n face states L[n][4], R[n][4] -> F[n][4].
+ * Both use the context's precision, hll variant, gamma and eps. */
+int cfs_weno5_faces(cfs_ctx* ctx, int n, const double* st, double* left, double* right);
+int cfs_hll_faces(cfs_ctx* ctx, int n, int dir, const double* L, const double* R, double* F);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFS_H */

@@ -1,0 +1,213 @@
+"""GPU parity of the stage engine, through the C ABI (ctypes binding), against
+the reference's own outputs (golden fixtures) and the C oracle.
+
+Tolerances:
+  * CFS_FP64_EXACT: bit-identical (reference operation order, no FMA).
+  * CFS_FP64: relative L-infinity <= 1e-12 per RK step, each step started from
+    the same state on both sides (relative = max|diff| / max|U| per variable).
+  * CFS_FP32_MIXED: density L1 error <= 1e-5 against the FP64 path at t_end,
+    conservation drift <= 1e-6 relative.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle_bind as ob
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+MACH3 = (1.4, 3.0, 0.0, 1.0)
+
+
+def _load(name):
+    return dict(np.load(GOLD / f"{name}.npz"))
+
+
+def _rel_linf(a, b):
+    out = 0.0
+    for v in range(4):
+        scale = max(np.abs(b[v]).max(), 1e-300)
+        out = max(out, np.abs(a[v] - b[v]).max() / scale)
+    return out
+
+
+def run_counters(s, first, count, cfl=0.0, dt=0.0, stages_per_step=3):
+    """Drives the engine like Run::solver's loop: counters first..first+count-1,
+    CFL dt recomputed at each step's first stage."""
+    dts = []
+    for k in range(first, first + count):
+        is_start = (k % stages_per_step) == 1 if stages_per_step == 3 else (k % 2) == 1
+        if cfl > 0 and is_start:
+            dt = s.compute_dt(cfl)
+        dts.append(dt)
+        s.stage(k, dt)
+    return np.array(dts)
+
+
+# ---------------------------------------------------------------- unit level
+def test_weno_and_hll_exact_are_bitwise_the_reference(cfsb):
+    g = _load("faces_weno_hll")
+    with cfsb.Solver(8, 8, precision=cfsb.FP64_EXACT) as s:
+        left, right = s.weno5_faces(g["stencils"])
+        assert np.array_equal(left, g["left"])
+        assert np.array_equal(right, g["right"])
+        for d in range(2):
+            assert np.array_equal(s.hll_faces(d, g["L"], g["R"]), g["F"][d])
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 2e-5), (0, 1e-13)])
+def test_weno_and_hll_fast_forms(cfsb, prec, tol):
+    g = _load("faces_weno_hll")
+    with cfsb.Solver(8, 8, precision=prec) as s:
+        left, right = s.weno5_faces(g["stencils"])
+        scale = np.abs(g["left"]).max(axis=0)
+        assert np.all(np.abs(left - g["left"]) <= tol * scale * 10)
+        assert np.all(np.abs(right - g["right"]) <= tol * scale * 10)
+        for d in range(2):
+            F = s.hll_faces(d, g["L"], g["R"])
+            ok = np.isfinite(g["F"][d])
+            fs = np.abs(g["F"][d][ok]).max()
+            assert np.all(np.abs(F[ok] - g["F"][d][ok]) <= tol * fs * 10)
+
+
+# ------------------------------------------------------ stage, exact form
+@pytest.mark.parametrize("name", ["quadrants_tvd3_48x40_cfl", "quadrants_tvd2_32x32_cfl",
+                                  "quadrants_dirichlet_tvd3_40x32"])
+def test_exact_stage_reproduces_reference_fixture(cfsb, name):
+    g = _load(name)
+    nx, ny, nst = int(g["cfg_nx"]), int(g["cfg_ny"]), int(g["cfg_nstages"])
+    integ = int(g["cfg_integrator"])
+    bc = tuple(int(b) for b in g.get("cfg_bc", np.zeros(4)))
+    bc_prim = g["cfg_bc_prim"] if "cfg_bc_prim" in g else None
+    rk = cfsb.RK_TVD2 if integ == 2 else cfsb.RK_TVD3_REFERENCE
+    with cfsb.Solver(nx, ny, precision=cfsb.FP64_EXACT, rk=rk, bc=bc, bc_prim=bc_prim, keep_rhs=True) as s:
+        s.set_state(g["U0"])
+        dts = run_counters(s, 1, nst, cfl=float(g.get("cfg_cfl", 0.0)), dt=float(g.get("cfg_dt", 1e-3)),
+                           stages_per_step=2 if integ == 2 else 3)
+        assert np.array_equal(dts, g["dt"])
+        assert np.array_equal(s.get_state(), g["U"])
+        assert np.array_equal(s.get_rhs(), g["rhs"])
+
+
+def test_exact_stage_with_immersed_circle_reproduces_reference_fixture(cfsb):
+    g = _load("circle_tvd3_64x64")
+    lst = _load("circle_64x64_lists")
+    with cfsb.Solver(64, 64, precision=cfsb.FP64_EXACT, bc=(1, 0, 0, 0), bc_prim=[MACH3] * 4) as s:
+        s.build_circle(0.2, 0.45, 0.55, 400, cfsb.IB_REFERENCE)
+        types, cells, donors, images = s.get_ib()
+        assert np.array_equal(types, lst["types"]) and np.array_equal(cells, lst["cells"])
+        assert np.array_equal(donors, lst["donors"]) and np.array_equal(images, lst["images"])
+        s.set_state(g["U0"])
+        run_counters(s, 1, int(g["cfg_nstages"]), dt=float(g["cfg_dt"]))
+        assert np.array_equal(s.get_state(), g["U"], equal_nan=True)
+
+
+def test_exact_long_run_matches_oracle(cfsb, workloads):
+    """Quadrant Riemann state, 128^2, TVD3 as written, CFL 0.5, 60 steps."""
+    nx = ny = 128
+    w = workloads.riemann_quadrants(nx, ny, seed=1)
+    with cfsb.Solver(nx, ny, precision=cfsb.FP64_EXACT) as s:
+        s.set_state(w.U0)
+        dts = run_counters(s, 1, 180, cfl=0.5)
+        got = s.get_state()
+    ref, ref_dt = ob.orc_run(ob.make_orc_config(nx, ny), w.U0, 1, 180, cfl=0.5)
+    assert np.array_equal(dts, ref_dt)
+    assert np.array_equal(got, ref, equal_nan=True)
+
+
+def test_exact_graph_advance_equals_stepwise(cfsb, workloads):
+    nx, ny = 96, 80
+    w = workloads.riemann_quadrants(nx, ny, seed=7)
+    with cfsb.Solver(nx, ny, precision=cfsb.FP64_EXACT) as s:
+        s.set_state(w.U0)
+        dts = run_counters(s, 1, 21, cfl=0.5)
+        stepwise = s.get_state()
+        s.set_state(w.U0)
+        t, dt_last = s.advance(7, cfl=0.5)
+        graph = s.get_state()
+    assert np.array_equal(graph, stepwise)
+    assert dt_last == dts[-1]
+    assert t == pytest.approx(dts[::3].sum(), rel=1e-15)
+
+
+def test_cfl_dt_is_bitwise_the_oracle(cfsb, workloads):
+    nx, ny = 200, 120
+    w = workloads.riemann_quadrants(nx, ny, seed=9)
+    for prec in (cfsb.FP64_EXACT, cfsb.FP64):
+        with cfsb.Solver(nx, ny, precision=prec) as s:
+            s.set_state(w.U0)
+            assert s.compute_dt(0.37) == ob.orc_cfl_dt(ob.make_orc_config(nx, ny), w.U0, 0.37)
+
+
+# ------------------------------------------------------- stage, FP64 form
+@pytest.mark.parametrize("rk,hll,bc", [
+    (1, 0, (0, 0, 0, 0)),          # reference TVD3 + reference HLL, Neumann
+    (0, 0, (1, 0, 0, 0)),          # reference TVD2, Dirichlet inflow
+    (2, 1, (2, 2, 2, 2)),          # SSP-RK3, Davis HLL, periodic
+    (2, 1, (2, 2, 0, 1)),          # periodic x, Neumann/Dirichlet y
+])
+def test_fp64_per_step_relative_linf(cfsb, workloads, rk, hll, bc):
+    nx, ny = 96, 72
+    w = workloads.riemann_quadrants(nx, ny, seed=3)
+    cfg = ob.make_orc_config(nx, ny, rk=rk, hll=hll, bc=bc, bc_prim=[MACH3] * 4)
+    S = 2 if rk == 0 else 3
+    U = w.U0.copy()
+    worst = 0.0
+    with cfsb.Solver(nx, ny, precision=cfsb.FP64, rk=rk, hll=hll, bc=bc, bc_prim=[MACH3] * 4) as s:
+        for step in range(12):
+            dt = ob.orc_cfl_dt(cfg, U, 0.45)
+            s.set_state(U)
+            s.step(dt)
+            got = s.get_state()
+            ref, _ = ob.orc_run(cfg, U, 1, S, dt=dt)
+            if not np.all(np.isfinite(ref)):
+                break
+            worst = max(worst, _rel_linf(got, ref))
+            U = ref
+    assert worst <= 1e-12, worst
+
+
+def test_fp64_full_quadrant_run_tracks_oracle(cfsb, workloads):
+    """256^2 quadrant configuration, 200 steps at CFL 0.5: the FP64 form stays
+    within 1e-9 relative of the oracle over the whole run (per-step error 1e-15
+    amplified by the shocks)."""
+    nx = ny = 256
+    w = workloads.riemann_quadrants(nx, ny, seed=1)
+    with cfsb.Solver(nx, ny, precision=cfsb.FP64) as s:
+        s.set_state(w.U0)
+        s.advance(200, cfl=0.5)
+        got = s.get_state()
+    ref, _ = ob.orc_run(ob.make_orc_config(nx, ny), w.U0, 1, 600, cfl=0.5)
+    assert np.all(np.isfinite(got))
+    assert _rel_linf(got, ref) <= 1e-9
+
+
+# -------------------------------------------------- FP32-mixed form
+def test_fp32_mixed_error_and_conservation(cfsb, workloads):
+    """Smooth periodic advection, 128^2 to t = 0.5 with a fixed dt: density L1
+    error against the FP64 path <= 1e-5, mass/energy drift <= 1e-6 relative."""
+    n = 128
+    w = workloads.smooth_advection(n)
+    kw = dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=(2, 2, 2, 2))
+    cfg = ob.make_orc_config(n, n, rk=2, hll=1, bc=(2, 2, 2, 2))
+    dt0 = ob.orc_cfl_dt(cfg, w.U0, 0.4)
+    nsteps = int(np.ceil(0.5 / dt0))
+    dt = 0.5 / nsteps
+    out = {}
+    for prec in (cfsb.FP64, cfsb.FP32_MIXED):
+        with cfsb.Solver(n, n, precision=prec, **kw) as s:
+            s.set_state(w.U0)
+            m0 = s.totals()
+            s.advance(nsteps, dt=dt)
+            out[prec] = (s.get_state(), m0, s.totals())
+    U64, U32 = out[cfsb.FP64][0], out[cfsb.FP32_MIXED][0]
+    l1 = np.abs(U32[0] - U64[0]).mean()
+    assert l1 <= 1e-5, l1
+    _, m0, m1 = out[cfsb.FP32_MIXED]
+    assert abs(m1[0] - m0[0]) / abs(m0[0]) <= 1e-6
+    assert abs(m1[3] - m0[3]) / abs(m0[3]) <= 1e-6
+    # and the FP64 path converges to the exact solution
+    exact = workloads.smooth_advection_exact(n, 0.5)
+    assert np.abs(U64[0] - exact).mean() < 1e-4
