@@ -376,24 +376,29 @@ static void add_ns_terms(const orc_config* c, const double* U, double* rhs) {
     for (int i = -W; i < nx + W; ++i)
         for (int j = -W; j < ny + W; ++j) {
             double u, v, T;
-            /* Corner positions are only read through gradients at distance <= 1
-             * from the grid, so the ghost rule applied per axis is enough. */
+            /* corner ghosts take the x-side rule first, then the y-side rule */
             prim(c, U, i, j, &u, &v, &T);
             PI(0, i, j) = u;
             PI(1, i, j) = v;
             PI(2, i, j) = T;
         }
+    /* d/dy at cells i = -2 .. nx+1 (x-face cross derivatives reach two cells
+     * past the grid along x), d/dx at j = -2 .. ny+1 likewise. */
 #pragma omp parallel for num_threads(c->nthreads > 0 ? c->nthreads : omp_get_max_threads())
-    for (int i = -1; i < nx + 1; ++i)
-        for (int j = -1; j < ny + 1; ++j)
+    for (int i = -2; i < nx + 2; ++i)
+        for (int j = 0; j < ny; ++j)
             for (int q = 0; q < 3; ++q) {
-                double sx = 0.0, sy = 0.0;
-                for (int m = 0; m < 5; ++m) {
-                    sx += THETA_C[m] * PI(q, i - 2 + m, j);
-                    sy += THETA_C[m] * PI(q, i, j - 2 + m);
-                }
-                GXI(q, i, j) = sx / dx;
+                double sy = 0.0;
+                for (int m = 0; m < 5; ++m) sy += THETA_C[m] * PI(q, i, j - 2 + m);
                 GYI(q, i, j) = sy / dy;
+            }
+#pragma omp parallel for num_threads(c->nthreads > 0 ? c->nthreads : omp_get_max_threads())
+    for (int i = 0; i < nx; ++i)
+        for (int j = -2; j < ny + 2; ++j)
+            for (int q = 0; q < 3; ++q) {
+                double sx = 0.0;
+                for (int m = 0; m < 5; ++m) sx += THETA_C[m] * PI(q, i - 2 + m, j);
+                GXI(q, i, j) = sx / dx;
             }
 #pragma omp parallel for num_threads(c->nthreads > 0 ? c->nthreads : omp_get_max_threads())
     for (int i = 0; i < nx; ++i)
