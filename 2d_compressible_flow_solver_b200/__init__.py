@@ -99,6 +99,9 @@ _SIGNATURES = {
     "cfs_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "cfs_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "cfs_conserved_totals": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "cfs_compute_dt_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_void_p, _c_double_p]),
     "cfs_weno5_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "cfs_hll_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p,
                                      _c_double_p]),

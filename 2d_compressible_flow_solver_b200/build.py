@@ -28,6 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = {
     "kernels_exact.cu": ["-fmad=false"],
     "kernels_fast.cu": [],
+    "cfl_static.cu": ["-fmad=false"],
 }
 CPP_SOURCES = ["cfs_api.cpp", "ib_setup.cpp"]
 

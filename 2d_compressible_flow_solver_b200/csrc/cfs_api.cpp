@@ -256,6 +256,9 @@ int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* d
 }  // namespace
 
 namespace cfs {
+// Error message of a context-free entry point, read by cfs_last_error(NULL).
+void record_global_error(const std::string& msg) { g_create_error = msg; }
+
 cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s) {
     if (p == kF64Exact) return launch_stage_exact(a, s);
     if (p == kF32Mixed) return launch_stage_f32(a, s);

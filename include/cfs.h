@@ -187,6 +187,22 @@ void* cfs_get_stream(cfs_ctx* ctx);
  * accumulated in FP64 (conservation check). */
 int cfs_conserved_totals(cfs_ctx* ctx, double totals[4]);
 
+/* CFL step of a caller-owned device state, for callers that cannot allocate
+ * device memory (no counterpart in the reference).  Same dt, bit for bit, as
+ * cfs_compute_dt on the same state; needs no context and calls no cudaMalloc,
+ * cudaFree or allocating library routine.  U: device array U[4][nx][ny]
+ * (reference order, FP64); types: device uint8 [nx][ny] (0 = fluid) or NULL
+ * for all fluid; stream: a cudaStream_t or NULL; *dt: host output.  Runs on the
+ * current device and waits for its stream before returning.
+ * Scratch is a fixed static device array, so nx*ny is limited to 16,777,216
+ * cells (4096 x 4096); larger grids are refused with CFS_ERR_INVALID.  The first
+ * call on a device looks up that array's device address (cudaGetSymbolAddress),
+ * so make the first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller.  Errors: cfs_last_error(NULL). */
+int cfs_compute_dt_static(const double* U, const uint8_t* types, int nx, int ny, double lx, double ly,
+                          double gamma, double cfl, void* stream, double* dt);
+
 /* Unit-level entry points (device batch, host buffers), mirroring one plugin
  * call each, for parity tests:
  * cfs_weno5_faces: Weno5th::comLeftPhase + comRightPhase (Weno5th.cpp:57-81) on

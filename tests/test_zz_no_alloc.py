@@ -1,0 +1,67 @@
+"""cfs_compute_dt_static: the CFL step for callers that cannot allocate device
+memory (a host code that owns all device memory through its own pool, or code
+that must not allocate inside its time loop).  It takes a device state the
+caller owns and must give the same dt, bit for bit, as the context-based
+cfs_compute_dt on the same state -- on two calls in a row, since every call
+reuses the same static scratch array.
+
+This file is collected last on purpose; it runs alone in a fresh process or
+after every other test."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _static_dt(cfsb, U_dev, types_dev, nx, ny, lx, ly, cfl, stream=None):
+    lib = cfsb.load_library()
+    dt = ctypes.c_double(0.0)
+    rc = lib.cfs_compute_dt_static(ctypes.c_void_p(U_dev), ctypes.c_void_p(types_dev), nx, ny, lx, ly, 1.4, cfl,
+                                   ctypes.c_void_p(stream), ctypes.byref(dt))
+    if rc != 0:
+        raise cfsb.CfsError(rc, lib.cfs_last_error(None).decode())
+    return dt.value
+
+
+def test_static_dt_matches_context_dt_twice(cfsb, workloads):
+    import torch
+
+    nx, ny = 300, 217
+    w = workloads.riemann_quadrants(nx, ny, seed=12)
+    with cfsb.Solver(nx, ny) as s:
+        s.set_state(w.U0)
+        ref = s.compute_dt(0.5)
+    U_dev = torch.tensor(w.U0, dtype=torch.float64, device="cuda:0").contiguous()
+    torch.cuda.synchronize()
+    first = _static_dt(cfsb, U_dev.data_ptr(), 0, nx, ny, 1.0, 1.0, 0.5)
+    second = _static_dt(cfsb, U_dev.data_ptr(), 0, nx, ny, 1.0, 1.0, 0.5)
+    assert first == ref and second == ref
+
+
+def test_static_dt_with_immersed_cells_and_a_stream(cfsb, workloads):
+    import torch
+
+    w = workloads.mach3_cylinder(256, 128)
+    types, *_ = cfsb.circle_setup(256, 128, 2.0, 1.0, *w.circle, 400)
+    U = w.U0.copy()
+    U[:, types != 0] = 0.0  # solid cells hold zeros as in the reference (Run.cpp:98-104)
+    with cfsb.Solver(256, 128, 2.0, 1.0, bc=w.bc, bc_prim=w.bc_prim) as s:
+        s.build_circle(*w.circle, 400)
+        s.set_state(U)
+        ref = s.compute_dt(0.5)
+    U_dev = torch.tensor(U, dtype=torch.float64, device="cuda:0").contiguous()
+    t_dev = torch.tensor(types, dtype=torch.uint8, device="cuda:0").contiguous()
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got = _static_dt(cfsb, U_dev.data_ptr(), t_dev.data_ptr(), 256, 128, 2.0, 1.0, 0.5, stream.cuda_stream)
+        assert got == ref
+
+
+def test_static_dt_refuses_grids_beyond_its_scratch(cfsb):
+    with pytest.raises(cfsb.CfsError) as e:
+        # the size check comes before any device work, so no state is needed
+        _static_dt(cfsb, 1 << 20, 0, 4097, 4096, 1.0, 1.0, 0.5)
+    assert e.value.code == 1 and "static scratch limit" in str(e.value)
