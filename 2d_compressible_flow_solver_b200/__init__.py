@@ -20,9 +20,9 @@ from pathlib import Path
 import numpy as np
 
 __all__ = [
-    "LIB_PATH", "CfsConfig", "CfsError", "Solver", "load_library", "exported_symbols", "circle_setup",
+    "LIB_PATH", "CfsConfig", "CfsCase", "CfsError", "Solver", "Batch", "load_library", "exported_symbols", "circle_setup",
     "FP64", "FP32_MIXED", "FP64_EXACT", "RK_TVD2", "RK_TVD3_REFERENCE", "RK_SSP3",
-    "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC",
+    "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
     "VISCOUS_OFF", "VISCOUS_NS",
 ]
@@ -34,7 +34,7 @@ HEADER_PATH = _HERE.parent / "include" / "cfs.h"
 FP64, FP32_MIXED, FP64_EXACT = 0, 1, 2
 RK_TVD2, RK_TVD3_REFERENCE, RK_SSP3 = 0, 1, 2
 HLL_REFERENCE, HLL_DAVIS = 0, 1
-BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC = 0, 1, 2
+BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC, BC_HALO = 0, 1, 2, 3
 CELL_FLUID, CELL_SOLID, CELL_IMMERSED_GHOST = 0, 1, 2
 IB_REFERENCE, IB_BILINEAR_SLIP = 0, 1
 VISCOUS_OFF, VISCOUS_NS = 0, 1
@@ -55,7 +55,18 @@ class CfsConfig(ctypes.Structure):
         ("bc", ctypes.c_int * 4), ("bc_prim", (ctypes.c_double * 4) * 4),
         ("viscous", ctypes.c_int),
         ("mu", ctypes.c_double), ("prandtl", ctypes.c_double), ("mach", ctypes.c_double),
-        ("keep_rhs", ctypes.c_int), ("device", ctypes.c_int),
+        ("keep_rhs", ctypes.c_int), ("device", ctypes.c_int), ("variant", ctypes.c_int),
+    ]
+
+
+class CfsCase(ctypes.Structure):
+    """Mirror of ``struct cfs_case`` (include/cfs.h)."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+        ("bc", ctypes.c_int * 4), ("bc_prim", (ctypes.c_double * 4) * 4),
+        ("circle", ctypes.c_int), ("radius", ctypes.c_double), ("cx", ctypes.c_double), ("cy", ctypes.c_double),
+        ("npoints", ctypes.c_int), ("ib_mode", ctypes.c_int), ("rows", ctypes.c_int),
     ]
 
 
@@ -72,6 +83,9 @@ _lib = None
 # name -> (restype, argtypes), one entry per declaration of include/cfs.h
 _SIGNATURES = {
     "cfs_abi_version": (ctypes.c_int, []),
+    "cfs_variant_count": (ctypes.c_int, []),
+    "cfs_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]),
     "cfs_config_default": (None, [ctypes.POINTER(CfsConfig)]),
     "cfs_create": (ctypes.c_int, [ctypes.POINTER(CfsConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "cfs_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -98,10 +112,23 @@ _SIGNATURES = {
                                    _c_double_p, _c_double_p]),
     "cfs_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "cfs_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "cfs_halo_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "cfs_halo_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "cfs_halo_unpack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_conserved_totals": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_compute_dt_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_void_p, _c_double_p]),
+    "cfs_batch_create": (ctypes.c_int, [ctypes.POINTER(CfsConfig), ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "cfs_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cfs_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cfs_batch_set_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
+    "cfs_batch_get_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
+    "cfs_batch_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         _c_double_p]),
+    "cfs_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ctypes.c_int)]),
     "cfs_weno5_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "cfs_hll_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p,
                                      _c_double_p]),
@@ -124,6 +151,17 @@ def load_library() -> ctypes.CDLL:
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+def variants() -> list[tuple[int, int, int]]:
+    """(rows, warps, min_blocks) of every stage-kernel variant, index v-1."""
+    lib = load_library()
+    out = []
+    for v in range(1, lib.cfs_variant_count() + 1):
+        r, w, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib.cfs_variant_info(v, ctypes.byref(r), ctypes.byref(w), ctypes.byref(b))
+        out.append((r.value, w.value, b.value))
+    return out
 
 
 def exported_symbols() -> list[str]:
@@ -163,7 +201,8 @@ class Solver:
     def __init__(self, nx: int, ny: int, lx: float = 1.0, ly: float = 1.0, *, precision: int = FP64,
                  rk: int = RK_TVD3_REFERENCE, hll: int = HLL_REFERENCE, bc=(BC_NEUMANN,) * 4, bc_prim=None,
                  gamma: float = 1.4, weno_eps: float = 1e-2, viscous: int = VISCOUS_OFF, mu: float = 1e-3,
-                 prandtl: float = 0.72, mach: float = 1.0, keep_rhs: bool = False, device: int = 0):
+                 prandtl: float = 0.72, mach: float = 1.0, keep_rhs: bool = False, device: int = 0,
+                 variant: int = 0):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
@@ -176,7 +215,7 @@ class Solver:
                 for q in range(4):
                     cfg.bc_prim[s][q] = float(bc_prim[s][q])
         cfg.viscous, cfg.mu, cfg.prandtl, cfg.mach = int(viscous), float(mu), float(prandtl), float(mach)
-        cfg.keep_rhs, cfg.device = int(bool(keep_rhs)), int(device)
+        cfg.keep_rhs, cfg.device, cfg.variant = int(bool(keep_rhs)), int(device), int(variant)
         self.config = cfg
         self.nx, self.ny = int(nx), int(ny)
         self._ctx = ctypes.c_void_p()
@@ -291,6 +330,17 @@ class Solver:
         """The context's cudaStream_t as an integer handle."""
         return int(self._lib.cfs_get_stream(self._ctx) or 0)
 
+    def halo_bytes(self) -> int:
+        n = ctypes.c_longlong(0)
+        self._check(self._lib.cfs_halo_bytes(self._ctx, ctypes.byref(n)))
+        return n.value
+
+    def halo_pack(self, side: int, dev_ptr: int) -> None:
+        self._check(self._lib.cfs_halo_pack(self._ctx, int(side), ctypes.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, side: int, dev_ptr: int) -> None:
+        self._check(self._lib.cfs_halo_unpack(self._ctx, int(side), ctypes.c_void_p(dev_ptr)))
+
     def totals(self) -> np.ndarray:
         out = np.zeros(4, dtype=np.float64)
         self._check(self._lib.cfs_conserved_totals(self._ctx, _dp(out)))
@@ -312,3 +362,86 @@ class Solver:
         F = np.empty_like(L)
         self._check(self._lib.cfs_hll_faces(self._ctx, L.shape[0], int(direction), _dp(L), _dp(R), _dp(F)))
         return F
+
+
+class Batch:
+    """Many independent grids advanced together (a ``cfs_batch``): one
+    persistent launch per stage for all cases, per-case CFL dt on the device."""
+
+    def __init__(self, cases, *, precision: int = FP32_MIXED, rk: int = RK_SSP3, hll: int = HLL_DAVIS,
+                 gamma: float = 1.4, weno_eps: float = 1e-2, device: int = 0):
+        self._lib = load_library()
+        cfg = CfsConfig()
+        self._lib.cfs_config_default(ctypes.byref(cfg))
+        cfg.precision, cfg.rk, cfg.hll, cfg.gamma, cfg.weno_eps, cfg.device = (
+            int(precision), int(rk), int(hll), float(gamma), float(weno_eps), int(device))
+        arr = (CfsCase * len(cases))()
+        self.shapes = []
+        for k, c in enumerate(cases):
+            d = arr[k]
+            d.nx, d.ny, d.lx, d.ly = int(c["nx"]), int(c["ny"]), float(c.get("lx", 1.0)), float(c.get("ly", 1.0))
+            for s in range(4):
+                d.bc[s] = int(c.get("bc", (BC_NEUMANN,) * 4)[s])
+                prim = c.get("bc_prim", [[1.0, 0.0, 0.0, 1.0]] * 4)[s]
+                for q in range(4):
+                    d.bc_prim[s][q] = float(prim[q])
+            circle = c.get("circle")
+            if circle is not None:
+                d.circle = 1
+                d.radius, d.cx, d.cy = (float(x) for x in circle)
+                d.npoints = int(c.get("npoints", 400))
+                d.ib_mode = int(c.get("ib_mode", IB_BILINEAR_SLIP))
+            d.rows = int(c.get("rows", 0))
+            self.shapes.append((d.nx, d.ny))
+        self._b = ctypes.c_void_p()
+        rc = self._lib.cfs_batch_create(ctypes.byref(cfg), len(cases), ctypes.cast(arr, ctypes.c_void_p),
+                                        ctypes.byref(self._b))
+        if rc != 0:
+            raise CfsError(rc, self._lib.cfs_batch_last_error(None).decode())
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise CfsError(rc, self._lib.cfs_batch_last_error(self._b).decode())
+
+    def close(self) -> None:
+        if self._b:
+            self._lib.cfs_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        cells = ctypes.c_longlong(0)
+        items = ctypes.c_int(0)
+        self._check(self._lib.cfs_batch_info(self._b, ctypes.byref(cells), ctypes.byref(items)))
+        return cells.value, items.value
+
+    def set_state(self, case: int, U) -> None:
+        nx, ny = self.shapes[case]
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (4, nx, ny):
+            raise ValueError(f"case {case}: state must have shape (4, {nx}, {ny})")
+        self._check(self._lib.cfs_batch_set_state(self._b, int(case), _dp(U)))
+
+    def get_state(self, case: int) -> np.ndarray:
+        nx, ny = self.shapes[case]
+        out = np.empty((4, nx, ny))
+        self._check(self._lib.cfs_batch_get_state(self._b, int(case), _dp(out)))
+        return out
+
+    def advance(self, nsteps: int, cfl: float = 0.0, dt: float = 0.0) -> np.ndarray:
+        """Runs nsteps RK steps of every case; returns each case's simulated time."""
+        t = np.zeros(len(self.shapes))
+        self._check(self._lib.cfs_batch_advance(self._b, int(nsteps), float(cfl), float(dt), _dp(t)))
+        return t
+

@@ -30,7 +30,7 @@ CU_SOURCES = {
     "kernels_fast.cu": [],
     "cfl_static.cu": ["-fmad=false"],
 }
-CPP_SOURCES = ["cfs_api.cpp", "ib_setup.cpp"]
+CPP_SOURCES = ["cfs_api.cpp", "cfs_batch.cpp", "ib_setup.cpp"]
 
 
 def _headers() -> list[Path]:

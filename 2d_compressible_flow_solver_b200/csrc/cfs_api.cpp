@@ -31,6 +31,7 @@ struct cfs_ctx {
     int next_stage = 0;   // stage the RK sequence expects next
     double* rhs = nullptr;
     double* staging = nullptr;
+    void* rv = nullptr;   // viscous RHS [3][nx][ny] (Navier-Stokes form only)
     uint8_t* types_d = nullptr;
     bool has_types = false;
     std::vector<uint8_t> types_h;
@@ -93,7 +94,8 @@ int validate(const cfs_config* g, std::string& msg) {
     if (g->rk < 0 || g->rk > 2) { msg = "unknown rk variant"; return CFS_ERR_INVALID; }
     if (g->hll < 0 || g->hll > 1) { msg = "unknown hll variant"; return CFS_ERR_INVALID; }
     for (int s = 0; s < 4; ++s)
-        if (g->bc[s] < 0 || g->bc[s] > 2) { msg = "unknown boundary kind on side " + std::to_string(s); return CFS_ERR_INVALID; }
+        if (g->bc[s] < 0 || g->bc[s] > 3) { msg = "unknown boundary kind on side " + std::to_string(s); return CFS_ERR_INVALID; }
+    if (g->bc[2] == CFS_BC_HALO || g->bc[3] == CFS_BC_HALO) { msg = "halo sides are left/right only"; return CFS_ERR_INVALID; }
     if ((g->bc[0] == CFS_BC_PERIODIC) != (g->bc[1] == CFS_BC_PERIODIC) ||
         (g->bc[2] == CFS_BC_PERIODIC) != (g->bc[3] == CFS_BC_PERIODIC)) {
         msg = "periodic sides come in pairs (left/right, bottom/top)";
@@ -105,7 +107,11 @@ int validate(const cfs_config* g, std::string& msg) {
             return CFS_ERR_INVALID;
         }
     if (g->viscous != CFS_VISCOUS_OFF && g->viscous != CFS_VISCOUS_NS) { msg = "unknown viscous mode"; return CFS_ERR_INVALID; }
-    if (g->viscous == CFS_VISCOUS_NS) { msg = "viscous terms are not available in this build"; return CFS_ERR_INVALID; }
+    if (g->variant < 0 || g->variant > cfs::kNumVariants) { msg = "unknown kernel variant"; return CFS_ERR_INVALID; }
+    if (g->viscous == CFS_VISCOUS_NS && (!(g->mu >= 0) || !(g->prandtl > 0) || !(g->mach > 0))) {
+        msg = "viscous terms need mu >= 0, prandtl > 0 and mach > 0";
+        return CFS_ERR_INVALID;
+    }
     return CFS_OK;
 }
 
@@ -124,6 +130,7 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.prandtl = c->cfg.prandtl;
     a.mach = c->cfg.mach;
     a.types = c->has_types ? c->types_d : nullptr;
+    a.variant = c->cfg.variant;
     return a;
 }
 
@@ -166,7 +173,21 @@ Roles roles_for(const cfs_ctx* c, int stage, int cur, int u0_idx, int u1_idx) {
 int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_mode, int parity, bool first,
                   bool last) {
     if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[r.in]), c->stream));
+    if (c->rv) {
+        cfs::ViscArgs va{};
+        va.in = c->S[r.in];
+        va.rv = c->rv;
+        va.L = c->L;
+        va.gamma = c->cfg.gamma;
+        va.dx = c->dx;
+        va.dy = c->dy;
+        va.mu = c->cfg.mu;
+        va.mach2 = c->cfg.mach * c->cfg.mach;
+        va.kT = c->cfg.mu / ((c->cfg.gamma - 1) * va.mach2 * c->cfg.prandtl);
+        CFS_CUDA(c, cfs::launch_viscous(c->prec, va, c->stream));
+    }
     cfs::StageArgs a = base_args(c);
+    a.rv = c->rv;
     a.in = c->S[r.in];
     a.u0 = r.u0 >= 0 ? c->S[r.u0] : nullptr;
     a.u1 = r.u1 >= 0 ? c->S[r.u1] : nullptr;
@@ -198,7 +219,9 @@ int run_stage(cfs_ctx* c, int stage, double dt) {
     return CFS_OK;
 }
 
-// Upload of per-ghost data for the device fill.
+// Upload of per-ghost data for the device fill.  Reference form: the pivoted
+// LDL^T factor of each donor matrix.  Slip form: donors and weights from
+// cfs::slip_donors (the given donors serve as its fallback).
 int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* donor4, const double* image,
               const double* normal) {
     release_graph(c);
@@ -214,37 +237,23 @@ int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* d
     c->ib_donor_h.assign(donor4, donor4 + 4 * static_cast<size_t>(n));
     c->ib_img_h.assign(image, image + 2 * static_cast<size_t>(n));
     if (n == 0) return CFS_OK;
-    std::vector<double> fac(16 * static_cast<size_t>(n), 0.0);
-    std::vector<int> perm(4 * static_cast<size_t>(n), 0);
-    for (int g = 0; g < n; ++g) {
-        double M[4][4];
-        for (int k = 0; k < 4; ++k) {
-            const int d = donor4[4 * g + k];
-            const int i = d / c->cfg.ny, j = d % c->cfg.ny;
-            const double x = (i + 0.5) * c->dx, y = (j + 0.5) * c->dy;  // CartesianMesh.cpp:92
-            M[k][0] = x * y;
-            M[k][1] = x;
-            M[k][2] = y;
-            M[k][3] = 1.0;
-        }
-        if (mode == CFS_IB_REFERENCE) {
-            cfs::ldlt4_lower(M, &fac[16 * g], &perm[4 * g]);
-        } else {
-            double w[4];
-            if (!cfs::bilinear_weights(M, image[2 * g], image[2 * g + 1], w))
-                return fail(c, CFS_ERR_INVALID, "singular donor matrix for immersed-ghost " + std::to_string(g));
-            for (int k = 0; k < 4; ++k) fac[16 * g + k] = w[k];
-            fac[16 * g + 4] = normal[2 * g];
-            fac[16 * g + 5] = normal[2 * g + 1];
-        }
+    std::vector<uint8_t> fluid_all;
+    const uint8_t* types = c->has_types ? c->types_h.data() : nullptr;
+    if (!types) {
+        fluid_all.assign(static_cast<size_t>(c->cfg.nx) * c->cfg.ny, 0);
+        types = fluid_all.data();
     }
+    std::vector<int32_t> dev_donor;
+    std::vector<double> fac;
+    std::vector<int> perm;
+    cfs::ib_factors(mode, types, c->cfg.nx, c->cfg.ny, c->dx, c->dy, n, donor4, image, normal, dev_donor, fac, perm);
     CFS_CUDA(c, cudaMalloc(&c->ib_cell, sizeof(int) * n));
     CFS_CUDA(c, cudaMalloc(&c->ib_donor, sizeof(int) * 4 * n));
     CFS_CUDA(c, cudaMalloc(&c->ib_perm, sizeof(int) * 4 * n));
     CFS_CUDA(c, cudaMalloc(&c->ib_img, sizeof(double) * 2 * n));
     CFS_CUDA(c, cudaMalloc(&c->ib_fac, sizeof(double) * 16 * n));
     CFS_CUDA(c, cudaMemcpy(c->ib_cell, cell, sizeof(int) * n, cudaMemcpyHostToDevice));
-    CFS_CUDA(c, cudaMemcpy(c->ib_donor, donor4, sizeof(int) * 4 * n, cudaMemcpyHostToDevice));
+    CFS_CUDA(c, cudaMemcpy(c->ib_donor, dev_donor.data(), sizeof(int) * 4 * n, cudaMemcpyHostToDevice));
     CFS_CUDA(c, cudaMemcpy(c->ib_perm, perm.data(), sizeof(int) * 4 * n, cudaMemcpyHostToDevice));
     CFS_CUDA(c, cudaMemcpy(c->ib_img, image, sizeof(double) * 2 * n, cudaMemcpyHostToDevice));
     CFS_CUDA(c, cudaMemcpy(c->ib_fac, fac.data(), sizeof(double) * 16 * n, cudaMemcpyHostToDevice));
@@ -264,6 +273,10 @@ cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s) {
     if (p == kF32Mixed) return launch_stage_f32(a, s);
     return launch_stage_f64(a, s);
 }
+cudaError_t launch_viscous(Prec p, const ViscArgs& a, cudaStream_t s) {
+    if (p == kF32Mixed) return launch_viscous_f32(a, s);
+    return launch_viscous_f64(a, s);
+}
 cudaError_t launch_weno_faces(Prec p, int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s) {
     if (p == kF64Exact) return launch_weno_faces_exact(n, st, l, r, g, eps, s);
     if (p == kF32Mixed) return launch_weno_faces_f32(n, st, l, r, g, eps, s);
@@ -280,6 +293,16 @@ cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const doub
 extern "C" {
 
 int cfs_abi_version(void) { return CFS_ABI_VERSION; }
+
+int cfs_variant_count(void) { return cfs::kNumVariants; }
+
+int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks) {
+    if (v < 1 || v > cfs::kNumVariants) return fail(nullptr, CFS_ERR_INVALID, "unknown kernel variant");
+    if (rows) *rows = cfs::kVariants[v - 1].rows;
+    if (warps) *warps = cfs::kVariants[v - 1].warps;
+    if (min_blocks) *min_blocks = cfs::kVariants[v - 1].min_blocks;
+    return CFS_OK;
+}
 
 void cfs_config_default(cfs_config* g) {
     if (!g) return;
@@ -343,6 +366,11 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
     }
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(cfg->nx) * cfg->ny;
     if (cudaMalloc(&c->staging, hb) != cudaSuccess) { c->err = "device allocation of the staging buffer failed"; return bail(CFS_ERR_NOMEM); }
+    if (cfg->viscous == CFS_VISCOUS_NS) {
+        const size_t vb = static_cast<size_t>(3) * cfg->nx * cfg->ny * c->L.elem_bytes;
+        if (cudaMalloc(&c->rv, vb) != cudaSuccess) { c->err = "device allocation of the viscous RHS failed"; return bail(CFS_ERR_NOMEM); }
+        cudaMemsetAsync(c->rv, 0, vb, c->stream);
+    }
     if (cfg->keep_rhs) {
         if (cudaMalloc(&c->rhs, hb) != cudaSuccess) { c->err = "device allocation of the RHS buffer failed"; return bail(CFS_ERR_NOMEM); }
         cudaMemsetAsync(c->rhs, 0, hb, c->stream);
@@ -366,6 +394,7 @@ int cfs_destroy(cfs_ctx* c) {
     for (void* p : c->S) cudaFree(p);
     cudaFree(c->rhs);
     cudaFree(c->staging);
+    cudaFree(c->rv);
     cudaFree(c->types_d);
     cudaFree(c->ib_cell);
     cudaFree(c->ib_donor);
@@ -384,9 +413,23 @@ int cfs_set_state(cfs_ctx* c, const double* U) {
     if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    if (c->L.elem_bytes == 4) {
+        // FP32 storage offsets: the FP32-rounded mean of each variable.
+        const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+        bool changed = false;
+        for (int v = 0; v < kVars; ++v) {
+            double sum = 0.0;
+            for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
+            float off = static_cast<float>(sum / static_cast<double>(n));
+            if (!std::isfinite(off)) off = 0.0f;
+            changed = changed || off != c->L.off[v];
+            c->L.off[v] = off;
+        }
+        if (changed) release_graph(c);
+    }
     CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
     CFS_CUDA(c, cfs::launch_pack(c->L.elem_bytes, c->staging, c->S[0], c->L, c->stream));
-    CFS_CUDA(c, cfs::launch_ghost_fill(c->L.elem_bytes, c->S[0], c->L, c->sides, c->stream));
+    for (int b = 0; b < 3; ++b) CFS_CUDA(c, cfs::launch_ghost_fill(c->L.elem_bytes, c->S[b], c->L, c->sides, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     c->cur = 0;
     c->u0_idx = c->u1_idx = -1;
@@ -610,6 +653,40 @@ int cfs_synchronize(cfs_ctx* c) {
 }
 
 void* cfs_get_stream(cfs_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int cfs_halo_bytes(cfs_ctx* c, long long* bytes) {
+    if (!c || !bytes) return fail(c, CFS_ERR_INVALID, "null argument");
+    *bytes = static_cast<long long>(kVars) * cfs::kGhost * c->L.pitch * c->L.elem_bytes;
+    return CFS_OK;
+}
+
+// Rows are contiguous in the padded layout: one side's 3 rows of a plane are
+// 3 * pitch consecutive elements, so a message is 4 plain copies.
+int cfs_halo_pack(cfs_ctx* c, int side, void* dst) {
+    if (!c || !dst || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo pack arguments");
+    const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
+    const int first = side == 0 ? 0 : c->cfg.nx - cfs::kGhost;
+    for (int v = 0; v < kVars; ++v) {
+        const char* src = static_cast<const char*>(c->S[c->cur]) +
+                          (static_cast<size_t>(v) * c->L.plane + static_cast<size_t>(first + cfs::kGhost) * c->L.pitch) * c->L.elem_bytes;
+        CFS_CUDA(c, cudaMemcpyAsync(static_cast<char*>(dst) + v * cfs::kGhost * row_bytes, src, cfs::kGhost * row_bytes,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return CFS_OK;
+}
+
+int cfs_halo_unpack(cfs_ctx* c, int side, const void* src) {
+    if (!c || !src || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo unpack arguments");
+    const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
+    const int first = side == 0 ? -cfs::kGhost : c->cfg.nx;
+    for (int v = 0; v < kVars; ++v) {
+        char* dst = static_cast<char*>(c->S[c->cur]) +
+                    (static_cast<size_t>(v) * c->L.plane + static_cast<size_t>(first + cfs::kGhost) * c->L.pitch) * c->L.elem_bytes;
+        CFS_CUDA(c, cudaMemcpyAsync(dst, static_cast<const char*>(src) + v * cfs::kGhost * row_bytes, cfs::kGhost * row_bytes,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return CFS_OK;
+}
 
 int cfs_conserved_totals(cfs_ctx* c, double totals[4]) {
     if (!c || !totals) return fail(c, CFS_ERR_INVALID, "null argument");

@@ -1,0 +1,473 @@
+// Batched cases (cfs_batch_*): many independent grids of uneven size in one
+// device arena, every stage of every case in one persistent launch, per-case
+// CFL dt on the device, whole steps replayed from a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "cfs.h"
+#include "cfs_launch.h"
+#include "cfs_layout.h"
+#include "ib_setup.h"
+
+using cfs::kVars;
+
+namespace {
+
+struct BatchCase {
+    cfs_case desc{};
+    cfs::Layout L{};
+    cfs::BcSides sides{};
+    double dx = 0, dy = 0;
+    size_t state_off = 0;   // bytes from the arena start to S0 (S1, S2 follow)
+    long long types_off = -1;
+    int rows = 32, nseg = 0, items_x = 0, items_y = 0;
+    std::vector<uint8_t> types;
+    int ib_n = 0, ib_mode = 0;
+    int ib_first = 0;       // first immersed-ghost index in the flattened lists
+};
+
+}  // namespace
+
+struct cfs_batch {
+    cfs_config common{};
+    cfs::Prec prec = cfs::kF32Mixed;
+    int elem = 4;
+    int n = 0;
+    std::vector<BatchCase> cases;
+    cudaStream_t stream = nullptr;
+    char* arena = nullptr;
+    uint8_t* types_d = nullptr;
+    int total_ig = 0;
+    int* ib_cell = nullptr;
+    int* ib_donor = nullptr;
+    int* ib_perm = nullptr;
+    double* ib_img = nullptr;
+    double* ib_fac = nullptr;
+    int* ig_case = nullptr;
+    int* ig_local = nullptr;
+    cfs::DevParams* P = nullptr;
+    cfs::StageArgs* dargs = nullptr;  // [parity][stage][case]
+    cfs::IbArgs* dib = nullptr;       // [input buffer][case]
+    int total_items = 0;
+    int* item_case = nullptr;
+    int* item_local = nullptr;
+    int* case_rows = nullptr;
+    int* case_items_x = nullptr;
+    unsigned int* counters = nullptr;  // [parity][stage]
+    double* staging = nullptr;
+    int grid = 0;
+    long long total_cells = 0;
+    bool args_dirty = true;
+    cudaGraphExec_t graph2 = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int bfail(cfs_batch* b, int code, const std::string& m);
+
+#define CFSB_CUDA(b, call)                                                                                   \
+    do {                                                                                                     \
+        cudaError_t e_ = (call);                                                                             \
+        if (e_ != cudaSuccess) return bfail((b), CFS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+thread_local std::string g_batch_create_error;
+
+int bfail(cfs_batch* b, int code, const std::string& m) {
+    if (b) b->err = m;
+    else g_batch_create_error = m;
+    return code;
+}
+
+int stages_of(int rk) { return rk == CFS_RK_TVD2 ? 2 : 3; }
+
+void* state_buf(const cfs_batch* b, const BatchCase& c, int k) {
+    return b->arena + c.state_off + static_cast<size_t>(k) * static_cast<size_t>(c.L.plane) * kVars * b->elem;
+}
+
+// Host images of the per-case stage and fill arguments (device copies in
+// dargs / dib); rebuilt when storage offsets change.
+int upload_args(cfs_batch* b) {
+    const int S = stages_of(b->common.rk);
+    std::vector<cfs::StageArgs> args(static_cast<size_t>(2) * 3 * b->n);
+    std::vector<cfs::IbArgs> ibs(static_cast<size_t>(3) * b->n);
+    for (int ci = 0; ci < b->n; ++ci) {
+        const BatchCase& c = b->cases[ci];
+        for (int p = 0; p < 2; ++p)
+            for (int s = 0; s < S; ++s) {
+                cfs::StageArgs a{};
+                a.L = c.L;
+                for (int q = 0; q < 4; ++q) a.bc[q] = c.sides.bc[q];
+                a.gamma = b->common.gamma;
+                a.eps = b->common.weno_eps;
+                a.dx = c.dx;
+                a.dy = c.dy;
+                a.rk = b->common.rk;
+                a.hll = b->common.hll;
+                a.types = c.types_off >= 0 ? b->types_d + c.types_off : nullptr;
+                a.stage = s;
+                // buffer roles of a step that starts in S0 (as cfs_advance)
+                int in = 0, out = 1, u0 = 0, u1 = -1;
+                if (s == 1) {
+                    in = 1;
+                    u1 = 1;
+                    out = b->common.rk == CFS_RK_TVD2 ? 0 : 2;
+                } else if (s == 2) {
+                    in = 2;
+                    u1 = 1;
+                    out = 0;
+                }
+                a.in = state_buf(b, c, in);
+                a.out = state_buf(b, c, out);
+                a.u0 = state_buf(b, c, u0);
+                a.u1 = u1 >= 0 ? state_buf(b, c, u1) : nullptr;
+                a.P = b->P + ci;
+                a.parity = p;
+                a.first_stage = s == 0 ? 1 : 0;
+                a.last_stage = s == S - 1 ? 1 : 0;
+                args[(static_cast<size_t>(p) * 3 + s) * b->n + ci] = a;
+            }
+        for (int k = 0; k < 3; ++k) {
+            cfs::IbArgs ia{};
+            ia.U = state_buf(b, c, k);
+            ia.L = c.L;
+            ia.n = c.ib_n;
+            ia.mode = c.ib_mode;
+            ia.cell = b->ib_cell ? b->ib_cell + c.ib_first : nullptr;
+            ia.donor = b->ib_donor ? b->ib_donor + 4 * static_cast<size_t>(c.ib_first) : nullptr;
+            ia.perm = b->ib_perm ? b->ib_perm + 4 * static_cast<size_t>(c.ib_first) : nullptr;
+            ia.image = b->ib_img ? b->ib_img + 2 * static_cast<size_t>(c.ib_first) : nullptr;
+            ia.fac = b->ib_fac ? b->ib_fac + 16 * static_cast<size_t>(c.ib_first) : nullptr;
+            ibs[static_cast<size_t>(k) * b->n + ci] = ia;
+        }
+    }
+    CFSB_CUDA(b, cudaMemcpy(b->dargs, args.data(), sizeof(cfs::StageArgs) * args.size(), cudaMemcpyHostToDevice));
+    CFSB_CUDA(b, cudaMemcpy(b->dib, ibs.data(), sizeof(cfs::IbArgs) * ibs.size(), cudaMemcpyHostToDevice));
+    if (b->graph2) {
+        cudaGraphExecDestroy(b->graph2);
+        b->graph2 = nullptr;
+    }
+    b->args_dirty = false;
+    return CFS_OK;
+}
+
+int enqueue_batch_step(cfs_batch* b, int parity) {
+    const int S = stages_of(b->common.rk);
+    for (int s = 0; s < S; ++s) {
+        const int slot = parity * 3 + s;
+        const int in = s;  // stage s reads S_s (S0, S1, S2)
+        CFSB_CUDA(b, cudaMemsetAsync(b->counters + slot, 0, sizeof(unsigned int), b->stream));
+        if (b->total_ig > 0)
+            CFSB_CUDA(b, cfs::launch_batch_ib_fill(b->elem, b->dib + static_cast<size_t>(in) * b->n, b->ig_case,
+                                                   b->ig_local, b->total_ig, b->stream));
+        CFSB_CUDA(b, cfs::launch_batch_stage(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->item_case,
+                                             b->item_local, b->case_rows, b->case_items_x, b->total_items,
+                                             b->counters + slot, b->grid, b->stream));
+    }
+    return CFS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cfs_batch_last_error(const cfs_batch* b) { return b ? b->err.c_str() : g_batch_create_error.c_str(); }
+
+int cfs_batch_destroy(cfs_batch* b) {
+    if (!b) return CFS_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph2) cudaGraphExecDestroy(b->graph2);
+    cudaFree(b->arena);
+    cudaFree(b->types_d);
+    cudaFree(b->ib_cell);
+    cudaFree(b->ib_donor);
+    cudaFree(b->ib_perm);
+    cudaFree(b->ib_img);
+    cudaFree(b->ib_fac);
+    cudaFree(b->ig_case);
+    cudaFree(b->ig_local);
+    cudaFree(b->P);
+    cudaFree(b->dargs);
+    cudaFree(b->dib);
+    cudaFree(b->item_case);
+    cudaFree(b->item_local);
+    cudaFree(b->case_rows);
+    cudaFree(b->case_items_x);
+    cudaFree(b->counters);
+    cudaFree(b->staging);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return CFS_OK;
+}
+
+int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases, cfs_batch** out) {
+    if (!out || !common || ncases <= 0 || !cases) return bfail(nullptr, CFS_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    if (common->precision != CFS_FP32_MIXED && common->precision != CFS_FP64)
+        return bfail(nullptr, CFS_ERR_INVALID, "batches run the throughput forms (CFS_FP32_MIXED or CFS_FP64)");
+    if (common->rk < 0 || common->rk > 2 || common->hll < 0 || common->hll > 1 || !(common->gamma > 1) ||
+        !(common->weno_eps > 0))
+        return bfail(nullptr, CFS_ERR_INVALID, "bad common configuration");
+    if (common->viscous != CFS_VISCOUS_OFF) return bfail(nullptr, CFS_ERR_INVALID, "batches are inviscid");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return bfail(nullptr, CFS_ERR_CUDA, "no CUDA device available (the engine has no CPU path)");
+    cfs_batch* b = new (std::nothrow) cfs_batch();
+    if (!b) return bfail(nullptr, CFS_ERR_NOMEM, "host allocation failed");
+    auto bail = [&](int code, const std::string& m) {
+        cfs_batch_destroy(b);
+        return bfail(nullptr, code, m);
+    };
+    b->common = *common;
+    b->prec = common->precision == CFS_FP32_MIXED ? cfs::kF32Mixed : cfs::kF64;
+    b->elem = b->prec == cfs::kF32Mixed ? 4 : 8;
+    b->n = ncases;
+    b->cases.resize(ncases);
+    if (cudaSetDevice(common->device) != cudaSuccess) return bail(CFS_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(CFS_ERR_CUDA, "stream creation failed");
+
+    // --- per-case layout, boundaries, immersed boundary (host)
+    size_t arena = 0, types_bytes = 0, max_cells = 0;
+    std::vector<int32_t> h_cell, h_donor, h_perm, h_igc, h_igl;
+    std::vector<double> h_img, h_fac;
+    for (int ci = 0; ci < ncases; ++ci) {
+        BatchCase& c = b->cases[ci];
+        c.desc = cases[ci];
+        const cfs_case& d = c.desc;
+        if (d.nx < 3 || d.ny < 3 || !(d.lx > 0) || !(d.ly > 0))
+            return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": bad grid");
+        for (int s = 0; s < 4; ++s) {
+            if (d.bc[s] < 0 || d.bc[s] > 2) return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": bad side");
+            c.sides.bc[s] = d.bc[s];
+            const double rho = d.bc_prim[s][0], u = d.bc_prim[s][1], v = d.bc_prim[s][2], p = d.bc_prim[s][3];
+            if (d.bc[s] == CFS_BC_DIRICHLET && !(rho > 0))
+                return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": Dirichlet density must be positive");
+            const double mx = rho * u, my = rho * v;
+            c.sides.U[s][0] = rho;
+            c.sides.U[s][1] = mx;
+            c.sides.U[s][2] = my;
+            c.sides.U[s][3] = d.bc[s] == CFS_BC_DIRICHLET ? p / (common->gamma - 1) + 0.5 * (mx * mx + my * my) / rho : 0.0;
+        }
+        if ((d.bc[0] == CFS_BC_PERIODIC) != (d.bc[1] == CFS_BC_PERIODIC) ||
+            (d.bc[2] == CFS_BC_PERIODIC) != (d.bc[3] == CFS_BC_PERIODIC))
+            return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": periodic sides come in pairs");
+        c.L = cfs::Layout::make(d.nx, d.ny, b->elem);
+        c.dx = d.lx / d.nx;
+        c.dy = d.ly / d.ny;
+        c.rows = d.rows > 0 ? d.rows : cfs::kVariants[(b->prec == cfs::kF32Mixed ? cfs::kDefaultVariantF32
+                                                                                   : cfs::kDefaultVariantF64) - 1].rows;
+        c.nseg = (d.ny + 29) / 30;
+        c.items_x = (c.nseg + cfs::kBatchWarps - 1) / cfs::kBatchWarps;
+        c.items_y = (d.nx + c.rows - 1) / c.rows;
+        c.state_off = arena;
+        arena += static_cast<size_t>(3) * static_cast<size_t>(c.L.bytes());
+        arena = (arena + 255) & ~static_cast<size_t>(255);
+        max_cells = std::max(max_cells, static_cast<size_t>(d.nx) * d.ny);
+        b->total_cells += static_cast<long long>(d.nx) * d.ny;
+        if (d.circle) {
+            cfs::IbList ib;
+            std::string e;
+            if (!cfs::build_circle(d.nx, d.ny, d.lx, d.ly, d.radius, d.cx, d.cy, d.npoints > 0 ? d.npoints : 400, ib, e))
+                return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": " + e);
+            c.types = ib.types;
+            c.types_off = static_cast<long long>(types_bytes);
+            types_bytes += c.types.size();
+            c.ib_n = static_cast<int>(ib.cell.size());
+            c.ib_mode = d.ib_mode;
+            c.ib_first = static_cast<int>(h_cell.size());
+            std::vector<int32_t> dd;
+            std::vector<double> fac;
+            std::vector<int> perm;
+            cfs::ib_factors(d.ib_mode, c.types.data(), d.nx, d.ny, c.dx, c.dy, c.ib_n, ib.donor.data(), ib.image.data(),
+                            ib.normal.data(), dd, fac, perm);
+            h_cell.insert(h_cell.end(), ib.cell.begin(), ib.cell.end());
+            h_donor.insert(h_donor.end(), dd.begin(), dd.end());
+            h_perm.insert(h_perm.end(), perm.begin(), perm.end());
+            h_img.insert(h_img.end(), ib.image.begin(), ib.image.end());
+            h_fac.insert(h_fac.end(), fac.begin(), fac.end());
+            for (int g = 0; g < c.ib_n; ++g) {
+                h_igc.push_back(ci);
+                h_igl.push_back(g);
+            }
+        }
+    }
+    b->total_ig = static_cast<int>(h_cell.size());
+
+    // --- work items, largest cases first
+    std::vector<int> order(ncases);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return static_cast<long long>(b->cases[x].desc.nx) * b->cases[x].desc.ny >
+               static_cast<long long>(b->cases[y].desc.nx) * b->cases[y].desc.ny;
+    });
+    std::vector<int> it_case, it_local, c_rows(ncases), c_ix(ncases);
+    for (int ci : order) {
+        const BatchCase& c = b->cases[ci];
+        for (int li = 0; li < c.items_x * c.items_y; ++li) {
+            it_case.push_back(ci);
+            it_local.push_back(li);
+        }
+    }
+    for (int ci = 0; ci < ncases; ++ci) {
+        c_rows[ci] = b->cases[ci].rows;
+        c_ix[ci] = b->cases[ci].items_x;
+    }
+    b->total_items = static_cast<int>(it_case.size());
+
+    // --- device allocations
+    auto dalloc = [&](void** p, size_t bytes) { return bytes == 0 || cudaMalloc(p, bytes) == cudaSuccess; };
+    if (!dalloc(reinterpret_cast<void**>(&b->arena), arena)) return bail(CFS_ERR_NOMEM, "state arena allocation failed");
+    if (!dalloc(reinterpret_cast<void**>(&b->types_d), types_bytes) ||
+        !dalloc(reinterpret_cast<void**>(&b->ib_cell), sizeof(int) * h_cell.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ib_donor), sizeof(int) * h_donor.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ib_perm), sizeof(int) * h_perm.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ib_img), sizeof(double) * h_img.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ib_fac), sizeof(double) * h_fac.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ig_case), sizeof(int) * h_igc.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->ig_local), sizeof(int) * h_igl.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->P), sizeof(cfs::DevParams) * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->dargs), sizeof(cfs::StageArgs) * 6 * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->dib), sizeof(cfs::IbArgs) * 3 * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->item_case), sizeof(int) * it_case.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->item_local), sizeof(int) * it_local.size()) ||
+        !dalloc(reinterpret_cast<void**>(&b->case_rows), sizeof(int) * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->case_items_x), sizeof(int) * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->counters), sizeof(unsigned int) * 6) ||
+        !dalloc(reinterpret_cast<void**>(&b->staging), sizeof(double) * kVars * max_cells))
+        return bail(CFS_ERR_NOMEM, "batch device allocation failed");
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return bytes == 0 || cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    bool ok = cudaMemset(b->arena, 0, arena) == cudaSuccess;
+    for (const BatchCase& c : b->cases)
+        if (c.types_off >= 0) ok = ok && h2d(b->types_d + c.types_off, c.types.data(), c.types.size());
+    ok = ok && h2d(b->ib_cell, h_cell.data(), sizeof(int) * h_cell.size()) &&
+         h2d(b->ib_donor, h_donor.data(), sizeof(int) * h_donor.size()) &&
+         h2d(b->ib_perm, h_perm.data(), sizeof(int) * h_perm.size()) &&
+         h2d(b->ib_img, h_img.data(), sizeof(double) * h_img.size()) &&
+         h2d(b->ib_fac, h_fac.data(), sizeof(double) * h_fac.size()) &&
+         h2d(b->ig_case, h_igc.data(), sizeof(int) * h_igc.size()) &&
+         h2d(b->ig_local, h_igl.data(), sizeof(int) * h_igl.size()) &&
+         h2d(b->item_case, it_case.data(), sizeof(int) * it_case.size()) &&
+         h2d(b->item_local, it_local.data(), sizeof(int) * it_local.size()) &&
+         h2d(b->case_rows, c_rows.data(), sizeof(int) * ncases) && h2d(b->case_items_x, c_ix.data(), sizeof(int) * ncases) &&
+         cudaMemset(b->P, 0, sizeof(cfs::DevParams) * ncases) == cudaSuccess;
+    if (!ok) return bail(CFS_ERR_CUDA, "batch upload failed");
+    for (int ci = 0; ci < ncases; ++ci)
+        for (int k = 0; k < 3; ++k)
+            if (cfs::launch_ghost_fill(b->elem, state_buf(b, b->cases[ci], k), b->cases[ci].L, b->cases[ci].sides,
+                                       b->stream) != cudaSuccess)
+                return bail(CFS_ERR_CUDA, "ghost fill failed");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, common->device);
+    b->grid = sms * cfs::batch_blocks_per_sm(b->prec);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(CFS_ERR_CUDA, "batch initialisation failed");
+    *out = b;
+    return CFS_OK;
+}
+
+int cfs_batch_info(const cfs_batch* b, long long* cells, int* items) {
+    if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
+    if (cells) *cells = b->total_cells;
+    if (items) *items = b->total_items;
+    return CFS_OK;
+}
+
+int cfs_batch_set_state(cfs_batch* b, int ci, const double* U) {
+    if (!b || !U || ci < 0 || ci >= b->n) return bfail(b, CFS_ERR_INVALID, "bad case or state");
+    BatchCase& c = b->cases[ci];
+    const size_t n = static_cast<size_t>(c.desc.nx) * c.desc.ny;
+    if (b->elem == 4) {
+        for (int v = 0; v < kVars; ++v) {
+            double sum = 0.0;
+            for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
+            float off = static_cast<float>(sum / static_cast<double>(n));
+            if (!std::isfinite(off)) off = 0.0f;
+            if (off != c.L.off[v]) b->args_dirty = true;
+            c.L.off[v] = off;
+        }
+    }
+    CFSB_CUDA(b, cudaMemcpyAsync(b->staging, U, sizeof(double) * kVars * n, cudaMemcpyHostToDevice, b->stream));
+    CFSB_CUDA(b, cfs::launch_pack(b->elem, b->staging, state_buf(b, c, 0), c.L, b->stream));
+    for (int k = 0; k < 3; ++k) CFSB_CUDA(b, cfs::launch_ghost_fill(b->elem, state_buf(b, c, k), c.L, c.sides, b->stream));
+    CFSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    return CFS_OK;
+}
+
+int cfs_batch_get_state(cfs_batch* b, int ci, double* U) {
+    if (!b || !U || ci < 0 || ci >= b->n) return bfail(b, CFS_ERR_INVALID, "bad case or state");
+    const BatchCase& c = b->cases[ci];
+    const size_t n = static_cast<size_t>(c.desc.nx) * c.desc.ny;
+    CFSB_CUDA(b, cfs::launch_unpack(b->elem, state_buf(b, c, 0), b->staging, c.L, b->stream));
+    CFSB_CUDA(b, cudaMemcpyAsync(U, b->staging, sizeof(double) * kVars * n, cudaMemcpyDeviceToHost, b->stream));
+    CFSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    return CFS_OK;
+}
+
+int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t) {
+    if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
+    if (nsteps < 0 || (!(cfl > 0) && !(dt > 0))) return bfail(b, CFS_ERR_INVALID, "give nsteps >= 0 and cfl > 0 or dt > 0");
+    CFSB_CUDA(b, cudaSetDevice(b->common.device));
+    if (b->args_dirty) {
+        const int rc = upload_args(b);
+        if (rc != CFS_OK) return rc;
+    }
+    std::vector<cfs::DevParams> hp(b->n);
+    for (auto& p : hp) {
+        p = cfs::DevParams{};
+        p.use_cfl = cfl > 0 ? 1 : 0;
+        p.cfl = cfl;
+        p.dt_fixed = dt;
+    }
+    CFSB_CUDA(b, cudaMemcpyAsync(b->P, hp.data(), sizeof(cfs::DevParams) * b->n, cudaMemcpyHostToDevice, b->stream));
+    if (cfl > 0) {
+        for (int ci = 0; ci < b->n; ++ci) {
+            const BatchCase& c = b->cases[ci];
+            CFSB_CUDA(b, cfs::launch_wmax(b->elem, state_buf(b, c, 0), c.L,
+                                          c.types_off >= 0 ? b->types_d + c.types_off : nullptr, b->common.gamma, c.dx,
+                                          c.dy, reinterpret_cast<unsigned long long*>(b->P + ci), b->stream));
+        }
+    }
+    if (nsteps >= 2 && !b->graph2) {
+        cudaGraph_t g = nullptr;
+        CFSB_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_batch_step(b, 0);
+        if (rc == CFS_OK) rc = enqueue_batch_step(b, 1);
+        const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+        if (rc != CFS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return bfail(b, CFS_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph2, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            b->graph2 = nullptr;
+            return bfail(b, CFS_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(ei));
+        }
+    }
+    for (int k = 0; k + 1 < nsteps; k += 2) CFSB_CUDA(b, cudaGraphLaunch(b->graph2, b->stream));
+    if (nsteps % 2 == 1) {
+        const int rc = enqueue_batch_step(b, 0);
+        if (rc != CFS_OK) return rc;
+    }
+    CFSB_CUDA(b, cudaMemcpyAsync(hp.data(), b->P, sizeof(cfs::DevParams) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    CFSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    for (int ci = 0; ci < b->n; ++ci) {
+        if (t) t[ci] = hp[ci].t;
+        if (nsteps > 0 && (!(hp[ci].dt_last > 0) || !std::isfinite(hp[ci].dt_last)))
+            return bfail(b, CFS_ERR_NUMERIC, "case " + std::to_string(ci) + ": time step became non-finite or non-positive");
+    }
+    return CFS_OK;
+}
+
+}  // extern "C"

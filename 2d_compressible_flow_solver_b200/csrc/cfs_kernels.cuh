@@ -20,12 +20,31 @@ struct PolF32   { using T = float;  using C = float;  static constexpr bool kExa
 enum { kRkTvd2 = 0, kRkTvd3Ref = 1, kRkSsp3 = 2 };
 enum { kHllReference = 0, kHllDavis = 1 };
 
-template <class C> struct Face5 { C r, mx, my, E, p, a; };
+// Reconstructed face state: conserved variables, pressure, sound speed and
+// (throughput forms) 1/rho.
+template <class C> struct Face5 { C r, mx, my, E, p, a, ri; };
 
 __device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
 __device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrtf(x); }
 __device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
+
+// State storage: FP64 holds the value; FP32 holds value - L.off[v].
+template <class T>
+__device__ __forceinline__ double dec(T stored, const Layout& L, int v) {
+    if constexpr (sizeof(T) == 4) return double(stored) + double(L.off[v]);
+    else return double(stored);
+}
+template <class T, class C>
+__device__ __forceinline__ C decc(T stored, const Layout& L, int v) {
+    if constexpr (sizeof(T) == 4) return C(stored) + C(L.off[v]);
+    else return C(stored);
+}
+template <class T>
+__device__ __forceinline__ T enc(double value, const Layout& L, int v) {
+    if constexpr (sizeof(T) == 4) return T(value - double(L.off[v]));
+    else return T(value);
+}
 
 // std::min / std::max as the reference uses them (RiemmanSolverHLL.cpp:41-42):
 // the first argument is returned unless the second compares smaller (larger),
@@ -102,6 +121,7 @@ __device__ __forceinline__ void finish_state(Face5<typename Pol::C>& s, double g
         s.a = sqrt(g * s.p / s.r);
     } else if constexpr (Pol::kMixed) {
         const C rinv = rcp_fast(s.r);
+        s.ri = rinv;
         const C ke = C(0.5) * (s.mx * s.mx + s.my * s.my) * rinv;
         if (ke > C(0.9) * s.E) {
             const double r = s.r, mx = s.mx, my = s.my, E = s.E;
@@ -114,6 +134,7 @@ __device__ __forceinline__ void finish_state(Face5<typename Pol::C>& s, double g
         }
     } else {
         const C rinv = rcp_fast(s.r);
+        s.ri = rinv;
         s.p = C(g - 1) * (s.E - C(0.5) * (s.mx * s.mx + s.my * s.my) * rinv);
         s.a = sqrt(C(g) * s.p * rinv);
     }
@@ -138,7 +159,7 @@ __device__ __forceinline__ void phys_flux(const Face5<typename Pol::C>& s, int d
         }
     } else {
         const C q = dir == 0 ? s.mx : s.my;
-        const C un = q * rcp_fast(s.r);
+        const C un = q * s.ri;
         F[0] = q;
         F[1] = s.mx * un + (dir == 0 ? s.p : C(0));
         F[2] = s.my * un + (dir == 0 ? C(0) : s.p);
@@ -179,15 +200,15 @@ __device__ __forceinline__ void hll_flux(const Face5<typename Pol::C>& L, const 
             SR = max_ref(uL + aL, uR + aR);
         }
     } else {
-        const C rinvL = rcp_fast(L.r), rinvR = rcp_fast(R.r);
-        const C uL = qL * rinvL, uR = qR * rinvR;
+        const C uL = qL * L.ri, uR = qR * R.ri;
         if (variant == kHllReference) {
             const C a_ave = C(0.5) * (aL + aR);
             const C rho_ave = C(0.5) * (L.r + R.r);
             const C ra = rho_ave * a_ave;
+            const C inv_ra = rcp_fast(ra);
             const C p_star = C(0.5) * (L.p + R.p) - C(0.5) * (uR - uL) * ra;
-            const C u_star = C(0.5) * (uR + uL) - C(0.5) * (R.p - L.p) * rcp_fast(ra);
-            const C ratio = rho_ave * rcp_fast(a_ave);
+            const C u_star = C(0.5) * (uR + uL) - C(0.5) * (R.p - L.p) * inv_ra;
+            const C ratio = rho_ave * rho_ave * inv_ra;
             const C rho_star_L = L.r + (uL - u_star) * ratio;
             const C rho_star_R = R.r - (uR - u_star) * ratio;
             const C gp = C(g) * p_star;
@@ -258,19 +279,34 @@ __device__ __forceinline__ double wave_sum(double rho, double mx, double my, dou
 // Writes one cell of the new state and the ghost copies it feeds: Neumann
 // ghosts copy the adjacent cell into all three layers (NeummanBoundary.cpp:31-45;
 // one ghost repeated three times in the stencil, CellInterface.cpp:147-179),
-// periodic ghosts wrap.  Dirichlet ghosts are constant and set at upload.
+// periodic ghosts wrap, and corner ghosts take both copies (the viscous
+// stencils read them).  Dirichlet ghosts are constant and set at upload.
 template <class T>
-__device__ __forceinline__ void store_cell(T* out, const Layout& L, const int bc[4], int v, int i, int j, T val) {
-    T* p = out + v * L.plane;
-    p[L.offset(i, j)] = val;
-    if (i == 0 && bc[0] == kNeumann) { p[L.offset(-1, j)] = val; p[L.offset(-2, j)] = val; p[L.offset(-3, j)] = val; }
-    if (i == L.nx - 1 && bc[1] == kNeumann) { p[L.offset(L.nx, j)] = val; p[L.offset(L.nx + 1, j)] = val; p[L.offset(L.nx + 2, j)] = val; }
-    if (bc[0] == kPeriodic && i >= L.nx - kGhost) p[L.offset(i - L.nx, j)] = val;
-    if (bc[1] == kPeriodic && i < kGhost) p[L.offset(i + L.nx, j)] = val;
-    if (j == 0 && bc[2] == kNeumann) { p[L.offset(i, -1)] = val; p[L.offset(i, -2)] = val; p[L.offset(i, -3)] = val; }
-    if (j == L.ny - 1 && bc[3] == kNeumann) { p[L.offset(i, L.ny)] = val; p[L.offset(i, L.ny + 1)] = val; p[L.offset(i, L.ny + 2)] = val; }
-    if (bc[2] == kPeriodic && j >= L.ny - kGhost) p[L.offset(i, j - L.ny)] = val;
-    if (bc[3] == kPeriodic && j < kGhost) p[L.offset(i, j + L.ny)] = val;
+__device__ __forceinline__ void store_cell4(T* out, const Layout& L, const int bc[4], int i, int j, const T val[kVars]) {
+    if (i >= kGhost && i < L.nx - kGhost && j >= kGhost && j < L.ny - kGhost) {  // no ghost copies
+        const long long off = L.offset(i, j);
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) out[v * L.plane + off] = val[v];
+        return;
+    }
+    int xi[4], yj[4];
+    int nxi = 1, nyj = 1;
+    xi[0] = i;
+    yj[0] = j;
+    if (bc[0] == kNeumann && i == 0) { xi[nxi++] = -1; xi[nxi++] = -2; xi[nxi++] = -3; }
+    if (bc[1] == kNeumann && i == L.nx - 1) { xi[nxi++] = L.nx; xi[nxi++] = L.nx + 1; xi[nxi++] = L.nx + 2; }
+    if (bc[0] == kPeriodic && i >= L.nx - kGhost) xi[nxi++] = i - L.nx;
+    if (bc[1] == kPeriodic && i < kGhost) xi[nxi++] = i + L.nx;
+    if (bc[2] == kNeumann && j == 0) { yj[nyj++] = -1; yj[nyj++] = -2; yj[nyj++] = -3; }
+    if (bc[3] == kNeumann && j == L.ny - 1) { yj[nyj++] = L.ny; yj[nyj++] = L.ny + 1; yj[nyj++] = L.ny + 2; }
+    if (bc[2] == kPeriodic && j >= L.ny - kGhost) yj[nyj++] = j - L.ny;
+    if (bc[3] == kPeriodic && j < kGhost) yj[nyj++] = j + L.ny;
+    for (int a = 0; a < nxi; ++a)
+        for (int b = 0; b < nyj; ++b) {
+            const long long off = L.offset(xi[a], yj[b]);
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) out[v * L.plane + off] = val[v];
+        }
 }
 
 template <int NT>
@@ -323,7 +359,7 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
         if (ok) {
             const long long off = L.offset(i, j);
 #pragma unroll
-            for (int v = 0; v < kVars; ++v) sU[v][r][c] = C(in[v * L.plane + off]);
+            for (int v = 0; v < kVars; ++v) sU[v][r][c] = decc<T, C>(in[v * L.plane + off], L, v);
         } else {
 #pragma unroll
             for (int v = 0; v < kVars; ++v) sU[v][r][c] = C(0);
@@ -396,6 +432,7 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
         const T* u1 = static_cast<const T*>(a.u1);
         T* out = static_cast<T*>(a.out);
         double nv[kVars];
+        T sv[kVars];
 #pragma unroll
         for (int v = 0; v < kVars; ++v) {
             double rv;
@@ -404,18 +441,20 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
             } else {
                 rv = -double(sFX[v][ti + 1][tj] - sFX[v][ti][tj]) / a.dx - double(sFY[v][ti][tj + 1] - sFY[v][ti][tj]) / a.dy;
             }
+            if (a.rv && v >= 1)
+                rv += double(static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
             const double cur = double(sU[v][ti + kGhost][tj + kGhost]);
             double val = cur;
             if (fluid) {
-                const double u0v = a.stage >= 1 ? double(u0[v * L.plane + off]) : 0.0;
-                const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? double(u1[v * L.plane + off]) : 0.0;
+                const double u0v = a.stage >= 1 ? dec<T>(u0[v * L.plane + off], L, v) : 0.0;
+                const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
                 val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
             }
-            const T stored = T(val);
-            nv[v] = double(stored);
-            store_cell<T>(out, L, a.bc, v, i, j, stored);
+            sv[v] = enc<T>(val, L, v);
+            nv[v] = dec<T>(sv[v], L, v);
             if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
         }
+        store_cell4<T>(out, L, a.bc, i, j, sv);
         if (a.P && a.last_stage && a.P->use_cfl && fluid) {
             const double w = wave_sum(nv[0], nv[1], nv[2], nv[3], a.gamma, a.dx, a.dy);
             if (w > wloc) wloc = w;
@@ -424,6 +463,137 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
     if (a.P && a.last_stage && a.P->use_cfl) {
         const double m = block_max<NT>(wloc, red);
         if (t == 0 && m > 0.0) atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// --------------------------------------------------- viscous (NS) terms
+// No reference counterpart is live: the reference computes a viscous flux but
+// never adds it (Cell.cpp:128-133, Run.cpp:177,188).  Here: u, v and
+// T = gamma Ma^2 p / rho on the tile and its 3-cell halo (corners included);
+// cell-centred 4th-order derivatives with the reference's table theta_c
+// (FourthOrderCS.h:34-36); at each face the normal derivative from theta_r[1]
+// over 6 cells (FourthOrderCS.h:28-32), the cross derivative and u, v
+// interpolated with zeta_r[1] (FourthOrderCS.h:38-42); stresses
+// sigma_11 = mu (4/3 u_x - 2/3 v_y), sigma_12 = mu (u_y + v_x), heat flux
+// kT T_x with kT = mu / ((gamma-1) Ma^2 Pr).
+__constant__ double kThetaR1[6] = {-3.0 / 640, 25.0 / 384, -75.0 / 64, 75.0 / 64, -25.0 / 384, 3.0 / 640};
+__constant__ double kThetaC[5] = {1.0 / 12, -8.0 / 12, 0.0, 8.0 / 12, -1.0 / 12};
+__constant__ double kZeta1[4] = {-1.0 / 16, 9.0 / 16, 9.0 / 16, -1.0 / 16};
+
+template <class Pol, int TI, int TJ>
+__global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
+    using T = typename Pol::T;
+    using C = typename Pol::C;
+    constexpr int NT = TI * TJ;
+    constexpr int HI = TI + 2 * kGhost, HJ = TJ + 2 * kGhost;
+    __shared__ C sP[3][HI][HJ];
+    __shared__ C sGY[3][TI + 4][TJ];
+    __shared__ C sGX[3][TI][TJ + 4];
+    __shared__ C sFV[3][TI + 1][TJ];
+    __shared__ C sGV[3][TI][TJ + 1];
+    const Layout& L = a.L;
+    const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+    const T* in = static_cast<const T*>(a.in);
+    const int t = threadIdx.x;
+    const C g = C(a.gamma), gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
+    for (int e = t; e < HI * HJ; e += NT) {
+        const int r = e / HJ, c = e - r * HJ;
+        const int i = i0 - kGhost + r, j = j0 - kGhost + c;
+        C u = C(0), v = C(0), Tt = C(0);
+        if (i < L.nx + kGhost && j < L.ny + kGhost) {
+            const long long off = L.offset(i, j);
+            const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
+            const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
+            const C rinv = C(1) / rho;
+            u = mx * rinv;
+            v = my * rinv;
+            const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);
+            Tt = cT * p * rinv;
+        }
+        sP[0][r][c] = u;
+        sP[1][r][c] = v;
+        sP[2][r][c] = Tt;
+    }
+    (void)g;
+    __syncthreads();
+    const C idx = C(1.0 / a.dx), idy = C(1.0 / a.dy);
+    for (int e = t; e < 3 * (TI + 4) * TJ; e += NT) {
+        const int q = e / ((TI + 4) * TJ), rem = e - q * (TI + 4) * TJ;
+        const int rr = rem / TJ, c = rem - rr * TJ;
+        C s = C(0);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) s += C(kThetaC[m]) * sP[q][rr + 1][c + 1 + m];
+        sGY[q][rr][c] = s * idy;
+    }
+    for (int e = t; e < 3 * TI * (TJ + 4); e += NT) {
+        const int q = e / (TI * (TJ + 4)), rem = e - q * TI * (TJ + 4);
+        const int r = rem / (TJ + 4), cc = rem - r * (TJ + 4);
+        C s = C(0);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) s += C(kThetaC[m]) * sP[q][r + 1 + m][cc + 1];
+        sGX[q][r][cc] = s * idx;
+    }
+    __syncthreads();
+    const C mu = C(a.mu), kT = C(a.kT), c43 = C(4.0 / 3.0), c23 = C(2.0 / 3.0);
+    for (int f = t; f < (TI + 1) * TJ; f += NT) {  // x-normal faces between rows i0+fi-1 and i0+fi
+        const int fi = f / TJ, fj = f - fi * TJ;
+        C dn[3], cr[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            C s = C(0), x = C(0);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s += C(kThetaR1[k]) * sP[q][fi + k][fj + kGhost];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) x += C(kZeta1[k]) * sGY[q][fi + k][fj];
+            dn[q] = s * idx;
+            cr[q] = x;
+        }
+        C uf = C(0), vf = C(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uf += C(kZeta1[k]) * sP[0][fi + 1 + k][fj + kGhost];
+            vf += C(kZeta1[k]) * sP[1][fi + 1 + k][fj + kGhost];
+        }
+        const C s11 = mu * (c43 * dn[0] - c23 * cr[1]);
+        const C s12 = mu * (cr[0] + dn[1]);
+        sFV[0][fi][fj] = s11;
+        sFV[1][fi][fj] = s12;
+        sFV[2][fi][fj] = uf * s11 + vf * s12 + kT * dn[2];
+    }
+    for (int f = t; f < TI * (TJ + 1); f += NT) {  // y-normal faces between columns j0+fj-1 and j0+fj
+        const int fi = f / (TJ + 1), fj = f - fi * (TJ + 1);
+        C dn[3], cr[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            C s = C(0), x = C(0);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s += C(kThetaR1[k]) * sP[q][fi + kGhost][fj + k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) x += C(kZeta1[k]) * sGX[q][fi][fj + k];
+            dn[q] = s * idy;
+            cr[q] = x;
+        }
+        C uf = C(0), vf = C(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uf += C(kZeta1[k]) * sP[0][fi + kGhost][fj + 1 + k];
+            vf += C(kZeta1[k]) * sP[1][fi + kGhost][fj + 1 + k];
+        }
+        const C s22 = mu * (c43 * dn[1] - c23 * cr[0]);
+        const C s21 = mu * (dn[0] + cr[1]);
+        sGV[0][fi][fj] = s21;
+        sGV[1][fi][fj] = s22;
+        sGV[2][fi][fj] = uf * s21 + vf * s22 + kT * dn[2];
+    }
+    __syncthreads();
+    const int ti = t / TJ, tj = t - (t / TJ) * TJ;
+    const int i = i0 + ti, j = j0 + tj;
+    if (i < L.nx && j < L.ny) {
+        T* rv = static_cast<T*>(a.rv);
+        const long long n = static_cast<long long>(L.nx) * L.ny, k = static_cast<long long>(i) * L.ny + j;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            rv[q * n + k] = T((sFV[q][ti + 1][tj] - sFV[q][ti][tj]) * idx + (sGV[q][ti][tj + 1] - sGV[q][ti][tj]) * idy);
     }
 }
 
@@ -436,9 +606,7 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
 // W0 X Y + W1 X + W2 Y + W3 and both momenta negated.  Mode 1: bilinear
 // weights and reflection of the wall-normal momentum only.  FP64 arithmetic.
 template <class T>
-__global__ void ib_fill_kernel(const IbArgs a) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.n) return;
+__device__ __forceinline__ void ib_fill_one(const IbArgs& a, int g) {
     const Layout& L = a.L;
     T* U = static_cast<T*>(a.U);
     double f[kVars][4];
@@ -448,7 +616,7 @@ __global__ void ib_fill_kernel(const IbArgs a) {
         const int i = d / L.ny, j = d - (d / L.ny) * L.ny;
         const long long off = L.offset(i, j);
 #pragma unroll
-        for (int v = 0; v < kVars; ++v) f[v][k] = double(U[v * L.plane + off]);
+        for (int v = 0; v < kVars; ++v) f[v][k] = dec<T>(U[v * L.plane + off], L, v);
     }
     const double* fac = a.fac + 16 * g;
     double val[kVars];
@@ -494,7 +662,25 @@ __global__ void ib_fill_kernel(const IbArgs a) {
     const int c = a.cell[g];
     const long long off = L.offset(c / L.ny, c - (c / L.ny) * L.ny);
 #pragma unroll
-    for (int v = 0; v < kVars; ++v) U[v * L.plane + off] = T(val[v]);
+    for (int v = 0; v < kVars; ++v) U[v * L.plane + off] = enc<T>(val[v], L, v);
+}
+
+template <class T>
+__global__ void ib_fill_kernel(const IbArgs a) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.n) return;
+    ib_fill_one<T>(a, g);
+}
+
+// Batched form: immersed-ghost cell g of the batch is cell local[g] of case
+// cases[g]; args[c] is case c's fill description (its state buffer, layout, lists).
+template <class T>
+__global__ void batch_ib_fill_kernel(const IbArgs* __restrict__ args, const int* __restrict__ cases,
+                                     const int* __restrict__ local, int total) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const IbArgs a = args[cases[g]];
+    ib_fill_one<T>(a, local[g]);
 }
 
 // ------------------------------------------------------ CFL reduction
@@ -508,8 +694,8 @@ __global__ void __launch_bounds__(NT) wmax_kernel(const T* U, const Layout L, co
         if (types && types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
         const long long off = L.offset(i, j);
-        const double w = wave_sum(double(U[off]), double(U[L.plane + off]), double(U[2 * L.plane + off]),
-                                  double(U[3 * L.plane + off]), g, dx, dy);
+        const double w = wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1), dec<T>(U[2 * L.plane + off], L, 2),
+                                  dec<T>(U[3 * L.plane + off], L, 3), g, dx, dy);
         if (w > m) m = w;
     }
     m = block_max<NT>(m, red);
@@ -526,7 +712,7 @@ __global__ void __launch_bounds__(NT) totals_kernel(const T* U, const Layout L, 
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
         const long long off = L.offset(i, j);
 #pragma unroll
-        for (int v = 0; v < kVars; ++v) s[v] += double(U[v * L.plane + off]);
+        for (int v = 0; v < kVars; ++v) s[v] += dec<T>(U[v * L.plane + off], L, v);
     }
 #pragma unroll
     for (int v = 0; v < kVars; ++v) {
@@ -547,7 +733,7 @@ __global__ void pack_kernel(const double* src, T* dst, const Layout L) {
         const int v = static_cast<int>(k / n);
         const long long c = k - v * n;
         const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
-        dst[v * L.plane + L.offset(i, j)] = T(src[k]);
+        dst[v * L.plane + L.offset(i, j)] = enc<T>(src[k], L, v);
     }
 }
 
@@ -559,47 +745,76 @@ __global__ void unpack_kernel(const T* src, double* dst, const Layout L) {
         const int v = static_cast<int>(k / n);
         const long long c = k - v * n;
         const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
-        dst[k] = double(src[v * L.plane + L.offset(i, j)]);
+        dst[k] = dec<T>(src[v * L.plane + L.offset(i, j)], L, v);
     }
 }
 
 // Fills all ghost layers of a state from its interior: Neumann copies of the
-// adjacent cell, periodic wraps, Dirichlet constants (bcU, conserved), as
+// adjacent cell, periodic wraps, Dirichlet constants (conserved), as
 // CartesianMesh::ApplyBoundaryCondition does once before the loop (Run.cpp:128).
+// Corner ghosts apply the x side's rule first, then the y side's.
+template <class T>
+__device__ __forceinline__ bool ghost_value(const T* p, const Layout& L, const BcSides& sides, int v, int gi, int gj,
+                                            T& out) {
+    int i = gi, j = gj;
+    if (gi < 0 || gi >= L.nx) {
+        const int s = gi < 0 ? 0 : 1;
+        const int bc = sides.bc[s];
+        if (bc == kDirichlet) { out = enc<T>(sides.U[s][v], L, v); return true; }
+        if (bc == kNeumann) i = gi < 0 ? 0 : L.nx - 1;
+        else if (bc == kPeriodic) i = gi < 0 ? gi + L.nx : gi - L.nx;
+        else return false;
+    }
+    if (gj < 0 || gj >= L.ny) {
+        const int s = gj < 0 ? 2 : 3;
+        const int bc = sides.bc[s];
+        if (bc == kDirichlet) { out = enc<T>(sides.U[s][v], L, v); return true; }
+        if (bc == kNeumann) j = gj < 0 ? 0 : L.ny - 1;
+        else if (bc == kPeriodic) j = gj < 0 ? gj + L.ny : gj - L.ny;
+        else return false;
+    }
+    out = p[L.offset(i, j)];
+    return true;
+}
+
 template <class T>
 __global__ void ghost_fill_kernel(T* U, const Layout L, BcSides sides) {
     const int per = (L.nx > L.ny ? L.nx : L.ny);
-    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < 4LL * kGhost * per * kVars;
+    const long long edge_items = 4LL * kGhost * per * kVars;
+    const long long corner_items = 4LL * kGhost * kGhost * kVars;
+    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < edge_items + corner_items;
          k += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int v = static_cast<int>(k % kVars);
-        long long rest = k / kVars;
-        const int pos = static_cast<int>(rest % per);
-        rest /= per;
-        const int layer = static_cast<int>(rest % kGhost) + 1;
-        const int side = static_cast<int>(rest / kGhost);
-        T* p = U + v * L.plane;
-        const int bc = sides.bc[side];
-        if (side < 2) {
-            const int j = pos;
-            if (j >= L.ny) continue;
-            const int gi = side == 0 ? -layer : L.nx - 1 + layer;
-            T val;
-            if (bc == kDirichlet) val = T(sides.U[side][v]);
-            else if (bc == kNeumann) val = p[L.offset(side == 0 ? 0 : L.nx - 1, j)];
-            else if (bc == kPeriodic) val = p[L.offset(side == 0 ? gi + L.nx : gi - L.nx, j)];
-            else continue;
-            p[L.offset(gi, j)] = val;
+        int gi, gj, v;
+        if (k < edge_items) {
+            v = static_cast<int>(k % kVars);
+            long long rest = k / kVars;
+            const int pos = static_cast<int>(rest % per);
+            rest /= per;
+            const int layer = static_cast<int>(rest % kGhost) + 1;
+            const int side = static_cast<int>(rest / kGhost);
+            if (side < 2) {
+                if (pos >= L.ny) continue;
+                gi = side == 0 ? -layer : L.nx - 1 + layer;
+                gj = pos;
+            } else {
+                if (pos >= L.nx) continue;
+                gi = pos;
+                gj = side == 2 ? -layer : L.ny - 1 + layer;
+            }
         } else {
-            const int i = pos;
-            if (i >= L.nx) continue;
-            const int gj = side == 2 ? -layer : L.ny - 1 + layer;
-            T val;
-            if (bc == kDirichlet) val = T(sides.U[side][v]);
-            else if (bc == kNeumann) val = p[L.offset(i, side == 2 ? 0 : L.ny - 1)];
-            else if (bc == kPeriodic) val = p[L.offset(i, side == 2 ? gj + L.ny : gj - L.ny)];
-            else continue;
-            p[L.offset(i, gj)] = val;
+            long long c = k - edge_items;
+            v = static_cast<int>(c % kVars);
+            c /= kVars;
+            const int ly = static_cast<int>(c % kGhost) + 1;
+            c /= kGhost;
+            const int lx = static_cast<int>(c % kGhost) + 1;
+            const int corner = static_cast<int>(c / kGhost);
+            gi = (corner & 1) ? L.nx - 1 + lx : -lx;
+            gj = (corner & 2) ? L.ny - 1 + ly : -ly;
         }
+        T* p = U + v * L.plane;
+        T val;
+        if (ghost_value<T>(p, L, sides, v, gi, gj, val)) p[L.offset(gi, gj)] = val;
     }
 }
 

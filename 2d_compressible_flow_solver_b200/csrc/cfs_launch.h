@@ -23,15 +23,42 @@ cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const 
 cudaError_t launch_pack(int elem_bytes, const double* src, void* dst, const Layout& L, cudaStream_t s);
 cudaError_t launch_unpack(int elem_bytes, const void* src, double* dst, const Layout& L, cudaStream_t s);
 cudaError_t launch_ghost_fill(int elem_bytes, void* U, const Layout& L, const BcSides& sides, cudaStream_t s);
+cudaError_t launch_viscous(Prec p, const ViscArgs& a, cudaStream_t s);
 cudaError_t launch_weno_faces(Prec p, int n, const double* st, double* left, double* right, double g, double eps,
                               cudaStream_t s);
 cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const double* R, double* F, double g,
                              int variant, cudaStream_t s);
 
+// Stage-kernel variants of the throughput forms (march_kernel template shapes).
+struct MarchVariant {
+    int rows, warps, min_blocks;
+};
+constexpr int kNumVariants = 6;
+constexpr MarchVariant kVariants[kNumVariants] = {
+    {64, 4, 1}, {64, 4, 4}, {64, 4, 5}, {32, 4, 5}, {128, 4, 4}, {64, 8, 2},
+};
+// 1-based defaults, the 4096^2 winners of the committed tuning table
+// (2d_compressible_flow_solver_b200/tuning.json).
+constexpr int kDefaultVariantF32 = 4;
+constexpr int kDefaultVariantF64 = 2;
+
+// Batched forms (cfs_batch_*): one launch covers every case of a batch.
+constexpr int kBatchWarps = 4;
+constexpr int kBatchMinBlocksF32 = 5;
+constexpr int kBatchMinBlocksF64 = 4;
+cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
+                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               int grid, cudaStream_t s);
+cudaError_t launch_batch_ib_fill(int elem_bytes, const IbArgs* args, const int* cases, const int* local, int total,
+                                 cudaStream_t s);
+int batch_blocks_per_sm(Prec p);
+
 // Per-policy entry points behind the dispatchers above.
 cudaError_t launch_stage_exact(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_viscous_f64(const ViscArgs& a, cudaStream_t s);
+cudaError_t launch_viscous_f32(const ViscArgs& a, cudaStream_t s);
 cudaError_t launch_weno_faces_exact(int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s);
 cudaError_t launch_weno_faces_f64(int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s);
 cudaError_t launch_weno_faces_f32(int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s);

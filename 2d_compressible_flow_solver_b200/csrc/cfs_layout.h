@@ -30,6 +30,10 @@ struct Layout {
     int joff;            // column of j = 0
     long long plane;     // elements per variable plane
     int elem_bytes;      // 8 (FP64) or 4 (FP32)
+    // FP32 storage keeps value - off[v] (off = an FP32 value near the variable's
+    // mean), so the rounding step of the stored state scales with the variation
+    // of the field rather than its magnitude.  Always 0 for FP64 storage.
+    float off[4];
 
     static Layout make(int nx, int ny, int elem_bytes) {
         Layout L;
@@ -41,6 +45,7 @@ struct Layout {
         const int need = L.joff + ny + kGhost;
         L.pitch = ((need + blk - 1) / blk) * blk;
         L.plane = static_cast<long long>(nx + 2 * kGhost) * L.pitch;
+        for (int v = 0; v < 4; ++v) L.off[v] = 0.0f;
         return L;
     }
     CFS_HD long long offset(int i, int j) const { return static_cast<long long>(i + kGhost) * pitch + joff + j; }
@@ -83,6 +88,17 @@ struct StageArgs {
     int parity;            // graph mode: which wmax slot holds this step's max
     int last_stage;        // 1: accumulate the CFL max of the new state into P->wmax[1-parity]
     int first_stage;       // 1: reset P->wmax[1-parity], advance P->t
+    const void* rv;        // optional viscous RHS (rho u, rho v, E) [3][nx][ny], storage type
+    int variant;           // throughput-form kernel variant (1-based; 0 = default)
+};
+
+// Viscous (Navier-Stokes) RHS of one state: (dFv/dx + dGv/dy) for the momentum
+// and energy equations, written to rv[3][nx][ny].
+struct ViscArgs {
+    const void* in;
+    void* rv;
+    Layout L;
+    double gamma, dx, dy, mu, kT, mach2;
 };
 
 struct IbArgs {

@@ -1,0 +1,346 @@
+// Row-marching stage kernel of the throughput forms (CFS_FP64, CFS_FP32_MIXED).
+//
+// Work decomposition: a warp owns a segment of kSeg = 30 consecutive y-cells
+// (columns j0 .. j0+29); its 32 lanes hold columns j0-1 .. j0+30, so every
+// interior cell has both y-neighbours' reconstructions inside the warp.  The
+// warp marches down x (rows) from i0-1 to i1:
+//  * the x-stencil of a lane is a 5-row register window of its column, one new
+//    row loaded per step (no shared memory, no block barrier);
+//  * the y-stencil comes from a per-warp row buffer in shared memory (the 32
+//    lane values plus 2 halo columns each side), synchronised with __syncwarp;
+//  * each cell reconstructs its own left- and right-biased WENO5 states per
+//    direction and variable from ONE set of smoothness indicators (the
+//    indicators of the two states are the same three numbers in mirrored
+//    order), then each face's HLL flux takes the left state of the cell below
+//    it and the right state of the cell above (a shuffle in y, the previous
+//    march step in x);
+//  * the RK update of row r-1 happens at step r, when its upper x-face exists.
+// Physical boundary faces use the reference's stencil (CellInterface.cpp:
+// 172-178: both walkers stop, so interior slots repeat the first interior cell).
+#pragma once
+#include "cfs_kernels.cuh"
+
+namespace cfs {
+
+constexpr int kSeg = 30;
+
+// Left- and right-biased WENO5 states of the middle cell of v0..v4
+// (Weno5th.cpp:4-28 applied to v0..v4 and to v4..v0) with shared smoothness
+// indicators and one reciprocal each.
+template <class C>
+__device__ __forceinline__ void weno5_pair(C v0, C v1, C v2, C v3, C v4, C eps, C& left, C& right) {
+    const C k13 = C(13.0 / 12.0), k14 = C(0.25);
+    const C d0 = v0 - C(2) * v1 + v2, e0 = v0 - C(4) * v1 + C(3) * v2;
+    const C d1 = v1 - C(2) * v2 + v3, e1 = v1 - v3;
+    const C d2 = v2 - C(2) * v3 + v4, e2 = C(3) * v2 - C(4) * v3 + v4;
+    C b0 = k13 * d0 * d0 + k14 * e0 * e0;
+    C b1 = k13 * d1 * d1 + k14 * e1 * e1;
+    C b2 = k13 * d2 * d2 + k14 * e2 * e2;
+    if (sizeof(C) == 4) {
+        b0 = fmin(b0, C(1e9));
+        b1 = fmin(b1, C(1e9));
+        b2 = fmin(b2, C(1e9));
+    }
+    C q0 = eps + b0, q1 = eps + b1, q2 = eps + b2;
+    q0 *= q0;
+    q1 *= q1;
+    q2 *= q2;
+    const C q01 = q0 * q1, q02 = q0 * q2, q12 = q1 * q2;
+    // left: linear weights (0.1, 0.6, 0.3) on indicators (b0, b1, b2)
+    const C aL0 = C(0.1) * q12, aL1 = C(0.6) * q02, aL2 = C(0.3) * q01;
+    const C pL0 = C(2) * v0 - C(7) * v1 + C(11) * v2;
+    const C pL1 = -v1 + C(5) * v2 + C(2) * v3;
+    const C pL2 = C(2) * v2 + C(5) * v3 - v4;
+    left = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * rcp_fast(C(6) * (aL0 + aL1 + aL2));
+    // right: the mirrored stencil's indicators are (b2, b1, b0)
+    const C aR0 = C(0.1) * q01, aR1 = C(0.6) * q02, aR2 = C(0.3) * q12;
+    const C pR0 = C(2) * v4 - C(7) * v3 + C(11) * v2;
+    const C pR1 = -v3 + C(5) * v2 + C(2) * v1;
+    const C pR2 = C(2) * v2 + C(5) * v1 - v0;
+    right = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * rcp_fast(C(6) * (aR0 + aR1 + aR2));
+}
+
+// Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).
+template <class Pol>
+__device__ __forceinline__ void cell_states(const typename Pol::C st[5][kVars], typename Pol::C eps, double g,
+                                            Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+    weno5_pair(st[0][0], st[1][0], st[2][0], st[3][0], st[4][0], eps, L.r, R.r);
+    weno5_pair(st[0][1], st[1][1], st[2][1], st[3][1], st[4][1], eps, L.mx, R.mx);
+    weno5_pair(st[0][2], st[1][2], st[2][2], st[3][2], st[4][2], eps, L.my, R.my);
+    weno5_pair(st[0][3], st[1][3], st[2][3], st[3][3], st[4][3], eps, L.E, R.E);
+    finish_state<Pol>(L, g);
+    finish_state<Pol>(R, g);
+}
+
+// Reference boundary face between an interior cell value c and a ghost value g
+// (lo = true: ghost below, stencil [g g g | c c c]; lo = false: [c c c | g g g]).
+template <class Pol>
+__device__ __forceinline__ void boundary_face_states(const typename Pol::C c[kVars], const typename Pol::C gh[kVars],
+                                                     bool lo, typename Pol::C eps, double g,
+                                                     Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+    using C = typename Pol::C;
+    C* lp[4] = {&L.r, &L.mx, &L.my, &L.E};
+    C* rp[4] = {&R.r, &R.mx, &R.my, &R.E};
+#pragma unroll
+    for (int v = 0; v < kVars; ++v) {
+        const C a = lo ? gh[v] : c[v], b = lo ? c[v] : gh[v];
+        // stencil s = (a, a, a, b, b, b): left from s0..s4, right from s5..s1
+        *lp[v] = weno5<Pol>(a, a, a, b, b, eps);
+        *rp[v] = weno5<Pol>(b, b, b, a, a, eps);
+    }
+    finish_state<Pol>(L, g);
+    finish_state<Pol>(R, g);
+}
+
+// One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
+// block column bx.  Every thread of the block calls it (it ends with a block
+// reduction when the CFL maximum is accumulated).
+template <class Pol, int kWarps>
+__device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
+                                           typename Pol::C (&rbuf)[kWarps][kVars][36], double* wred) {
+    using T = typename Pol::T;
+    using C = typename Pol::C;
+    const Layout& L = a.L;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int seg = bx * kWarps + wid;
+    const int j0 = seg * kSeg;
+    const int i0 = by * rows;
+    const int i1 = min(i0 + rows, L.nx);
+    const int j = j0 - 1 + lane;                 // this lane's column
+    const bool col_ok = j <= L.ny + kGhost - 1;  // inside the padded row
+    const bool owner = lane >= 1 && lane <= kSeg && j < L.ny;  // updates cells of this column
+    const T* in = static_cast<const T*>(a.in);
+    const C eps = C(a.eps);
+    const double g = a.gamma;
+    const double dt = stage_dt(a);
+    const double inv_dx = 1.0 / a.dx, inv_dy = 1.0 / a.dy;
+    const float inv_dxf = float(inv_dx);
+    // FP32 update coefficients of this stage: new = cA x0 + cB x1 + (c dt) R with
+    // x0 = U^0 (or the current state at stage 0), x1 = U^1 (TVD3 as written,
+    // stage 2) or the current state (TVD2rdRK.h:16-19, TVD3rdRK.h:14-18).
+    float cA = 1.0f, cB = 0.0f, cdt = float(dt);
+    bool x1_u1 = false;
+    if (a.stage == 1) {
+        if (a.rk == kRkTvd2) { cA = 0.5f; cB = 0.5f; cdt = float(0.5 * dt); }
+        else { cA = 0.75f; cB = 0.25f; cdt = float(0.25 * dt); }
+    } else if (a.stage == 2) {
+        // cA + cB must be exactly 1 in FP32, else the deviation form scales the
+        // stored deviations by (cA + cB) every step: cB = fl(2/3), cA = 1 - cB
+        // (an exact FP32 subtraction).
+        cB = float(2.0 / 3.0);
+        cA = 1.0f - cB;
+        cdt = float((2.0 / 3.0) * dt);
+        x1_u1 = a.rk == kRkTvd3Ref;
+    }
+    const bool lo_x = a.bc[0] == kNeumann || a.bc[0] == kDirichlet;
+    const bool hi_x = a.bc[1] == kNeumann || a.bc[1] == kDirichlet;
+    const bool lo_y = a.bc[2] == kNeumann || a.bc[2] == kDirichlet;
+    const bool hi_y = a.bc[3] == kNeumann || a.bc[3] == kDirichlet;
+    if (a.P && a.first_stage && bx == 0 && by == 0 && threadIdx.x == 0) {
+        a.P->wmax[1 - a.parity] = 0ull;
+        a.P->t += dt;
+        a.P->dt_last = dt;
+    }
+    const bool active_warp = j0 < L.ny;  // uniform per warp
+
+    auto load_row = [&](int r, C out[kVars]) {
+        if (col_ok) {
+            const long long off = L.offset(r, j);
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) out[v] = decc<T, C>(in[v * L.plane + off], L, v);
+        } else {
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) out[v] = C(0);
+        }
+    };
+
+    C win[5][kVars];
+    Face5<C> Lx{};                             // left x-state of the previous row
+    C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
+    C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
+    double wloc = 0.0;
+    if (active_warp) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) load_row(i0 - 3 + k, win[k]);
+    }
+    for (int r = i0 - 1; active_warp && r <= i1; ++r) {
+        // ---- x reconstruction of row r
+        Face5<C> Lr, Rr;
+        cell_states<Pol>(win, eps, g, Lr, Rr);
+        C FX[kVars] = {C(0), C(0), C(0), C(0)};
+        if (r >= i0) {
+            Face5<C> Lf = Lx;
+            Face5<C> Rf = Rr;
+            if (r == 0 && lo_x) boundary_face_states<Pol>(win[2], win[1], true, eps, g, Lf, Rf);
+            else if (r == L.nx && hi_x) boundary_face_states<Pol>(win[1], win[2], false, eps, g, Lf, Rf);
+            hll_flux<Pol>(Lf, Rf, 0, a.hll, g, FX);
+            // ---- update of row r-1 (its upper x-face is r - 1/2)
+            const int i = r - 1;
+            if (i >= i0 && owner) {
+                const bool fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+                const long long off = L.offset(i, j);
+                const T* u0 = static_cast<const T*>(a.u0);
+                const T* u1 = static_cast<const T*>(a.u1);
+                T* out = static_cast<T*>(a.out);
+                double nv[kVars];
+                T sv[kVars];
+                if constexpr (Pol::kMixed) {
+                    // FP32 update of the stored deviations (value - off): the RK
+                    // coefficients of a stage sum to 1, so the offsets cancel and
+                    // the rounding step is that of the deviation.
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) {
+                        float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
+                        if (a.rv && v >= 1)
+                            rvf += static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
+                        const float cur = in[v * L.plane + off];
+                        float nd = cur;
+                        if (fluid) {
+                            const float x0 = a.stage == 0 ? cur : u0[v * L.plane + off];
+                            const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
+                            nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
+                        }
+                        sv[v] = nd;
+                        nv[v] = double(nd) + double(L.off[v]);
+                        if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
+                    }
+                } else {
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) {
+                        double rv = -double(FX[v] - FXp[v]) * inv_dx + double(RY[v]);
+                        if (a.rv && v >= 1)
+                            rv += double(static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
+                        const double cur = double(win[1][v]);
+                        double val = cur;
+                        if (fluid) {
+                            const double u0v = a.stage >= 1 ? dec<T>(u0[v * L.plane + off], L, v) : 0.0;
+                            const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
+                            val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
+                        }
+                        sv[v] = enc<T>(val, L, v);
+                        nv[v] = dec<T>(sv[v], L, v);
+                        if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
+                    }
+                }
+                store_cell4<T>(out, L, a.bc, i, j, sv);
+                if (a.P && a.last_stage && a.P->use_cfl && fluid) {
+                    const double w = wave_sum(nv[0], nv[1], nv[2], nv[3], g, a.dx, a.dy);
+                    if (w > wloc) wloc = w;
+                }
+            }
+        }
+        // ---- y work of row r
+        if (r >= i0 && r < i1) {
+            C* rb = &rbuf[wid][0][0];
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) rb[v * 36 + lane + 2] = win[2][v];
+            if (lane < 2 || lane >= 30) {  // halo columns j0-3, j0-2 and j0+31, j0+32
+                const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
+                const int slot = lane < 2 ? lane : lane + 4;
+                if (hc <= L.ny + kGhost - 1) {
+                    const long long off = L.offset(r, hc);
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = decc<T, C>(in[v * L.plane + off], L, v);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = C(0);
+                }
+            }
+            __syncwarp();
+            C st[5][kVars];
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) st[k][v] = rb[v * 36 + lane + k];
+            Face5<C> Ly, Ry;
+            cell_states<Pol>(st, eps, g, Ly, Ry);
+            // right state of the cell above (lane + 1)
+            Face5<C> Rn;
+            Rn.r = __shfl_down_sync(0xffffffffu, Ry.r, 1);
+            Rn.mx = __shfl_down_sync(0xffffffffu, Ry.mx, 1);
+            Rn.my = __shfl_down_sync(0xffffffffu, Ry.my, 1);
+            Rn.E = __shfl_down_sync(0xffffffffu, Ry.E, 1);
+            Rn.p = __shfl_down_sync(0xffffffffu, Ry.p, 1);
+            Rn.a = __shfl_down_sync(0xffffffffu, Ry.a, 1);
+            Rn.ri = __shfl_down_sync(0xffffffffu, Ry.ri, 1);
+            // face between column j and j+1 (face index j+1)
+            if (j + 1 == 0 && lo_y) {
+                C cc[kVars], gg[kVars];
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) { gg[v] = st[2][v]; cc[v] = st[3][v]; }
+                boundary_face_states<Pol>(cc, gg, true, eps, g, Ly, Rn);
+            } else if (j + 1 == L.ny && hi_y) {
+                C cc[kVars], gg[kVars];
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) { cc[v] = st[2][v]; gg[v] = st[3][v]; }
+                boundary_face_states<Pol>(cc, gg, false, eps, g, Ly, Rn);
+            }
+            C FY[kVars];
+            hll_flux<Pol>(Ly, Rn, 1, a.hll, g, FY);
+#pragma unroll
+            for (int v = 0; v < kVars; ++v) {
+                const C below = __shfl_up_sync(0xffffffffu, FY[v], 1);
+                RY[v] = C(-double(FY[v] - below) * inv_dy);
+            }
+            __syncwarp();
+        }
+        // ---- carry to the next row
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) FXp[v] = FX[v];
+        Lx = Lr;
+        if (r < i1) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) win[k][v] = win[k + 1][v];
+            load_row(r + 3, win[4]);
+        }
+    }
+    if (a.P && a.last_stage && a.P->use_cfl) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) wloc = fmax(wloc, __shfl_xor_sync(0xffffffffu, wloc, o));
+        if (lane == 0) wred[wid] = wloc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = 0.0;
+            for (int w = 0; w < kWarps; ++w) m = fmax(m, wred[w]);
+            if (m > 0.0) atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(m)));
+        }
+        __syncthreads();
+    }
+}
+
+template <class Pol, int kRows, int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
+    __shared__ typename Pol::C rbuf[kWarps][kVars][36];
+    __shared__ double wred[kWarps];
+    march_item<Pol, kWarps>(a, blockIdx.x, blockIdx.y, kRows, rbuf, wred);
+}
+
+// Persistent batched form: one launch runs one stage of every case of a batch.
+// Each block pulls work items (case, block column, row chunk) from a global
+// counter, largest cases first, until none are left.  args[c] holds case c's
+// stage arguments (its own layout, boundaries, buffers, dt slot); rows[c] is
+// the row chunk the autotuner chose for its size.
+template <class Pol, int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
+    batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ item_case,
+                       const int* __restrict__ item_local, const int* __restrict__ case_rows,
+                       const int* __restrict__ case_items_x, int total, unsigned int* counter) {
+    __shared__ typename Pol::C rbuf[kWarps][kVars][36];
+    __shared__ double wred[kWarps];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+        __syncthreads();
+        const int w = s_item;
+        __syncthreads();
+        if (w >= total) break;
+        const int c = item_case[w], li = item_local[w];
+        const int ix = case_items_x[c];
+        const StageArgs a = args[c];
+        march_item<Pol, kWarps>(a, li % ix, li / ix, case_rows[c], rbuf, wred);
+    }
+}
+
+}  // namespace cfs

@@ -180,31 +180,71 @@ void ldlt4_lower(const double M[4][4], double fac[10], int perm[4]) {
     for (int k = 0; k < 4; ++k) fac[6 + k] = d[k];
 }
 
-bool bilinear_weights(const double M[4][4], double X, double Y, double w[4]) {
-    double A[4][5];
-    const double rhs[4] = {X * Y, X, Y, 1.0};
-    for (int r = 0; r < 4; ++r) {
-        for (int c = 0; c < 4; ++c) A[r][c] = M[c][r];
-        A[r][4] = rhs[r];
-    }
+void slip_donors(const uint8_t* types, int nx, int ny, double dx, double dy, double X, double Y,
+                 const int32_t fallback[4], int32_t donor[4], double w[4]) {
+    const double fx = (X - 0.5 * dx) / dx, fy = (Y - 0.5 * dy) / dy;
+    const int i0 = static_cast<int>(std::floor(fx)), j0 = static_cast<int>(std::floor(fy));
+    const double tx = fx - i0, ty = fy - j0;
+    const int ci[4] = {i0, i0 + 1, i0, i0 + 1};
+    const int cj[4] = {j0, j0, j0 + 1, j0 + 1};
+    const double cw[4] = {(1 - tx) * (1 - ty), tx * (1 - ty), (1 - tx) * ty, tx * ty};
+    int keep = -1;
+    double sum = 0.0;
     for (int k = 0; k < 4; ++k) {
-        int piv = k;
-        for (int r = k + 1; r < 4; ++r)
-            if (std::fabs(A[r][k]) > std::fabs(A[piv][k])) piv = r;
-        if (A[piv][k] == 0.0) return false;
-        if (piv != k)
-            for (int c = 0; c < 5; ++c) std::swap(A[k][c], A[piv][c]);
-        for (int r = k + 1; r < 4; ++r) {
-            const double m = A[r][k] / A[k][k];
-            for (int c = k; c < 5; ++c) A[r][c] -= m * A[k][c];
+        const bool ok = ci[k] >= 0 && ci[k] < nx && cj[k] >= 0 && cj[k] < ny &&
+                        types[static_cast<size_t>(ci[k]) * ny + cj[k]] == 0;
+        donor[k] = ok ? ci[k] * ny + cj[k] : -1;
+        w[k] = ok ? cw[k] : 0.0;
+        if (ok) {
+            sum += cw[k];
+            if (keep < 0) keep = k;
         }
     }
-    for (int r = 3; r >= 0; --r) {
-        double s = A[r][4];
-        for (int c = r + 1; c < 4; ++c) s -= A[r][c] * w[c];
-        w[r] = s / A[r][r];
+    if (sum > 1e-3) {
+        for (int k = 0; k < 4; ++k) {
+            if (donor[k] < 0) donor[k] = donor[keep];
+            w[k] = w[k] / sum;
+        }
+        return;
     }
-    return true;
+    double s = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const int i = fallback[k] / ny, j = fallback[k] % ny;
+        const double ddx = (i + 0.5) * dx - X, ddy = (j + 0.5) * dy - Y;
+        w[k] = 1.0 / (ddx * ddx + ddy * ddy + 1e-300);
+        donor[k] = fallback[k];
+        s += w[k];
+    }
+    for (int k = 0; k < 4; ++k) w[k] /= s;
+}
+
+void ib_factors(int mode, const uint8_t* types, int nx, int ny, double dx, double dy, int n, const int32_t* donor4,
+                const double* image, const double* normal, std::vector<int32_t>& dev_donor, std::vector<double>& fac,
+                std::vector<int>& perm) {
+    fac.assign(16 * static_cast<size_t>(n), 0.0);
+    perm.assign(4 * static_cast<size_t>(n), 0);
+    dev_donor.assign(donor4, donor4 + 4 * static_cast<size_t>(n));
+    for (int g = 0; g < n; ++g) {
+        if (mode == 0) {
+            double M[4][4];
+            for (int k = 0; k < 4; ++k) {
+                const int d = donor4[4 * g + k];
+                const int i = d / ny, j = d % ny;
+                const double x = (i + 0.5) * dx, y = (j + 0.5) * dy;  // CartesianMesh.cpp:92
+                M[k][0] = x * y;
+                M[k][1] = x;
+                M[k][2] = y;
+                M[k][3] = 1.0;
+            }
+            ldlt4_lower(M, &fac[16 * g], &perm[4 * g]);
+        } else {
+            double w[4];
+            slip_donors(types, nx, ny, dx, dy, image[2 * g], image[2 * g + 1], &donor4[4 * g], &dev_donor[4 * g], w);
+            for (int k = 0; k < 4; ++k) fac[16 * g + k] = w[k];
+            fac[16 * g + 4] = normal[2 * g];
+            fac[16 * g + 5] = normal[2 * g + 1];
+        }
+    }
 }
 
 }  // namespace cfs

@@ -25,9 +25,22 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
 // (Eigen's ldlt(), ImagePoint.cpp:44): fac = l10 l20 l21 l30 l31 l32 d0 d1 d2 d3.
 void ldlt4_lower(const double M[4][4], double fac[10], int perm[4]);
 
-// Weights w with w . f equal to the bilinear interpolant of the donor values f
-// at (X, Y): solves M^T w = (XY, X, Y, 1) with partial pivoting.
-// Returns false when M is singular.
-bool bilinear_weights(const double M[4][4], double X, double Y, double w[4]);
+// Donors and weights of the slip-wall form for one image point (X, Y): the
+// 2 x 2 block of cell centres around the point with tensor-product bilinear
+// weights; donors that are not fluid (or off the grid) are dropped and the
+// remaining weights renormalised (a dropped slot repeats a kept donor with
+// weight 0).  When the kept weight is below 1e-3, inverse-squared-distance
+// weights over the `fallback` donors (the reference's 4 nearest fluid cells).
+// types: [nx*ny], 0 = fluid.  Donor indices are i*ny + j.
+void slip_donors(const uint8_t* types, int nx, int ny, double dx, double dy, double X, double Y,
+                 const int32_t fallback[4], int32_t donor[4], double w[4]);
+
+// Device-side fill data of n immersed-ghost cells.  Reference form: the
+// pivoted LDL^T factor of each donor matrix (fac[16g..16g+9], perm[4g..]).
+// Slip form: slip_donors' donors (dev_donor) and weights (fac[16g..16g+3]) with
+// the wall normal (fac[16g+4..5]); donor4 serve as its fallback.
+void ib_factors(int mode, const uint8_t* types, int nx, int ny, double dx, double dy, int n, const int32_t* donor4,
+                const double* image, const double* normal, std::vector<int32_t>& dev_donor, std::vector<double>& fac,
+                std::vector<int>& perm);
 
 }  // namespace cfs

@@ -32,6 +32,15 @@ cudaError_t launch_ib_fill(int elem_bytes, const IbArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_batch_ib_fill(int elem_bytes, const IbArgs* args, const int* cases, const int* local, int total,
+                                 cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    const int nt = 128, nb = (total + nt - 1) / nt;
+    if (elem_bytes == 8) batch_ib_fill_kernel<double><<<nb, nt, 0, s>>>(args, cases, local, total);
+    else batch_ib_fill_kernel<float><<<nb, nt, 0, s>>>(args, cases, local, total);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_wmax(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double g, double dx,
                         double dy, unsigned long long* out, cudaStream_t s) {
     constexpr int nt = 256;
@@ -66,7 +75,7 @@ cudaError_t launch_unpack(int elem_bytes, const void* src, double* dst, const La
 
 cudaError_t launch_ghost_fill(int elem_bytes, void* U, const Layout& L, const BcSides& sides, cudaStream_t s) {
     const int per = L.nx > L.ny ? L.nx : L.ny;
-    const int nt = 256, nb = flat_blocks(4LL * kGhost * per * kVars, nt);
+    const int nt = 256, nb = flat_blocks(4LL * kGhost * per * kVars + 4LL * kGhost * kGhost * kVars, nt);
     if (elem_bytes == 8) ghost_fill_kernel<double><<<nb, nt, 0, s>>>(static_cast<double*>(U), L, sides);
     else ghost_fill_kernel<float><<<nb, nt, 0, s>>>(static_cast<float*>(U), L, sides);
     return cudaGetLastError();

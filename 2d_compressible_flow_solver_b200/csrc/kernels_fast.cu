@@ -2,22 +2,78 @@
 // FP32-mixed form.  Built with FMA contraction on (nvcc default).
 #include "cfs_kernels.cuh"
 #include "cfs_launch.h"
+#include "cfs_march.cuh"
 
 namespace cfs {
 
-namespace {
-inline dim3 stage_grid(const Layout& L) {
-    return dim3((L.ny + kTileJ - 1) / kTileJ, (L.nx + kTileI - 1) / kTileI);
-}
-}  // namespace
-
-cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
-    stage_kernel<PolF64, kTileI, kTileJ><<<stage_grid(a.L), kTileI * kTileJ, 0, s>>>(a);
+template <class Pol, int R, int W, int B>
+cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
+    const int nseg = (a.L.ny + kSeg - 1) / kSeg;
+    const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
+    march_kernel<Pol, R, W, B><<<grid, 32 * W, 0, s>>>(a);
     return cudaGetLastError();
 }
 
+template <class Pol>
+cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
+    static_assert(kNumVariants == 6, "variant table and dispatch disagree");
+    switch (v) {
+        case 1: return launch_march<Pol, kVariants[0].rows, kVariants[0].warps, kVariants[0].min_blocks>(a, s);
+        case 2: return launch_march<Pol, kVariants[1].rows, kVariants[1].warps, kVariants[1].min_blocks>(a, s);
+        case 3: return launch_march<Pol, kVariants[2].rows, kVariants[2].warps, kVariants[2].min_blocks>(a, s);
+        case 4: return launch_march<Pol, kVariants[3].rows, kVariants[3].warps, kVariants[3].min_blocks>(a, s);
+        case 5: return launch_march<Pol, kVariants[4].rows, kVariants[4].warps, kVariants[4].min_blocks>(a, s);
+        case 6: return launch_march<Pol, kVariants[5].rows, kVariants[5].warps, kVariants[5].min_blocks>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
+    return launch_march_variant<PolF64>(a, a.variant > 0 ? a.variant : kDefaultVariantF64, s);
+}
+
 cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
-    stage_kernel<PolF32, kTileI, kTileJ><<<stage_grid(a.L), kTileI * kTileJ, 0, s>>>(a);
+    return launch_march_variant<PolF32>(a, a.variant > 0 ? a.variant : kDefaultVariantF32, s);
+}
+
+cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
+                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               int grid, cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    if (p == kF32Mixed)
+        batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32><<<grid, 32 * kBatchWarps, 0, s>>>(
+            args, item_case, item_local, case_rows, case_items_x, total, counter);
+    else
+        batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64><<<grid, 32 * kBatchWarps, 0, s>>>(
+            args, item_case, item_local, case_rows, case_items_x, total, counter);
+    return cudaGetLastError();
+}
+
+int batch_blocks_per_sm(Prec p) {
+    int n = 0;
+    if (p == kF32Mixed)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32>,
+                                                      32 * kBatchWarps, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64>,
+                                                      32 * kBatchWarps, 0);
+    return n > 0 ? n : 1;
+}
+
+constexpr int kViscTI = 8;
+constexpr int kViscTJ = 32;
+
+inline dim3 visc_grid(const Layout& L) {
+    return dim3((L.ny + kViscTJ - 1) / kViscTJ, (L.nx + kViscTI - 1) / kViscTI);
+}
+
+cudaError_t launch_viscous_f64(const ViscArgs& a, cudaStream_t s) {
+    viscous_kernel<PolF64, kViscTI, kViscTJ><<<visc_grid(a.L), kViscTI * kViscTJ, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_viscous_f32(const ViscArgs& a, cudaStream_t s) {
+    viscous_kernel<PolF32, kViscTI, kViscTJ><<<visc_grid(a.L), kViscTI * kViscTJ, 0, s>>>(a);
     return cudaGetLastError();
 }
 

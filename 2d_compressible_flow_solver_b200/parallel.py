@@ -1,0 +1,157 @@
+"""Multi-GPU decomposition: one grid split into slabs along x, one slab per
+rank (one GPU per rank), the B200 replacement of the reference's MPI
+decomposition (source/parallel/CartesianParallel.cpp:3-60 decomposition,
+:62-148 process-boundary ghost cells, :172-427 halo exchange).
+
+Per RK stage each rank sends the 3 interior rows next to each inner side to
+its neighbour and receives the neighbour's rows into its 3 ghost rows (rows
+are contiguous in the engine's layout, so a message is 4 device copies of
+3 x pitch elements).  Per step the CFL time step is the minimum over ranks.
+Only the exchange is a collective step; everything else stays on each GPU.
+The immersed boundary is not decomposed (a slab solver has none).
+
+Message order (point-to-point ops match in posting order per peer): every
+rank posts send(right rows -> right), send(left rows -> left),
+recv(left ghost <- left), recv(right ghost <- right).  A rank's first message
+to its right neighbour is therefore that neighbour's first receive from its
+left, also when one rank is both neighbours (two ranks, periodic).
+"""
+from __future__ import annotations
+
+import importlib
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent.name
+
+
+def slab_bounds(nx_global: int, world: int, rank: int) -> tuple[int, int]:
+    """Rows [i0, i1) of `rank`: near-equal slabs, the first nx % world ranks one row longer."""
+    base, extra = divmod(nx_global, world)
+    i0 = rank * base + min(rank, extra)
+    return i0, i0 + base + (1 if rank < extra else 0)
+
+
+def neighbours(world: int, rank: int, periodic_x: bool) -> tuple[int | None, int | None]:
+    """(left, right) ranks, None at a physical side of the global grid."""
+    if world == 1:
+        return None, None
+    left = rank - 1 if rank > 0 else (world - 1 if periodic_x else None)
+    right = rank + 1 if rank < world - 1 else (0 if periodic_x else None)
+    return left, right
+
+
+class HaloExchange:
+    """Ordered halo exchange of one slab.  `slab` provides nbytes(), pack(side,
+    tensor), unpack(side, tensor) and sync(); `dist` is torch.distributed."""
+
+    def __init__(self, slab, dist, left, right, device):
+        import torch
+
+        self.slab, self.dist, self.left, self.right = slab, dist, left, right
+        n = slab.nbytes()
+        mk = lambda: torch.empty(n, dtype=torch.uint8, device=device)  # noqa: E731
+        self.send = {0: mk(), 1: mk()}
+        self.recv = {0: mk(), 1: mk()}
+
+    def exchange(self) -> None:
+        import torch
+
+        if self.left is None and self.right is None:
+            return
+        for side, peer in ((0, self.left), (1, self.right)):
+            if peer is not None:
+                self.slab.pack(side, self.send[side])
+        self.slab.sync()
+        d = self.dist
+        ops = []
+        if self.right is not None:
+            ops.append(d.P2POp(d.isend, self.send[1], self.right))
+        if self.left is not None:
+            ops.append(d.P2POp(d.isend, self.send[0], self.left))
+        if self.left is not None:
+            ops.append(d.P2POp(d.irecv, self.recv[0], self.left))
+        if self.right is not None:
+            ops.append(d.P2POp(d.irecv, self.recv[1], self.right))
+        for req in d.batch_isend_irecv(ops):
+            req.wait()
+        if self.send[0].is_cuda:
+            torch.cuda.synchronize(self.send[0].device)
+        for side, peer in ((0, self.left), (1, self.right)):
+            if peer is not None:
+                self.slab.unpack(side, self.recv[side])
+
+
+class _EngineSlab:
+    """HaloExchange adapter of the CUDA engine (cfs_halo_* entry points)."""
+
+    def __init__(self, solver):
+        self.s = solver
+
+    def nbytes(self):
+        return self.s.halo_bytes()
+
+    def pack(self, side, t):
+        self.s.halo_pack(side, t.data_ptr())
+
+    def unpack(self, side, t):
+        self.s.halo_unpack(side, t.data_ptr())
+
+    def sync(self):
+        self.s.synchronize()
+
+
+def global_min(dist, value: float, device) -> float:
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    return float(t.item())
+
+
+class SlabSolver:
+    """Engine solver of one slab of a global nx_global x ny grid on [0,lx]x[0,ly].
+    bc is the global (left, right, bottom, top); inner x sides become halo sides."""
+
+    def __init__(self, nx_global: int, ny: int, lx: float, ly: float, *, dist, rank: int, world: int, device: int,
+                 bc=(2, 2, 2, 2), **solver_kw):
+        cfsb = importlib.import_module(_PKG)
+        self.dist, self.rank, self.world, self.device = dist, rank, world, device
+        self.i0, self.i1 = slab_bounds(nx_global, world, rank)
+        periodic_x = bc[0] == cfsb.BC_PERIODIC
+        self.left, self.right = neighbours(world, rank, periodic_x)
+        local_bc = list(bc)
+        if self.left is not None:
+            local_bc[0] = cfsb.BC_HALO
+        if self.right is not None:
+            local_bc[1] = cfsb.BC_HALO
+        nloc = self.i1 - self.i0
+        self.solver = cfsb.Solver(nloc, ny, lx * nloc / nx_global, ly, bc=tuple(local_bc), device=device, **solver_kw)
+        self.stages = 2 if self.solver.config.rk == cfsb.RK_TVD2 else 3
+        self.halo = HaloExchange(_EngineSlab(self.solver), dist, self.left, self.right, f"cuda:{device}")
+
+    def set_state(self, U_local) -> None:
+        self.solver.set_state(U_local)
+        self.halo.exchange()
+
+    def get_state(self):
+        return self.solver.get_state()
+
+    def compute_dt(self, cfl: float) -> float:
+        dt = self.solver.compute_dt(cfl)
+        return global_min(self.dist, dt, f"cuda:{self.device}") if self.world > 1 else dt
+
+    def step(self, dt: float) -> None:
+        for k in range(1, self.stages + 1):
+            self.solver.stage(k, dt)
+            self.halo.exchange()
+
+    def advance(self, nsteps: int, cfl: float) -> float:
+        t = 0.0
+        for _ in range(nsteps):
+            dt = self.compute_dt(cfl)
+            self.step(dt)
+            t += dt
+        return t
+
+    def close(self) -> None:
+        self.solver.close()

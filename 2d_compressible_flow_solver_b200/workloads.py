@@ -116,3 +116,39 @@ def shear_layer(n: int = 1024, seed: int = 1, mu: float = 1.0 / 2000.0) -> Workl
     U = conserved(np.ones((n, n)), u, v, 2.5)
     return Workload(f"shear_layer_{n}", n, n, 1.0, 1.0, U, bc=(2, 2, 2, 2), cfl=0.5, steps=5000,
                     meta={"seed": seed, "a": a.tolist(), "mu": mu, "prandtl": 0.72})
+
+
+def batch_cases(ncases: int = 512, seed: int = 1, sizes=None):
+    """Uneven batch: grid edges nx, ny drawn from {64, 80, ..., 768} (multiples of
+    16); the first half are seeded four-quadrant states on [0,1]^2 with
+    transmissive sides; the second half a Mach M ~ U[2, 3] freestream
+    (rho 1.4, p 1, u = M sqrt(gamma p / rho)) past a circle of radius
+    r ~ U[0.03, 0.1] centred in [3r, 1-3r]^2, Dirichlet inflow on the left,
+    transmissive elsewhere, slip wall.  Every cell, those inside the body
+    included, starts at the freestream: cells deeper in the body than the ghost
+    layer keep that state and are still read by the fluid cells' 3-cell WENO
+    stencils.  (The reference fills fluid cells only, Run.cpp:98-104, leaving
+    zero-density solid cells inside those stencils.)  Returns (case
+    descriptions, states)."""
+    rng = np.random.default_rng(seed)
+    edges = np.arange(64, 769, 16) if sizes is None else np.asarray(sizes)
+    cases, states = [], []
+    for k in range(ncases):
+        nx, ny = int(rng.choice(edges)), int(rng.choice(edges))
+        if k < ncases // 2:
+            w = riemann_quadrants(nx, ny, seed=int(rng.integers(1 << 30)))
+            cases.append({"nx": nx, "ny": ny, "lx": 1.0, "ly": 1.0, "bc": (0, 0, 0, 0)})
+            states.append(w.U0)
+        else:
+            mach = rng.uniform(2.0, 3.0)
+            r = rng.uniform(0.03, 0.1)
+            cx, cy = rng.uniform(3 * r, 1 - 3 * r), rng.uniform(3 * r, 1 - 3 * r)
+            rho, p = 1.4, 1.0
+            u = mach * math.sqrt(GAMMA * p / rho)
+            prim = [rho, u, 0.0, p]
+            U = conserved(np.full((nx, ny), rho), u, 0.0, p)
+            cases.append({"nx": nx, "ny": ny, "lx": 1.0, "ly": 1.0, "bc": (1, 0, 0, 0), "bc_prim": [prim] * 4,
+                          "circle": (r, cx, cy), "ib_mode": 1})
+            states.append(U)
+    return cases, states
+

@@ -185,8 +185,11 @@ def engine_arm(args):
         if world > 1:
             dist.barrier()
 
+    autotune = importlib.import_module(f"{PKG}.autotune")
+    variants = {cfsb.FP32_MIXED: autotune.best_variant("f32", n * n), cfsb.FP64: autotune.best_variant("f64", n * n)}
+
     def timed_advance(prec, steps, warm):
-        s = cfsb.Solver(n, n, precision=prec, **kw)
+        s = cfsb.Solver(n, n, precision=prec, variant=variants[prec], **kw)
         s.set_state(w.U0)
         stream = torch.cuda.ExternalStream(s.stream, device=local)
         if warm:
@@ -234,6 +237,7 @@ def engine_arm(args):
             "config": {"workload": f"smooth periodic advection {n}x{n} (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1), "
                                    "SSP-RK3, WENO5 eps 1e-2, Davis HLL, CFL 0.4 on-device dt",
                        "precision": "fp32-mixed", "grid": [n, n], "cells_per_gpu": cells,
+                       "kernel_variant": {"f32": variants[cfsb.FP32_MIXED], "f64": variants[cfsb.FP64]},
                        "l2": "inputs larger than L2 (3 state buffers of "
                              f"{4 * 4 * cells / 1e6:.0f} MB each)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -320,6 +324,62 @@ def engine_arm(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------ batch arm
+def batch_arm(args):
+    """Uneven batch of independent cases (512 by default): aggregate
+    Mcell-steps/s of the persistent batched engine (FP32-mixed and FP64) and of
+    a loop of plain FP64 single-grid solvers over the same cases."""
+    import torch
+
+    cfsb = importlib.import_module(PKG)
+    wl = importlib.import_module(f"{PKG}.workloads")
+    cases, states = wl.batch_cases(args.cases, seed=1)
+    K, W = args.steps, args.warmup
+    out = {"workload": f"{args.cases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
+                       "cylinder (slip wall), SSP-RK3, Davis HLL, per-case CFL 0.5", "steps": K, "warmup": W}
+
+    def run_batch(prec):
+        with cfsb.Batch(cases, precision=prec) as b:
+            cells, items = b.info()
+            for k, U in enumerate(states):
+                b.set_state(k, U)
+            b.advance(W, cfl=0.5)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.advance(K, cfl=0.5)
+            wall = time.perf_counter() - t0
+        return cells, items, cells * K / wall / 1e6, wall
+
+    cells, items, v32, w32 = run_batch(cfsb.FP32_MIXED)
+    _, _, v64, w64 = run_batch(cfsb.FP64)
+    out.update({"cells": cells, "work_items_per_stage": items,
+                "batched_fp32": round(v32, 1), "batched_fp64": round(v64, 1)})
+    solvers = []
+    for c, U in zip(cases, states):
+        s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
+                        bc=c["bc"], bc_prim=c.get("bc_prim"))
+        if "circle" in c:
+            s.build_circle(*c["circle"], 400, cfsb.IB_BILINEAR_SLIP)
+        s.set_state(U)
+        s.advance(W, cfl=0.5)
+        solvers.append(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.advance(K, cfl=0.5)
+    wall = time.perf_counter() - t0
+    for s in solvers:
+        s.close()
+    loop64 = cells * K / wall / 1e6
+    peak, _ = hbm_peak()
+    out.update({"loop_plain_fp64": round(loop64, 1), "batched_fp32_over_loop_fp64": round(v32 / loop64, 2),
+                "batched_fp32_over_batched_fp64": round(v32 / v64, 2),
+                "batched_fp32_hbm_frac": round(v32 * 1e6 * WORDS_PER_CELL_STEP * 4 / 1e9 / peak, 4),
+                "timing": "host wall clock around cfs_batch_advance / the per-case cfs_advance loop (each call "
+                          "waits for its stream)"})
+    print(json.dumps(out), flush=True)
+
+
 # ----------------------------------------------------------- reference arm
 def reference_arm(args):
     rank, world, _ = env_rank()
@@ -360,10 +420,15 @@ def main():
     ap.add_argument("--n", type=int, default=4096, help="grid edge (cells) per GPU")
     ap.add_argument("--accuracy-n", type=int, default=1024, help="grid of the FP32-vs-FP64 check (0 = skip)")
     ap.add_argument("--cpu-sample", type=int, default=384, help="grid edge of one CPU-baseline sample")
+    ap.add_argument("--workload", choices=["smooth", "batch"], default="smooth",
+                    help="smooth: the headline 4096^2 line; batch: the uneven-batch comparison (one JSON line)")
+    ap.add_argument("--cases", type=int, default=512, help="cases of the batch workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "batch":
+        batch_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         engine_arm(args)

@@ -58,7 +58,10 @@ enum cfs_hll {
 enum cfs_bc {
     CFS_BC_NEUMANN = 0,    /* NeummanBoundary (NeummanBoundary.cpp:31-45): ghost = adjacent cell */
     CFS_BC_DIRICHLET = 1,  /* DirichletBoundary (DirichletBoundary.cpp:32-46): fixed state */
-    CFS_BC_PERIODIC = 2    /* no reference counterpart */
+    CFS_BC_PERIODIC = 2,   /* no reference counterpart */
+    CFS_BC_HALO = 3        /* left/right only: ghost rows filled by the caller from a neighbouring
+                              subdomain (cfs_halo_unpack), as CartesianParallel::exchangedata fills
+                              the process-boundary ghost cells (CartesianParallel.cpp:172-427) */
 };
 
 enum cfs_cell_type { CFS_CELL_FLUID = 0, CFS_CELL_SOLID = 1, CFS_CELL_IMMERSED_GHOST = 2 };
@@ -66,7 +69,10 @@ enum cfs_cell_type { CFS_CELL_FLUID = 0, CFS_CELL_SOLID = 1, CFS_CELL_IMMERSED_G
 enum cfs_ib_mode {
     CFS_IB_REFERENCE = 0,      /* ImagePoint::InterpolatePhase (ImagePoint.cpp:20-82): LDLT of the
                                   donor matrix's lower triangle, both momenta negated (Cell.cpp:172-181) */
-    CFS_IB_BILINEAR_SLIP = 1   /* true bilinear weights, only the wall-normal momentum reflected */
+    CFS_IB_BILINEAR_SLIP = 1   /* bilinear weights over the 2 x 2 cell block around the image point
+                                  (fluid cells only, renormalised; inverse-distance weights over the
+                                  given donors when that block has no fluid weight), only the
+                                  wall-normal momentum reflected (slip wall) */
 };
 
 enum cfs_viscous { CFS_VISCOUS_OFF = 0, CFS_VISCOUS_NS = 1 };
@@ -85,9 +91,18 @@ typedef struct cfs_config {
     double mu, prandtl, mach;/* Navier-Stokes constants (constant viscosity, T = gamma Ma^2 p / rho) */
     int keep_rhs;            /* 1: keep the last stage's RHS for cfs_get_rhs (Cell::comRHS m_flux) */
     int device;              /* CUDA device ordinal */
+    int variant;             /* stage-kernel variant of the throughput forms (tile rows x warps x
+                                occupancy target, see cfs_variant_info); 0 = the tuned default */
 } cfs_config;
 
 typedef struct cfs_ctx cfs_ctx;
+
+/* Number of stage-kernel variants of the throughput forms, and the shape of
+ * variant v (1-based): rows marched per warp, warps per block, minimum resident
+ * blocks per SM requested from the compiler.  Returns CFS_ERR_INVALID for an
+ * unknown v. */
+int cfs_variant_count(void);
+int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks);
 
 /* Fills a config with the reference's defaults: gamma 1.4, eps 1e-2, FP64,
  * TVD3 as written, reference HLL, Neumann sides, inviscid. */
@@ -121,7 +136,8 @@ int cfs_set_cell_types(cfs_ctx* ctx, const uint8_t* types);
 /* Immersed-ghost list: n cells (i*ny + j), 4 fluid donors each (i*ny + j, in
  * the reference's nearest-first order), the image point (x, y) of each, and
  * for CFS_IB_BILINEAR_SLIP the unit wall normal.  Replaces the ImagePoint
- * objects Circle::SetImagepoint builds (Circle.cpp:105-138). */
+ * objects Circle::SetImagepoint builds (Circle.cpp:105-138).  Set the cell
+ * types first: the slip form picks its donors among fluid cells. */
 int cfs_set_ib(cfs_ctx* ctx, int mode, int n, const int32_t* cell, const int32_t* donor4,
                const double* image_xy, const double* normal_xy);
 
@@ -176,6 +192,16 @@ int cfs_step(cfs_ctx* ctx, double dt);
  * the simulated time advanced, *dt_last the last dt. */
 int cfs_advance(cfs_ctx* ctx, int nsteps, double cfl, double dt, double* t_elapsed, double* dt_last);
 
+/* Halo exchange of a slab decomposition along x (the reference's process
+ * boundaries, CartesianParallel.cpp:62-148).  side 0 = left (low x), 1 = right.
+ * cfs_halo_bytes: size of one side's message (3 rows x 4 variables, ghost
+ * columns included, the state's storage type).  pack: the 3 interior rows next
+ * to `side` of the current state -> dev_dst (device memory).  unpack: dev_src ->
+ * the 3 ghost rows of `side`.  Both are ordered on the context's stream. */
+int cfs_halo_bytes(cfs_ctx* ctx, long long* bytes);
+int cfs_halo_pack(cfs_ctx* ctx, int side, void* dev_dst);
+int cfs_halo_unpack(cfs_ctx* ctx, int side, const void* dev_src);
+
 /* Waits for the context's stream. */
 int cfs_synchronize(cfs_ctx* ctx);
 
@@ -186,6 +212,39 @@ void* cfs_get_stream(cfs_ctx* ctx);
 /* Sums over fluid cells of rho, rho u, rho v and E times the cell area,
  * accumulated in FP64 (conservation check). */
 int cfs_conserved_totals(cfs_ctx* ctx, double totals[4]);
+
+/* ---- Batched cases -------------------------------------------------------
+ * Hundreds of independent grids of uneven size advanced together: every stage
+ * of every case runs in ONE persistent launch whose blocks pull work items
+ * (case, block column, row chunk) from a device counter, largest cases first;
+ * each case keeps its own CFL time step, computed on the device; whole steps
+ * are replayed from a CUDA graph.  Throughput forms only (CFS_FP32_MIXED,
+ * CFS_FP64).  No reference counterpart (the reference runs one grid). */
+typedef struct cfs_case {
+    int nx, ny;
+    double lx, ly;
+    int bc[4];
+    double bc_prim[4][4];
+    int circle;              /* 1: circle immersed boundary (cfs_ib_build_circle) */
+    double radius, cx, cy;
+    int npoints;
+    int ib_mode;             /* enum cfs_ib_mode */
+    int rows;                /* row chunk of a work item (0: from the tuning default) */
+} cfs_case;
+
+typedef struct cfs_batch cfs_batch;
+
+/* common supplies precision, rk, hll, gamma, weno_eps and device. */
+int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases, cfs_batch** out);
+int cfs_batch_destroy(cfs_batch* b);
+const char* cfs_batch_last_error(const cfs_batch* b);
+int cfs_batch_set_state(cfs_batch* b, int c, const double* U);
+int cfs_batch_get_state(cfs_batch* b, int c, double* U);
+/* nsteps RK steps of every case with per-case CFL dt (cfl > 0) or a common
+ * fixed dt; t (optional, [ncases]) receives each case's simulated time. */
+int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t);
+/* Total cells of the batch and the number of work items of one stage launch. */
+int cfs_batch_info(const cfs_batch* b, long long* cells, int* items);
 
 /* CFL step of a caller-owned device state, for callers that cannot allocate
  * device memory (no counterpart in the reference).  Same dt, bit for bit, as

@@ -175,8 +175,12 @@ int orc_hll(const orc_config* c, const double L4[4], const double R4[4], int dir
 
 /* Interface flux from the 6-cell stencil s[0..5] = cells (a-3 .. a+2) across the
  * face between cells a-1 and a: left state from s[0..4], right state from the
- * reversed s[5..1] (Weno5th.cpp:57-81), then HLL (CellInterface.cpp:68-89). */
-static void face_flux(const orc_config* c, const double s[6][NV], int dir, double F[4]) {
+ * reversed s[5..1] (Weno5th.cpp:57-81), then HLL (CellInterface.cpp:68-89).
+ * Positivity fallbacks (no reference counterpart): ORC_POS_FACE replaces a
+ * state with rho <= 0 or p <= 0 (or NaN) by the cell next to the face on its
+ * side; ORC_POS_BODY also takes both cells' values (first order) when lowo,
+ * i.e. the stencil holds an immersed-ghost or solid cell. */
+static void face_flux(const orc_config* c, const double s[6][NV], int dir, double F[4], int lowo) {
     double sl[5][NV], sr[5][NV], L[5], R[5];
     for (int k = 0; k < 5; ++k)
         for (int q = 0; q < NV; ++q) {
@@ -185,6 +189,18 @@ static void face_flux(const orc_config* c, const double s[6][NV], int dir, doubl
         }
     reconstruct(c, sl, L);
     reconstruct(c, sr, R);
+    if (c->positivity) {
+        /* first-order fallback of a non-physical WENO state: the cell next to
+         * the face on that side (s[2] left, s[3] right) */
+        if (lowo || !(L[0] > 0) || !(L[4] > 0)) {
+            for (int q = 0; q < NV; ++q) L[q] = s[2][q];
+            L[4] = pressure(c->gamma, L[0], L[1], L[2], L[3]);
+        }
+        if (lowo || !(R[0] > 0) || !(R[4] > 0)) {
+            for (int q = 0; q < NV; ++q) R[q] = s[3][q];
+            R[4] = pressure(c->gamma, R[0], R[1], R[2], R[3]);
+        }
+    }
     hll(c, L, R, dir, F);
 }
 
@@ -236,31 +252,46 @@ static void ldlt4_solve(const ldlt4* f, const double b[4], double x[4]) {
     for (int k = 0; k < 4; ++k) x[f->perm[k]] = y[k];
 }
 
-/* Solves M^T w = p by Gaussian elimination with partial pivoting, so that
- * w . f is the bilinear interpolant through the 4 donors evaluated at the
- * image point (no reference counterpart). */
-static void bilinear_weights(const double M[4][4], const double p[4], double w[4]) {
-    double A[4][5];
-    for (int r = 0; r < 4; ++r) {
-        for (int c = 0; c < 4; ++c) A[r][c] = M[c][r];
-        A[r][4] = p[r];
-    }
+/* Slip-form donors (no reference counterpart): bilinear tensor weights over the
+ * 2 x 2 block of cell centres around (X, Y), restricted to fluid cells and
+ * renormalised; inverse-squared-distance weights over the given donors when the
+ * block keeps less than 1e-3 of the weight. */
+static void slip_weights(const orc_config* c, const uint8_t* types, double X, double Y, const int32_t fb[4],
+                         int32_t d[4], double w[4]) {
+    const int nx = c->nx, ny = c->ny;
+    const double dx = c->lx / nx, dy = c->ly / ny;
+    const double fx = (X - 0.5 * dx) / dx, fy = (Y - 0.5 * dy) / dy;
+    const int i0 = (int)floor(fx), j0 = (int)floor(fy);
+    const double tx = fx - i0, ty = fy - j0;
+    double sum = 0.0;
+    int keep = -1;
     for (int k = 0; k < 4; ++k) {
-        int piv = k;
-        for (int r = k + 1; r < 4; ++r)
-            if (fabs(A[r][k]) > fabs(A[piv][k])) piv = r;
-        if (piv != k)
-            for (int c = 0; c < 5; ++c) { double t = A[k][c]; A[k][c] = A[piv][c]; A[piv][c] = t; }
-        for (int r = k + 1; r < 4; ++r) {
-            const double m = A[r][k] / A[k][k];
-            for (int c = k; c < 5; ++c) A[r][c] -= m * A[k][c];
+        const int i = i0 + (k & 1), j = j0 + (k >> 1);
+        const double wk = ((k & 1) ? tx : 1 - tx) * ((k >> 1) ? ty : 1 - ty);
+        const int ok = i >= 0 && i < nx && j >= 0 && j < ny && (!types || types[(size_t)i * ny + j] == ORC_CELL_FLUID);
+        d[k] = ok ? i * ny + j : -1;
+        w[k] = ok ? wk : 0.0;
+        if (ok) {
+            sum += wk;
+            if (keep < 0) keep = k;
         }
     }
-    for (int r = 3; r >= 0; --r) {
-        double s = A[r][4];
-        for (int c = r + 1; c < 4; ++c) s -= A[r][c] * w[c];
-        w[r] = s / A[r][r];
+    if (sum > 1e-3) {
+        for (int k = 0; k < 4; ++k) {
+            if (d[k] < 0) d[k] = d[keep];
+            w[k] /= sum;
+        }
+        return;
     }
+    double s = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const int i = fb[k] / ny, j = fb[k] % ny;
+        const double ex = (i + 0.5) * dx - X, ey = (j + 0.5) * dy - Y;
+        w[k] = 1.0 / (ex * ex + ey * ey + 1e-300);
+        d[k] = fb[k];
+        s += w[k];
+    }
+    for (int k = 0; k < 4; ++k) w[k] /= s;
 }
 
 /* Cell::comImmersedGhostPhase -> ImagePoint::InterpolatePhase
@@ -298,10 +329,13 @@ int orc_ib_fill(const orc_config* c, const orc_ib* ib, double* U) {
             val[1] = -val[1];
             val[2] = -val[2];
         } else {
-            const double p[4] = {X * Y, X, Y, 1.0};
+            int32_t d[4];
             double w[4];
-            bilinear_weights(M, p, w);
-            for (int q = 0; q < NV; ++q) val[q] = w[0] * f[q][0] + w[1] * f[q][1] + w[2] * f[q][2] + w[3] * f[q][3];
+            slip_weights(c, ib->types, X, Y, &ib->donor[4 * g], d, w);
+            for (int q = 0; q < NV; ++q) {
+                val[q] = 0.0;
+                for (int k = 0; k < 4; ++k) val[q] += w[k] * U[(size_t)q * n + (size_t)d[k]];
+            }
             const double nx_ = ib->normal[2 * g], ny_ = ib->normal[2 * g + 1];
             const double mn = val[1] * nx_ + val[2] * ny_;
             val[1] = val[1] - 2.0 * mn * nx_;
@@ -461,22 +495,26 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
     for (int a = 0; a <= nx; ++a)
         for (int j = 0; j < ny; ++j) {
             double s[6][NV], F[4];
+            int lowo = 0;
             for (int k = 0; k < 6; ++k) {
                 const int ii = face_slot(a, k, nx, c->bc[0] == ORC_BC_PERIODIC, c->bc[1] == ORC_BC_PERIODIC);
                 for (int q = 0; q < NV; ++q) s[k][q] = cval(c, U, q, ii, j);
+                if (c->positivity == ORC_POS_BODY && types && ii >= 0 && ii < nx && types[(size_t)ii * ny + j]) lowo = 1;
             }
-            face_flux(c, s, 0, F);
+            face_flux(c, s, 0, F, lowo);
             for (int q = 0; q < NV; ++q) FX[(size_t)q * nfx + (size_t)a * ny + j] = F[q];
         }
 #pragma omp parallel for num_threads(c->nthreads > 0 ? c->nthreads : omp_get_max_threads())
     for (int i = 0; i < nx; ++i)
         for (int a = 0; a <= ny; ++a) {
             double s[6][NV], F[4];
+            int lowo = 0;
             for (int k = 0; k < 6; ++k) {
                 const int jj = face_slot(a, k, ny, c->bc[2] == ORC_BC_PERIODIC, c->bc[3] == ORC_BC_PERIODIC);
                 for (int q = 0; q < NV; ++q) s[k][q] = cval(c, U, q, i, jj);
+                if (c->positivity == ORC_POS_BODY && types && jj >= 0 && jj < ny && types[(size_t)i * ny + jj]) lowo = 1;
             }
-            face_flux(c, s, 1, F);
+            face_flux(c, s, 1, F, lowo);
             for (int q = 0; q < NV; ++q) FY[(size_t)q * nfy + (size_t)i * (ny + 1) + a] = F[q];
         }
 #pragma omp parallel for num_threads(c->nthreads > 0 ? c->nthreads : omp_get_max_threads())
@@ -491,7 +529,6 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
                 rhs[(size_t)q * n + k] = -(f1 - f0) / dx - (f3 - f2) / dy;
             }
         }
-    (void)types;
     free(FX);
     free(FY);
     if (c->viscous) add_ns_terms(c, U, rhs);

@@ -20,6 +20,7 @@ enum { ORC_HLL_REFERENCE = 0, ORC_HLL_DAVIS = 1 };
 enum { ORC_BC_NEUMANN = 0, ORC_BC_DIRICHLET = 1, ORC_BC_PERIODIC = 2 };
 enum { ORC_CELL_FLUID = 0, ORC_CELL_SOLID = 1, ORC_CELL_GHOST = 2 };
 enum { ORC_IB_REFERENCE = 0, ORC_IB_BILINEAR_SLIP = 1 };
+enum { ORC_POS_OFF = 0, ORC_POS_FACE = 1, ORC_POS_BODY = 2 };
 
 typedef struct {
     int nx, ny;
@@ -33,6 +34,7 @@ typedef struct {
     int viscous;          /* 0 off, 1 Navier-Stokes terms added to the RHS */
     double mu, prandtl, mach;
     int nthreads;         /* 0 = OpenMP default */
+    int positivity;       /* ORC_POS_* (face-state fallbacks, see face_flux) */
 } orc_config;
 
 typedef struct {
@@ -42,6 +44,7 @@ typedef struct {
     const double* image;   /* [2n] image point (x, y) */
     const double* normal;  /* [2n] unit wall normal, used by ORC_IB_BILINEAR_SLIP */
     int mode;
+    const uint8_t* types;  /* [nx*ny] cell types, used by ORC_IB_BILINEAR_SLIP (NULL: all fluid) */
 } orc_ib;
 
 /* One RK stage, in the order of one Run::solver iteration (Run.cpp:153-203):

@@ -41,12 +41,14 @@ class OrcConfig(ctypes.Structure):
                 ("gamma", ctypes.c_double), ("weno_eps", ctypes.c_double), ("rk", ctypes.c_int),
                 ("hll", ctypes.c_int), ("bc", ctypes.c_int * 4), ("bc_U", (ctypes.c_double * 4) * 4),
                 ("viscous", ctypes.c_int), ("mu", ctypes.c_double), ("prandtl", ctypes.c_double),
-                ("mach", ctypes.c_double), ("nthreads", ctypes.c_int)]
+                ("mach", ctypes.c_double), ("nthreads", ctypes.c_int),
+                ("positivity", ctypes.c_int)]
 
 
 class OrcIB(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("cell", ctypes.c_void_p), ("donor", ctypes.c_void_p),
-                ("image", ctypes.c_void_p), ("normal", ctypes.c_void_p), ("mode", ctypes.c_int)]
+                ("image", ctypes.c_void_p), ("normal", ctypes.c_void_p), ("mode", ctypes.c_int),
+                ("types", ctypes.c_void_p)]
 
 
 def ensure_built() -> None:
@@ -115,9 +117,10 @@ def make_ref_config(nx, ny, lx=1.0, ly=1.0, integrator=3, dt=1e-3, cfl=0.0, bc=(
 
 
 def make_orc_config(nx, ny, lx=1.0, ly=1.0, rk=RK_TVD3_REFERENCE, hll=0, bc=(0, 0, 0, 0), bc_prim=None,
-                    weno_eps=1e-2, viscous=0, mu=1e-3, prandtl=0.72, mach=1.0, nthreads=0) -> OrcConfig:
+                    weno_eps=1e-2, viscous=0, mu=1e-3, prandtl=0.72, mach=1.0, nthreads=0,
+                    positivity=0) -> OrcConfig:
     c = OrcConfig(nx=nx, ny=ny, lx=lx, ly=ly, gamma=GAMMA, weno_eps=weno_eps, rk=rk, hll=hll, viscous=viscous,
-                  mu=mu, prandtl=prandtl, mach=mach, nthreads=nthreads)
+                  mu=mu, prandtl=prandtl, mach=mach, nthreads=nthreads, positivity=positivity)
     for s in range(4):
         c.bc[s] = int(bc[s])
         cons = dirichlet_conserved(bc_prim[s] if bc_prim is not None else (1.0, 0.0, 0.0, 1.0))
@@ -155,7 +158,8 @@ def ref_ib_info(nx, ny, lx, ly, circle, npoints=400, max_ig=200000):
 class OrcIBList:
     """Keeps the arrays of an OrcIB alive."""
 
-    def __init__(self, cells, donors, images, normals=None, mode=0):
+    def __init__(self, cells, donors, images, normals=None, mode=0, types=None):
+        self.types = None if types is None else np.ascontiguousarray(types, dtype=np.uint8).ravel()
         self.cells = np.ascontiguousarray(cells, dtype=np.int32)
         self.donors = np.ascontiguousarray(donors, dtype=np.int32).ravel()
         self.images = np.ascontiguousarray(images, dtype=np.float64).ravel()
@@ -163,7 +167,8 @@ class OrcIBList:
         self.normals = (np.zeros(2 * n) if normals is None
                         else np.ascontiguousarray(normals, dtype=np.float64).ravel())
         self.s = OrcIB(n=n, cell=self.cells.ctypes.data, donor=self.donors.ctypes.data,
-                       image=self.images.ctypes.data, normal=self.normals.ctypes.data, mode=mode)
+                       image=self.images.ctypes.data, normal=self.normals.ctypes.data, mode=mode,
+                       types=None if self.types is None else self.types.ctypes.data)
 
 
 def orc_run(cfg: OrcConfig, U0, first, count, dt=1e-3, cfl=0.0, types=None, ib: OrcIBList | None = None):

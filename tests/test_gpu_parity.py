@@ -186,9 +186,12 @@ def test_fp64_full_quadrant_run_tracks_oracle(cfsb, workloads):
 
 # -------------------------------------------------- FP32-mixed form
 def test_fp32_mixed_error_and_conservation(cfsb, workloads):
-    """Smooth periodic advection, 128^2 to t = 0.5 with a fixed dt: density L1
-    error against the FP64 path <= 1e-5, mass/energy drift <= 1e-6 relative."""
-    n = 128
+    """Smooth periodic advection, 256^2 to t = 0.5 (about 1,500 steps) with a
+    fixed dt: density L1 error against the FP64 path <= 2e-6 (the FP32 storage
+    rounding floor is a few 1e-7 here; a systematic per-step bias of 3e-8 --
+    RK coefficients that do not sum to 1 in FP32 -- would already give ~6e-6),
+    mass/energy drift <= 1e-6 relative."""
+    n = 256
     w = workloads.smooth_advection(n)
     kw = dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=(2, 2, 2, 2))
     cfg = ob.make_orc_config(n, n, rk=2, hll=1, bc=(2, 2, 2, 2))
@@ -204,10 +207,35 @@ def test_fp32_mixed_error_and_conservation(cfsb, workloads):
             out[prec] = (s.get_state(), m0, s.totals())
     U64, U32 = out[cfsb.FP64][0], out[cfsb.FP32_MIXED][0]
     l1 = np.abs(U32[0] - U64[0]).mean()
-    assert l1 <= 1e-5, l1
+    assert l1 <= 2e-6, l1
     _, m0, m1 = out[cfsb.FP32_MIXED]
     assert abs(m1[0] - m0[0]) / abs(m0[0]) <= 1e-6
     assert abs(m1[3] - m0[3]) / abs(m0[3]) <= 1e-6
     # and the FP64 path converges to the exact solution
     exact = workloads.smooth_advection_exact(n, 0.5)
     assert np.abs(U64[0] - exact).mean() < 1e-4
+
+
+def test_fp64_slip_cylinder_per_step(cfsb, workloads):
+    """Mach-3 cylinder (2 x 1 domain, 256 x 128), slip-wall immersed boundary,
+    SSP-RK3 + Davis HLL: per-step relative L-infinity <= 1e-12 against the oracle."""
+    nx, ny = 256, 128
+    w = workloads.mach3_cylinder(nx, ny)
+    types, cells, donors, images, normals = cfsb.circle_setup(nx, ny, 2.0, 1.0, *w.circle, 400)
+    U = w.U0.copy()  # freestream in the body too: solid cells stay inside the fluid stencils
+    cfg = ob.make_orc_config(nx, ny, lx=2.0, ly=1.0, rk=2, hll=1, bc=w.bc, bc_prim=w.bc_prim)
+    ib = ob.OrcIBList(cells, donors, images, normals, mode=1, types=types)
+    worst = 0.0
+    with cfsb.Solver(nx, ny, 2.0, 1.0, precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=w.bc,
+                     bc_prim=w.bc_prim) as s:
+        s.build_circle(*w.circle, 400, cfsb.IB_BILINEAR_SLIP)
+        for _ in range(10):
+            dt = ob.orc_cfl_dt(cfg, U, 0.5, types)
+            s.set_state(U)
+            s.step(dt)
+            got = s.get_state()
+            ref, _ = ob.orc_run(cfg, U, 1, 3, dt=dt, types=types, ib=ib)
+            assert np.all(np.isfinite(ref))
+            worst = max(worst, _rel_linf(got, ref))
+            U = ref
+    assert worst <= 1e-12, worst
