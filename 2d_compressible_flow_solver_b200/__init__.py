@@ -38,6 +38,8 @@ BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC, BC_HALO = 0, 1, 2, 3
 CELL_FLUID, CELL_SOLID, CELL_IMMERSED_GHOST = 0, 1, 2
 IB_REFERENCE, IB_BILINEAR_SLIP = 0, 1
 VISCOUS_OFF, VISCOUS_NS = 0, 1
+POSITIVITY_OFF, POSITIVITY_FACE, POSITIVITY_BODY = 0, 1, 2
+ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _c_int32_p = ctypes.POINTER(ctypes.c_int32)
@@ -56,6 +58,7 @@ class CfsConfig(ctypes.Structure):
         ("viscous", ctypes.c_int),
         ("mu", ctypes.c_double), ("prandtl", ctypes.c_double), ("mach", ctypes.c_double),
         ("keep_rhs", ctypes.c_int), ("device", ctypes.c_int), ("variant", ctypes.c_int),
+        ("positivity", ctypes.c_int), ("rounding", ctypes.c_int),
     ]
 
 
@@ -85,7 +88,7 @@ _SIGNATURES = {
     "cfs_abi_version": (ctypes.c_int, []),
     "cfs_variant_count": (ctypes.c_int, []),
     "cfs_variant_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                                        ctypes.POINTER(ctypes.c_int)]),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "cfs_config_default": (None, [ctypes.POINTER(CfsConfig)]),
     "cfs_create": (ctypes.c_int, [ctypes.POINTER(CfsConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "cfs_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -153,14 +156,14 @@ def load_library() -> ctypes.CDLL:
     return _lib
 
 
-def variants() -> list[tuple[int, int, int]]:
-    """(rows, warps, min_blocks) of every stage-kernel variant, index v-1."""
+def variants() -> list[tuple[int, int, int, int]]:
+    """(rows, warps, min_blocks, prefetch) of every stage-kernel variant, index v-1."""
     lib = load_library()
     out = []
     for v in range(1, lib.cfs_variant_count() + 1):
-        r, w, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        lib.cfs_variant_info(v, ctypes.byref(r), ctypes.byref(w), ctypes.byref(b))
-        out.append((r.value, w.value, b.value))
+        r, w, b, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib.cfs_variant_info(v, ctypes.byref(r), ctypes.byref(w), ctypes.byref(b), ctypes.byref(p))
+        out.append((r.value, w.value, b.value, p.value))
     return out
 
 
@@ -202,7 +205,7 @@ class Solver:
                  rk: int = RK_TVD3_REFERENCE, hll: int = HLL_REFERENCE, bc=(BC_NEUMANN,) * 4, bc_prim=None,
                  gamma: float = 1.4, weno_eps: float = 1e-2, viscous: int = VISCOUS_OFF, mu: float = 1e-3,
                  prandtl: float = 0.72, mach: float = 1.0, keep_rhs: bool = False, device: int = 0,
-                 variant: int = 0):
+                 variant: int = 0, positivity: int = 0, rounding: int = ROUND_STOCHASTIC):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
@@ -216,6 +219,7 @@ class Solver:
                     cfg.bc_prim[s][q] = float(bc_prim[s][q])
         cfg.viscous, cfg.mu, cfg.prandtl, cfg.mach = int(viscous), float(mu), float(prandtl), float(mach)
         cfg.keep_rhs, cfg.device, cfg.variant = int(bool(keep_rhs)), int(device), int(variant)
+        cfg.positivity, cfg.rounding = int(positivity), int(rounding)
         self.config = cfg
         self.nx, self.ny = int(nx), int(ny)
         self._ctx = ctypes.c_void_p()
@@ -369,12 +373,14 @@ class Batch:
     persistent launch per stage for all cases, per-case CFL dt on the device."""
 
     def __init__(self, cases, *, precision: int = FP32_MIXED, rk: int = RK_SSP3, hll: int = HLL_DAVIS,
-                 gamma: float = 1.4, weno_eps: float = 1e-2, device: int = 0):
+                 gamma: float = 1.4, weno_eps: float = 1e-2, device: int = 0, positivity: int = POSITIVITY_OFF,
+                 rounding: int = ROUND_STOCHASTIC):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
         cfg.precision, cfg.rk, cfg.hll, cfg.gamma, cfg.weno_eps, cfg.device = (
             int(precision), int(rk), int(hll), float(gamma), float(weno_eps), int(device))
+        cfg.positivity, cfg.rounding = int(positivity), int(rounding)
         arr = (CfsCase * len(cases))()
         self.shapes = []
         for k, c in enumerate(cases):

@@ -33,6 +33,8 @@ struct cfs_ctx {
     double* staging = nullptr;
     void* rv = nullptr;   // viscous RHS [3][nx][ny] (Navier-Stokes form only)
     uint8_t* types_d = nullptr;
+    uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
+    unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
     bool has_types = false;
     std::vector<uint8_t> types_h;
     // immersed ghosts
@@ -108,6 +110,18 @@ int validate(const cfs_config* g, std::string& msg) {
         }
     if (g->viscous != CFS_VISCOUS_OFF && g->viscous != CFS_VISCOUS_NS) { msg = "unknown viscous mode"; return CFS_ERR_INVALID; }
     if (g->variant < 0 || g->variant > cfs::kNumVariants) { msg = "unknown kernel variant"; return CFS_ERR_INVALID; }
+    if (g->positivity < CFS_POSITIVITY_OFF || g->positivity > CFS_POSITIVITY_BODY) {
+        msg = "unknown positivity mode";
+        return CFS_ERR_INVALID;
+    }
+    if (g->rounding != CFS_ROUND_STOCHASTIC && g->rounding != CFS_ROUND_NEAREST) {
+        msg = "unknown rounding mode";
+        return CFS_ERR_INVALID;
+    }
+    if (g->precision == CFS_FP64_EXACT && g->positivity != CFS_POSITIVITY_OFF) {
+        msg = "FP64_EXACT runs the reference's scheme: positivity fallbacks need FP64 or FP32_MIXED";
+        return CFS_ERR_INVALID;
+    }
     if (g->viscous == CFS_VISCOUS_NS && (!(g->mu >= 0) || !(g->prandtl > 0) || !(g->mach > 0))) {
         msg = "viscous terms need mu >= 0, prandtl > 0 and mach > 0";
         return CFS_ERR_INVALID;
@@ -131,6 +145,10 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.mach = c->cfg.mach;
     a.types = c->has_types ? c->types_d : nullptr;
     a.variant = c->cfg.variant;
+    a.positivity = c->cfg.positivity;
+    a.rounding = c->cfg.rounding;
+    a.seed = c->steps_done;
+    a.lowo = c->cfg.positivity == CFS_POSITIVITY_BODY && c->has_types ? c->lowo_d : nullptr;
     return a;
 }
 
@@ -216,6 +234,7 @@ int run_stage(cfs_ctx* c, int stage, double dt) {
     if (stage == 1) c->u1_idx = r.u1;
     c->cur = r.out;
     c->next_stage = (stage + 1) % stages_per_step(c->cfg.rk);
+    if (c->next_stage == 0) ++c->steps_done;
     return CFS_OK;
 }
 
@@ -296,11 +315,12 @@ int cfs_abi_version(void) { return CFS_ABI_VERSION; }
 
 int cfs_variant_count(void) { return cfs::kNumVariants; }
 
-int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks) {
+int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks, int* prefetch) {
     if (v < 1 || v > cfs::kNumVariants) return fail(nullptr, CFS_ERR_INVALID, "unknown kernel variant");
     if (rows) *rows = cfs::kVariants[v - 1].rows;
     if (warps) *warps = cfs::kVariants[v - 1].warps;
     if (min_blocks) *min_blocks = cfs::kVariants[v - 1].min_blocks;
+    if (prefetch) *prefetch = cfs::kVariants[v - 1].prefetch ? 1 : 0;
     return CFS_OK;
 }
 
@@ -396,6 +416,7 @@ int cfs_destroy(cfs_ctx* c) {
     cudaFree(c->staging);
     cudaFree(c->rv);
     cudaFree(c->types_d);
+    cudaFree(c->lowo_d);
     cudaFree(c->ib_cell);
     cudaFree(c->ib_donor);
     cudaFree(c->ib_perm);
@@ -466,6 +487,11 @@ int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
     CFS_CUDA(c, cudaMemcpy(c->types_d, types, n, cudaMemcpyHostToDevice));
     c->types_h.assign(types, types + n);
     c->has_types = true;
+    if (c->cfg.positivity == CFS_POSITIVITY_BODY) {
+        const std::vector<uint8_t> f = cfs::low_order_faces(types, c->cfg.nx, c->cfg.ny, c->cfg.bc);
+        if (!c->lowo_d) CFS_CUDA(c, cudaMalloc(&c->lowo_d, f.size()));
+        CFS_CUDA(c, cudaMemcpy(c->lowo_d, f.data(), f.size(), cudaMemcpyHostToDevice));
+    }
     return CFS_OK;
 }
 
@@ -594,6 +620,7 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     hp.use_cfl = cfl > 0 ? 1 : 0;
     hp.cfl = cfl;
     hp.dt_fixed = dt;
+    hp.seed[0] = hp.seed[1] = c->steps_done;
     CFS_CUDA(c, cudaMemcpyAsync(c->P, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
     if (hp.use_cfl) {
         if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[0]), c->stream));
@@ -641,6 +668,7 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     if (t_elapsed) *t_elapsed = out.t;
     if (dt_last) *dt_last = out.dt_last;
+    c->steps_done += static_cast<unsigned int>(nsteps);
     if (nsteps > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
         return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
     return CFS_OK;

@@ -29,6 +29,8 @@ struct BatchCase {
     long long types_off = -1;
     int rows = 32, nseg = 0, items_x = 0, items_y = 0;
     std::vector<uint8_t> types;
+    std::vector<uint8_t> lowo;   // CFS_POSITIVITY_BODY face flags, [nx+1][ny+1]
+    long long lowo_off = -1;
     int ib_n = 0, ib_mode = 0;
     int ib_first = 0;       // first immersed-ghost index in the flattened lists
 };
@@ -44,6 +46,7 @@ struct cfs_batch {
     cudaStream_t stream = nullptr;
     char* arena = nullptr;
     uint8_t* types_d = nullptr;
+    uint8_t* lowo_d = nullptr;
     int total_ig = 0;
     int* ib_cell = nullptr;
     int* ib_donor = nullptr;
@@ -65,6 +68,7 @@ struct cfs_batch {
     int grid = 0;
     long long total_cells = 0;
     bool args_dirty = true;
+    unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
     cudaGraphExec_t graph2 = nullptr;
     std::string err;
 };
@@ -113,6 +117,9 @@ int upload_args(cfs_batch* b) {
                 a.rk = b->common.rk;
                 a.hll = b->common.hll;
                 a.types = c.types_off >= 0 ? b->types_d + c.types_off : nullptr;
+                a.positivity = b->common.positivity;
+                a.rounding = b->common.rounding;
+                a.lowo = c.lowo_off >= 0 ? b->lowo_d + c.lowo_off : nullptr;
                 a.stage = s;
                 // buffer roles of a step that starts in S0 (as cfs_advance)
                 int in = 0, out = 1, u0 = 0, u1 = -1;
@@ -187,6 +194,7 @@ int cfs_batch_destroy(cfs_batch* b) {
     if (b->graph2) cudaGraphExecDestroy(b->graph2);
     cudaFree(b->arena);
     cudaFree(b->types_d);
+    cudaFree(b->lowo_d);
     cudaFree(b->ib_cell);
     cudaFree(b->ib_donor);
     cudaFree(b->ib_perm);
@@ -217,6 +225,10 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         !(common->weno_eps > 0))
         return bfail(nullptr, CFS_ERR_INVALID, "bad common configuration");
     if (common->viscous != CFS_VISCOUS_OFF) return bfail(nullptr, CFS_ERR_INVALID, "batches are inviscid");
+    if (common->positivity < CFS_POSITIVITY_OFF || common->positivity > CFS_POSITIVITY_BODY)
+        return bfail(nullptr, CFS_ERR_INVALID, "unknown positivity mode");
+    if (common->rounding != CFS_ROUND_STOCHASTIC && common->rounding != CFS_ROUND_NEAREST)
+        return bfail(nullptr, CFS_ERR_INVALID, "unknown rounding mode");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return bfail(nullptr, CFS_ERR_CUDA, "no CUDA device available (the engine has no CPU path)");
@@ -236,7 +248,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         return bail(CFS_ERR_CUDA, "stream creation failed");
 
     // --- per-case layout, boundaries, immersed boundary (host)
-    size_t arena = 0, types_bytes = 0, max_cells = 0;
+    size_t arena = 0, types_bytes = 0, lowo_bytes = 0, max_cells = 0;
     std::vector<int32_t> h_cell, h_donor, h_perm, h_igc, h_igl;
     std::vector<double> h_img, h_fac;
     for (int ci = 0; ci < ncases; ++ci) {
@@ -281,6 +293,11 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
             c.types = ib.types;
             c.types_off = static_cast<long long>(types_bytes);
             types_bytes += c.types.size();
+            if (common->positivity == CFS_POSITIVITY_BODY) {
+                c.lowo = cfs::low_order_faces(c.types.data(), d.nx, d.ny, d.bc);
+                c.lowo_off = static_cast<long long>(lowo_bytes);
+                lowo_bytes += c.lowo.size();
+            }
             c.ib_n = static_cast<int>(ib.cell.size());
             c.ib_mode = d.ib_mode;
             c.ib_first = static_cast<int>(h_cell.size());
@@ -327,6 +344,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     auto dalloc = [&](void** p, size_t bytes) { return bytes == 0 || cudaMalloc(p, bytes) == cudaSuccess; };
     if (!dalloc(reinterpret_cast<void**>(&b->arena), arena)) return bail(CFS_ERR_NOMEM, "state arena allocation failed");
     if (!dalloc(reinterpret_cast<void**>(&b->types_d), types_bytes) ||
+        !dalloc(reinterpret_cast<void**>(&b->lowo_d), lowo_bytes) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_cell), sizeof(int) * h_cell.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_donor), sizeof(int) * h_donor.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_perm), sizeof(int) * h_perm.size()) ||
@@ -350,6 +368,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     bool ok = cudaMemset(b->arena, 0, arena) == cudaSuccess;
     for (const BatchCase& c : b->cases)
         if (c.types_off >= 0) ok = ok && h2d(b->types_d + c.types_off, c.types.data(), c.types.size());
+    for (const BatchCase& c : b->cases)
+        if (c.lowo_off >= 0) ok = ok && h2d(b->lowo_d + c.lowo_off, c.lowo.data(), c.lowo.size());
     ok = ok && h2d(b->ib_cell, h_cell.data(), sizeof(int) * h_cell.size()) &&
          h2d(b->ib_donor, h_donor.data(), sizeof(int) * h_donor.size()) &&
          h2d(b->ib_perm, h_perm.data(), sizeof(int) * h_perm.size()) &&
@@ -425,6 +445,7 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
     for (auto& p : hp) {
         p = cfs::DevParams{};
         p.use_cfl = cfl > 0 ? 1 : 0;
+        p.seed[0] = p.seed[1] = b->steps_done;
         p.cfl = cfl;
         p.dt_fixed = dt;
     }
@@ -462,6 +483,7 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
     }
     CFSB_CUDA(b, cudaMemcpyAsync(hp.data(), b->P, sizeof(cfs::DevParams) * b->n, cudaMemcpyDeviceToHost, b->stream));
     CFSB_CUDA(b, cudaStreamSynchronize(b->stream));
+    b->steps_done += static_cast<unsigned int>(nsteps);
     for (int ci = 0; ci < b->n; ++ci) {
         if (t) t[ci] = hp[ci].t;
         if (nsteps > 0 && (!(hp[ci].dt_last > 0) || !std::isfinite(hp[ci].dt_last)))

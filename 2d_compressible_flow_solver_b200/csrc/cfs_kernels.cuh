@@ -267,6 +267,44 @@ __device__ __forceinline__ double rk_update(int rk, int stage, double dt, double
     return (1.0 / 3.0) * u0v + (2.0 / 3.0) * cur + (2.0 / 3.0) * dt * r;
 }
 
+// ------------------------------------------------------ stochastic rounding
+// FP32 storage of the FP32-mixed form rounds each new state value
+// stochastically (no reference counterpart): to one of the two floats around
+// the exact FP64 value, the farther one with probability proportional to its
+// nearness.  Round-to-nearest biases the error of a smooth, slowly moving
+// state (neighbouring cells and steps round the same way), so it grows with
+// the step count; stochastic rounding leaves an unbiased random walk.
+// Random bits: MurmurHash3's 32-bit finaliser (public domain) of cell and step.
+__device__ __forceinline__ unsigned int fmix32(unsigned int h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ unsigned int cell_hash(int i, int j, unsigned int step_seed) {
+    return fmix32(static_cast<unsigned int>(i) * 0x9e3779b1u ^ fmix32(static_cast<unsigned int>(j) ^ (step_seed * 0x632be5abu)));
+}
+
+// The float next to f (finite) in the direction of sign(dir).
+__device__ __forceinline__ float float_step(float f, double dir) {
+    if (f == 0.0f) return dir > 0 ? 1.401298464e-45f : -1.401298464e-45f;
+    const unsigned int b = __float_as_uint(f);
+    return __uint_as_float((f > 0.0f) == (dir > 0) ? b + 1u : b - 1u);
+}
+
+// x rounded to float stochastically with the 8 random bits u8.
+__device__ __forceinline__ float round_stochastic(double x, unsigned int u8) {
+    const float f = __double2float_rn(x);
+    const double e = x - double(f);  // exact
+    if (!(fabs(e) > 0.0) || !isfinite(f)) return f;
+    const float n = float_step(f, e);
+    const double gap = fabs(double(n) - double(f));
+    return (double(u8) + 0.5) * (1.0 / 256.0) * gap < fabs(e) ? n : f;
+}
+
 // (|u| + a)/dx + (|v| + a)/dy of one cell, FP64, in the order of the CFL
 // reduction every caller shares.
 __device__ __forceinline__ double wave_sum(double rho, double mx, double my, double E, double g, double dx, double dy) {

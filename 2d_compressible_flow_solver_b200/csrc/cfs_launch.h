@@ -32,15 +32,17 @@ cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const doub
 // Stage-kernel variants of the throughput forms (march_kernel template shapes).
 struct MarchVariant {
     int rows, warps, min_blocks;
+    bool prefetch;  // software-prefetching form of the row march
 };
-constexpr int kNumVariants = 6;
+constexpr int kNumVariants = 10;
 constexpr MarchVariant kVariants[kNumVariants] = {
-    {64, 4, 1}, {64, 4, 4}, {64, 4, 5}, {32, 4, 5}, {128, 4, 4}, {64, 8, 2},
+    {64, 4, 1, false}, {64, 4, 4, false}, {64, 4, 5, false}, {32, 4, 5, false}, {128, 4, 4, false},
+    {64, 8, 2, false}, {64, 4, 4, true},  {32, 4, 5, true},  {64, 4, 3, true},  {64, 8, 2, true},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).
-constexpr int kDefaultVariantF32 = 4;
-constexpr int kDefaultVariantF64 = 2;
+constexpr int kDefaultVariantF32 = 6;
+constexpr int kDefaultVariantF64 = 6;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
 constexpr int kBatchWarps = 4;

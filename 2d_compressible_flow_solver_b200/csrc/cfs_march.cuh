@@ -92,10 +92,37 @@ __device__ __forceinline__ void boundary_face_states(const typename Pol::C c[kVa
     finish_state<Pol>(R, g);
 }
 
+// Positivity fallbacks (no reference counterpart).  A face state is admissible
+// when rho > 0 and p > 0 (NaN fails); otherwise, or when the face is flagged
+// low order, it becomes the value of the cell next to the face on its side.
+template <class Pol>
+__device__ __forceinline__ bool admissible(const Face5<typename Pol::C>& s) {
+    return s.r > typename Pol::C(0) && s.p > typename Pol::C(0);
+}
+
+template <class Pol>
+__device__ __forceinline__ void first_order_state(const typename Pol::C c[kVars], double g, Face5<typename Pol::C>& s) {
+    s.r = c[0];
+    s.mx = c[1];
+    s.my = c[2];
+    s.E = c[3];
+    finish_state<Pol>(s, g);
+}
+
+template <class Pol>
+__device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C cl[kVars], const typename Pol::C cr[kVars],
+                                               double g, Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+    if (low || !admissible<Pol>(L)) first_order_state<Pol>(cl, g, L);
+    if (low || !admissible<Pol>(R)) first_order_state<Pol>(cr, g, R);
+}
+
 // One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
 // block column bx.  Every thread of the block calls it (it ends with a block
-// reduction when the CFL maximum is accumulated).
-template <class Pol, int kWarps>
+// reduction when the CFL maximum is accumulated).  kPf: software prefetch -
+// the next row two iterations ahead, the y halo columns one row ahead, and the
+// RK operands of the row being updated before its x reconstruction - so that
+// global-load latency overlaps a row of arithmetic.
+template <class Pol, int kWarps, bool kPf = false>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][kVars][36], double* wred) {
     using T = typename Pol::T;
@@ -118,20 +145,24 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     // FP32 update coefficients of this stage: new = cA x0 + cB x1 + (c dt) R with
     // x0 = U^0 (or the current state at stage 0), x1 = U^1 (TVD3 as written,
     // stage 2) or the current state (TVD2rdRK.h:16-19, TVD3rdRK.h:14-18).
-    float cA = 1.0f, cB = 0.0f, cdt = float(dt);
+    float cA = 1.0f, cB = 0.0f;
+    double cdtd = dt;  // dt coefficient of the stage, FP64
     bool x1_u1 = false;
     if (a.stage == 1) {
-        if (a.rk == kRkTvd2) { cA = 0.5f; cB = 0.5f; cdt = float(0.5 * dt); }
-        else { cA = 0.75f; cB = 0.25f; cdt = float(0.25 * dt); }
+        if (a.rk == kRkTvd2) { cA = 0.5f; cB = 0.5f; cdtd = 0.5 * dt; }
+        else { cA = 0.75f; cB = 0.25f; cdtd = 0.25 * dt; }
     } else if (a.stage == 2) {
         // cA + cB must be exactly 1 in FP32, else the deviation form scales the
         // stored deviations by (cA + cB) every step: cB = fl(2/3), cA = 1 - cB
         // (an exact FP32 subtraction).
         cB = float(2.0 / 3.0);
         cA = 1.0f - cB;
-        cdt = float((2.0 / 3.0) * dt);
+        cdtd = (2.0 / 3.0) * dt;
         x1_u1 = a.rk == kRkTvd3Ref;
     }
+    const float cdt = float(cdtd);
+    const bool sr = Pol::kMixed && a.rounding == 0;
+    const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
     const bool lo_x = a.bc[0] == kNeumann || a.bc[0] == kDirichlet;
     const bool hi_x = a.bc[1] == kNeumann || a.bc[1] == kDirichlet;
     const bool lo_y = a.bc[2] == kNeumann || a.bc[2] == kDirichlet;
@@ -140,6 +171,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         a.P->wmax[1 - a.parity] = 0ull;
         a.P->t += dt;
         a.P->dt_last = dt;
+        a.P->seed[1 - a.parity] = a.P->seed[a.parity] + 1u;
     }
     const bool active_warp = j0 < L.ny;  // uniform per warp
 
@@ -154,7 +186,36 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
     };
 
+    auto load_halo = [&](int r, C h[kVars]) {
+        if (lane < 2 || lane >= 30) {  // halo columns j0-3, j0-2 and j0+31, j0+32
+            const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
+            if (hc <= L.ny + kGhost - 1) {
+                const long long off = L.offset(r, hc);
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) h[v] = decc<T, C>(in[v * L.plane + off], L, v);
+            } else {
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) h[v] = C(0);
+            }
+        }
+    };
+    // RK operands of cell (i, j): fluid flag, the stored value (FP32 form), U^0.
+    // (U^1, read by the reference's TVD3 stage 2 only, is loaded at its use.)
+    bool pf_fluid = true;
+    T pf_cur[kVars], pf_u0[kVars];
+    auto load_update = [&](int i) {
+        const long long off = L.offset(i, j);
+        pf_fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) {
+            pf_cur[v] = Pol::kMixed ? in[v * L.plane + off] : T(0);
+            pf_u0[v] = a.stage >= 1 ? static_cast<const T*>(a.u0)[v * L.plane + off] : T(0);
+        }
+    };
+
     C win[5][kVars];
+    C nxt[kVars];   // kPf: the row after win[4]
+    C hal[kVars];   // kPf: halo columns of the next y row
     Face5<C> Lx{};                             // left x-state of the previous row
     C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
     C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
@@ -162,8 +223,15 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     if (active_warp) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) load_row(i0 - 3 + k, win[k]);
+        if constexpr (kPf) {
+            load_row(i0 + 2, nxt);
+            load_halo(i0, hal);
+        }
     }
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
+        if constexpr (kPf) {
+            if (r - 1 >= i0 && owner) load_update(r - 1);
+        }
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
         cell_states<Pol>(win, eps, g, Lr, Rr);
@@ -173,13 +241,18 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             Face5<C> Rf = Rr;
             if (r == 0 && lo_x) boundary_face_states<Pol>(win[2], win[1], true, eps, g, Lf, Rf);
             else if (r == L.nx && hi_x) boundary_face_states<Pol>(win[1], win[2], false, eps, g, Lf, Rf);
+            if (a.positivity) {
+                const bool low = a.lowo && j >= 0 && j < L.ny && r <= L.nx &&
+                                 (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j] & 1);
+                positivity_fix<Pol>(low, win[1], win[2], g, Lf, Rf);
+            }
             hll_flux<Pol>(Lf, Rf, 0, a.hll, g, FX);
             // ---- update of row r-1 (its upper x-face is r - 1/2)
             const int i = r - 1;
             if (i >= i0 && owner) {
-                const bool fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+                if constexpr (!kPf) load_update(i);
+                const bool fluid = pf_fluid;
                 const long long off = L.offset(i, j);
-                const T* u0 = static_cast<const T*>(a.u0);
                 const T* u1 = static_cast<const T*>(a.u1);
                 T* out = static_cast<T*>(a.out);
                 double nv[kVars];
@@ -187,18 +260,26 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 if constexpr (Pol::kMixed) {
                     // FP32 update of the stored deviations (value - off): the RK
                     // coefficients of a stage sum to 1, so the offsets cancel and
-                    // the rounding step is that of the deviation.
+                    // the rounding step is that of the deviation.  Stochastic
+                    // rounding forms the new deviation exactly in FP64 (float
+                    // products are exact there) and rounds it once.
+                    const unsigned int h = sr && fluid ? cell_hash(i, j, step_seed) : 0u;
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
                         if (a.rv && v >= 1)
                             rvf += static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
-                        const float cur = in[v * L.plane + off];
+                        const float cur = pf_cur[v];
                         float nd = cur;
                         if (fluid) {
-                            const float x0 = a.stage == 0 ? cur : u0[v * L.plane + off];
+                            const float x0 = a.stage == 0 ? cur : pf_u0[v];
                             const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
-                            nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
+                            if (sr) {
+                                const double tot = fma(cdtd, double(rvf), fma(double(cA), double(x0), double(cB) * double(x1)));
+                                nd = round_stochastic(tot, (h >> (8 * v)) & 255u);
+                            } else {
+                                nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
+                            }
                         }
                         sv[v] = nd;
                         nv[v] = double(nd) + double(L.off[v]);
@@ -213,7 +294,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         const double cur = double(win[1][v]);
                         double val = cur;
                         if (fluid) {
-                            const double u0v = a.stage >= 1 ? dec<T>(u0[v * L.plane + off], L, v) : 0.0;
+                            const double u0v = a.stage >= 1 ? dec<T>(pf_u0[v], L, v) : 0.0;
                             const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
                             val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
                         }
@@ -234,17 +315,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             C* rb = &rbuf[wid][0][0];
 #pragma unroll
             for (int v = 0; v < kVars; ++v) rb[v * 36 + lane + 2] = win[2][v];
-            if (lane < 2 || lane >= 30) {  // halo columns j0-3, j0-2 and j0+31, j0+32
-                const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
+            if constexpr (!kPf) load_halo(r, hal);
+            if (lane < 2 || lane >= 30) {
                 const int slot = lane < 2 ? lane : lane + 4;
-                if (hc <= L.ny + kGhost - 1) {
-                    const long long off = L.offset(r, hc);
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = decc<T, C>(in[v * L.plane + off], L, v);
-                } else {
-#pragma unroll
-                    for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = C(0);
-                }
+                for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = hal[v];
             }
             __syncwarp();
             C st[5][kVars];
@@ -275,6 +350,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 for (int v = 0; v < kVars; ++v) { cc[v] = st[2][v]; gg[v] = st[3][v]; }
                 boundary_face_states<Pol>(cc, gg, false, eps, g, Ly, Rn);
             }
+            if (a.positivity) {
+                const bool low = a.lowo && j >= -1 && j < L.ny &&
+                                 (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j + 1] & 2);
+                positivity_fix<Pol>(low, st[2], st[3], g, Ly, Rn);
+            }
             C FY[kVars];
             hll_flux<Pol>(Ly, Rn, 1, a.hll, g, FY);
 #pragma unroll
@@ -293,7 +373,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             for (int k = 0; k < 4; ++k)
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[k][v] = win[k + 1][v];
-            load_row(r + 3, win[4]);
+            if constexpr (kPf) {
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) win[4][v] = nxt[v];
+                if (r + 4 <= i1 + 2) load_row(r + 4, nxt);
+                if (r + 1 < i1) load_halo(r + 1, hal);
+            } else {
+                load_row(r + 3, win[4]);
+            }
         }
     }
     if (a.P && a.last_stage && a.P->use_cfl) {
@@ -310,11 +397,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     }
 }
 
-template <class Pol, int kRows, int kWarps, int kMinBlocks>
+template <class Pol, int kRows, int kWarps, int kMinBlocks, bool kPf>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ typename Pol::C rbuf[kWarps][kVars][36];
     __shared__ double wred[kWarps];
-    march_item<Pol, kWarps>(a, blockIdx.x, blockIdx.y, kRows, rbuf, wred);
+    march_item<Pol, kWarps, kPf>(a, blockIdx.x, blockIdx.y, kRows, rbuf, wred);
 }
 
 // Persistent batched form: one launch runs one stage of every case of a batch.

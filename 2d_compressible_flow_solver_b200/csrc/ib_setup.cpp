@@ -247,4 +247,35 @@ void ib_factors(int mode, const uint8_t* types, int nx, int ny, double dx, doubl
     }
 }
 
+static inline int face_slot(int a, int k, int n, bool lo_rule, bool hi_rule) {
+    int i = a - 3 + k;
+    if (a == 0 && lo_rule && k >= 3) i = 0;
+    if (a == n && hi_rule && k <= 2) i = n - 1;
+    return i;
+}
+
+std::vector<uint8_t> low_order_faces(const uint8_t* types, int nx, int ny, const int bc[4]) {
+    auto rule = [&](int s) { return bc[s] == 0 || bc[s] == 1; };  // Neumann or Dirichlet side
+    std::vector<uint8_t> f(static_cast<size_t>(nx + 1) * (ny + 1), 0);
+    for (int a = 0; a <= nx; ++a)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < 6; ++k) {
+                const int i = face_slot(a, k, nx, rule(0), rule(1));
+                if (i >= 0 && i < nx && types[static_cast<size_t>(i) * ny + j]) {
+                    f[static_cast<size_t>(a) * (ny + 1) + j] |= 1;
+                    break;
+                }
+            }
+    for (int i = 0; i < nx; ++i)
+        for (int a = 0; a <= ny; ++a)
+            for (int k = 0; k < 6; ++k) {
+                const int j = face_slot(a, k, ny, rule(2), rule(3));
+                if (j >= 0 && j < ny && types[static_cast<size_t>(i) * ny + j]) {
+                    f[static_cast<size_t>(i) * (ny + 1) + a] |= 2;
+                    break;
+                }
+            }
+    return f;
+}
+
 }  // namespace cfs

@@ -43,4 +43,13 @@ void ib_factors(int mode, const uint8_t* types, int nx, int ny, double dx, doubl
                 const double* image, const double* normal, std::vector<int32_t>& dev_donor, std::vector<double>& fac,
                 std::vector<int>& perm);
 
+// Face flags of the body positivity mode, [nx+1][ny+1] bytes: bit 0 of (i, j)
+// for the x-face between cells (i-1, j) and (i, j), bit 1 for the y-face between
+// (i, j-1) and (i, j).  A flag is set when a cell of the face's 6-cell stencil
+// that lies in the grid is not fluid.  The stencil slots are those the stage
+// kernels read, including the reference's boundary-face rule on Neumann and
+// Dirichlet sides (CellInterface.cpp:172-178: every interior slot of a
+// physical-boundary face is the first interior cell).  bc: cfs_bc per side.
+std::vector<uint8_t> low_order_faces(const uint8_t* types, int nx, int ny, const int bc[4]);
+
 }  // namespace cfs

@@ -6,24 +6,34 @@
 
 namespace cfs {
 
-template <class Pol, int R, int W, int B>
+template <class Pol, int R, int W, int B, bool Pf>
 cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     const int nseg = (a.L.ny + kSeg - 1) / kSeg;
     const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
-    march_kernel<Pol, R, W, B><<<grid, 32 * W, 0, s>>>(a);
+    march_kernel<Pol, R, W, B, Pf><<<grid, 32 * W, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+template <class Pol, int K>
+cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
+    constexpr MarchVariant v = kVariants[K];
+    return launch_march<Pol, v.rows, v.warps, v.min_blocks, v.prefetch>(a, s);
 }
 
 template <class Pol>
 cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
-    static_assert(kNumVariants == 6, "variant table and dispatch disagree");
+    static_assert(kNumVariants == 10, "variant table and dispatch disagree");
     switch (v) {
-        case 1: return launch_march<Pol, kVariants[0].rows, kVariants[0].warps, kVariants[0].min_blocks>(a, s);
-        case 2: return launch_march<Pol, kVariants[1].rows, kVariants[1].warps, kVariants[1].min_blocks>(a, s);
-        case 3: return launch_march<Pol, kVariants[2].rows, kVariants[2].warps, kVariants[2].min_blocks>(a, s);
-        case 4: return launch_march<Pol, kVariants[3].rows, kVariants[3].warps, kVariants[3].min_blocks>(a, s);
-        case 5: return launch_march<Pol, kVariants[4].rows, kVariants[4].warps, kVariants[4].min_blocks>(a, s);
-        case 6: return launch_march<Pol, kVariants[5].rows, kVariants[5].warps, kVariants[5].min_blocks>(a, s);
+        case 1: return launch_march_k<Pol, 0>(a, s);
+        case 2: return launch_march_k<Pol, 1>(a, s);
+        case 3: return launch_march_k<Pol, 2>(a, s);
+        case 4: return launch_march_k<Pol, 3>(a, s);
+        case 5: return launch_march_k<Pol, 4>(a, s);
+        case 6: return launch_march_k<Pol, 5>(a, s);
+        case 7: return launch_march_k<Pol, 6>(a, s);
+        case 8: return launch_march_k<Pol, 7>(a, s);
+        case 9: return launch_march_k<Pol, 8>(a, s);
+        case 10: return launch_march_k<Pol, 9>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -236,7 +236,8 @@ def engine_arm(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"smooth periodic advection {n}x{n} (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1), "
                                    "SSP-RK3, WENO5 eps 1e-2, Davis HLL, CFL 0.4 on-device dt",
-                       "precision": "fp32-mixed", "grid": [n, n], "cells_per_gpu": cells,
+                       "precision": "fp32-mixed (FP32 storage, stochastic rounding)", "grid": [n, n],
+                       "cells_per_gpu": cells,
                        "kernel_variant": {"f32": variants[cfsb.FP32_MIXED], "f64": variants[cfsb.FP64]},
                        "l2": "inputs larger than L2 (3 state buffers of "
                              f"{4 * 4 * cells / 1e6:.0f} MB each)"},
@@ -336,10 +337,11 @@ def batch_arm(args):
     cases, states = wl.batch_cases(args.cases, seed=1)
     K, W = args.steps, args.warmup
     out = {"workload": f"{args.cases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
-                       "cylinder (slip wall), SSP-RK3, Davis HLL, per-case CFL 0.5", "steps": K, "warmup": W}
+                       "cylinder (slip wall), SSP-RK3, Davis HLL, body positivity fallback, per-case CFL 0.5",
+           "steps": K, "warmup": W}
 
     def run_batch(prec):
-        with cfsb.Batch(cases, precision=prec) as b:
+        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_BODY) as b:
             cells, items = b.info()
             for k, U in enumerate(states):
                 b.set_state(k, U)
@@ -357,7 +359,7 @@ def batch_arm(args):
     solvers = []
     for c, U in zip(cases, states):
         s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
-                        bc=c["bc"], bc_prim=c.get("bc_prim"))
+                        bc=c["bc"], bc_prim=c.get("bc_prim"), positivity=cfsb.POSITIVITY_BODY)
         if "circle" in c:
             s.build_circle(*c["circle"], 400, cfsb.IB_BILINEAR_SLIP)
         s.set_state(U)

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define CFS_ABI_VERSION 1
+#define CFS_ABI_VERSION 2
 
 enum cfs_status {
     CFS_OK = 0,
@@ -77,6 +77,27 @@ enum cfs_ib_mode {
 
 enum cfs_viscous { CFS_VISCOUS_OFF = 0, CFS_VISCOUS_NS = 1 };
 
+/* Face-state positivity fallbacks of the throughput forms (no reference
+ * counterpart: the reference's WENO5-on-conserved + HLL scheme has none and
+ * reaches negative pressure on strong inflow past a body).  FP64_EXACT accepts
+ * CFS_POSITIVITY_OFF only. */
+enum cfs_positivity {
+    CFS_POSITIVITY_OFF = 0,   /* reconstructed states used as they come (the reference) */
+    CFS_POSITIVITY_FACE = 1,  /* a face state with rho <= 0 or p <= 0 (or NaN) is replaced by the
+                                 value of the cell next to the face on its side (first order) */
+    CFS_POSITIVITY_BODY = 2   /* FACE, and both states of every face whose 6-cell stencil holds an
+                                 immersed-ghost or solid cell are first order */
+};
+
+/* Rounding of the FP32 state storage of CFS_FP32_MIXED (no reference
+ * counterpart; the FP64 forms round to nearest). */
+enum cfs_rounding {
+    CFS_ROUND_STOCHASTIC = 0,  /* the new state is formed exactly in FP64 and rounded to one of its two
+                                  neighbouring floats with probability by nearness (random bits hashed
+                                  from cell and step): an unbiased error that does not build up */
+    CFS_ROUND_NEAREST = 1      /* FP32 FMA update, round to nearest */
+};
+
 typedef struct cfs_config {
     int nx, ny;              /* cells; CartesianMesh::setnumberCellsX/YGlobal (Run.cpp:17-18) */
     double lx, ly;           /* domain lengths; setGlobalLengthX/Y (Run.cpp:19-20) */
@@ -93,16 +114,19 @@ typedef struct cfs_config {
     int device;              /* CUDA device ordinal */
     int variant;             /* stage-kernel variant of the throughput forms (tile rows x warps x
                                 occupancy target, see cfs_variant_info); 0 = the tuned default */
+    int positivity;          /* enum cfs_positivity */
+    int rounding;            /* enum cfs_rounding (CFS_FP32_MIXED) */
 } cfs_config;
 
 typedef struct cfs_ctx cfs_ctx;
 
 /* Number of stage-kernel variants of the throughput forms, and the shape of
  * variant v (1-based): rows marched per warp, warps per block, minimum resident
- * blocks per SM requested from the compiler.  Returns CFS_ERR_INVALID for an
- * unknown v. */
+ * blocks per SM requested from the compiler, and whether the row march
+ * prefetches its loads a row ahead (1) or loads at the point of use (0).
+ * Returns CFS_ERR_INVALID for an unknown v. */
 int cfs_variant_count(void);
-int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks);
+int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks, int* prefetch);
 
 /* Fills a config with the reference's defaults: gamma 1.4, eps 1e-2, FP64,
  * TVD3 as written, reference HLL, Neumann sides, inviscid. */
@@ -234,7 +258,7 @@ typedef struct cfs_case {
 
 typedef struct cfs_batch cfs_batch;
 
-/* common supplies precision, rk, hll, gamma, weno_eps and device. */
+/* common supplies precision, rk, hll, gamma, weno_eps, positivity, rounding and device. */
 int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases, cfs_batch** out);
 int cfs_batch_destroy(cfs_batch* b);
 const char* cfs_batch_last_error(const cfs_batch* b);

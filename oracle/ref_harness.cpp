@@ -22,6 +22,10 @@
 #include <chrono>
 #include <cstring>
 
+#ifdef CFS_WITH_GPU_PLUGINS
+#include "cfs_plugins.h"
+#endif
+
 // The four process globals the reference's mesh objects reach through `extern`
 // (Run.cpp:5-8).
 std::shared_ptr<Model> model;
@@ -449,5 +453,55 @@ int ref_viscous(const ref_config* c, const double* U_in, double* grad_out, doubl
     reset_globals();
     return 0;
 }
+
+#ifdef CFS_WITH_GPU_PLUGINS
+// ref_run's loop with the product's GPU plugins registered in place of the
+// reference's (the drop-in at Run.cpp:41-48): EulerMod, Weno5th, HLL and the
+// RK class are swapped for cfs_plugins' subclasses before the pre-loop, so the
+// reference's own loop drives one cfs_stage per iteration.  precision:
+// cfs_precision.  Fixed dt only.  Returns 0, or -1 with the message in err.
+int ref_gpu_run(const ref_config* c, const double* U_in, int nstages, int precision, double* U_out, char* err,
+                int err_len) {
+    try {
+        Sim s;
+        initialize(s, *c, U_in);
+        cfs_config cfg;
+        cfs_config_default(&cfg);
+        cfg.nx = c->nx;
+        cfg.ny = c->ny;
+        cfg.lx = c->lx;
+        cfg.ly = c->ly;
+        cfg.precision = precision;
+        cfg.rk = c->integrator == 2 ? CFS_RK_TVD2 : CFS_RK_TVD3_REFERENCE;
+        cfg.hll = CFS_HLL_REFERENCE;
+        for (int k = 0; k < 4; ++k) {
+            cfg.bc[k] = c->bc_type[k] == 1 ? CFS_BC_DIRICHLET : CFS_BC_NEUMANN;
+            for (int q = 0; q < 4; ++q) cfg.bc_prim[k][q] = c->bc_prim[k][q];
+        }
+        auto gpu = std::make_shared<cfs_plugins::Session>(cfg, s.cells);
+        if (c->circle) gpu->set_circle(c->radius, c->cx, c->cy, c->npoints);
+        gpu->set_sync_interval(0);
+        model = std::make_shared<cfs_plugins::GpuModel>();
+        interpolation = std::make_shared<cfs_plugins::GpuInterpolation>();
+        riemmansolver = std::make_shared<cfs_plugins::GpuRiemannSolver>();
+        s.rk = std::make_shared<cfs_plugins::GpuExplicit>(gpu);
+        preloop(s, c->dt);
+        for (int i = 1; i <= nstages; ++i) stage(s, i);
+        gpu->sync_to_host();
+        if (U_out) dump_state(s, *c, U_out);
+        const long long ran = gpu->stages_run();
+        s.rk.reset();
+        reset_globals();
+        return ran == nstages ? 0 : -1;
+    } catch (const std::exception& e) {
+        if (err && err_len > 0) {
+            std::strncpy(err, e.what(), static_cast<size_t>(err_len - 1));
+            err[err_len - 1] = 0;
+        }
+        reset_globals();
+        return -1;
+    }
+}
+#endif
 
 }  // extern "C"

@@ -18,6 +18,7 @@ ROOT = Path(__file__).resolve().parents[1]
 ORACLE = ROOT / "oracle"
 REF_STRICT = ORACLE / "_ref" / "libref_strict.so"
 REF_PERF = ORACLE / "_ref" / "libref_perf.so"
+REF_GPU = ORACLE / "_ref" / "libref_gpu.so"
 ORACLE_LIB = ORACLE / "libcfs_oracle.so"
 REFERENCE_TREE = Path("/root/reference")
 
@@ -127,6 +128,24 @@ def make_orc_config(nx, ny, lx=1.0, ly=1.0, rk=RK_TVD3_REFERENCE, hll=0, bc=(0, 
         for q in range(4):
             c.bc_U[s][q] = cons[q]
     return c
+
+
+def ref_gpu_lib() -> ctypes.CDLL:
+    """The reference's classes with the product's GPU plugins registered
+    (oracle/Makefile target gpu; built where the reference tree is)."""
+    return ctypes.CDLL(str(REF_GPU))
+
+
+def ref_gpu_run(nx, ny, U0, nstages, precision=2, **kw):
+    """The reference loop driven through the GPU plugins: returns the state."""
+    c = make_ref_config(nx, ny, **kw)
+    U0 = np.ascontiguousarray(U0, dtype=np.float64)
+    out = np.zeros_like(U0)
+    err = ctypes.create_string_buffer(512)
+    rc = ref_gpu_lib().ref_gpu_run(ctypes.byref(c), P(U0), int(nstages), int(precision), P(out), err, 512)
+    if rc != 0:
+        raise RuntimeError(f"ref_gpu_run failed: {err.value.decode()}")
+    return out
 
 
 def ref_run(nx, ny, U0, nstages, **kw):

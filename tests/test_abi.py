@@ -25,7 +25,7 @@ def test_every_declared_entry_point_is_exported_and_bound(cfsb):
 
 def test_abi_version_and_defaults(cfsb):
     lib = cfsb.load_library()
-    assert lib.cfs_abi_version() == 1
+    assert lib.cfs_abi_version() == 2
     import ctypes
     cfg = cfsb.CfsConfig()
     lib.cfs_config_default(ctypes.byref(cfg))
@@ -61,3 +61,14 @@ def test_no_cpu_fallback_without_a_device(cfsb):
     with pytest.raises(cfsb.CfsError) as e:
         cfsb.Solver(16, 16)
     assert e.value.code == 2
+
+
+def test_gpu_plugin_harness_links_the_product_library():
+    """oracle/_ref/libref_gpu.so (reference classes + GPU plugins) loads on a
+    host without a GPU and exports its entry point; it resolves libcfs.so
+    from the package directory."""
+    import oracle_bind as ob
+    if not ob.REF_GPU.exists():
+        pytest.skip("built only where the reference tree is")
+    lib = ob.ref_gpu_lib()
+    assert hasattr(lib, "ref_gpu_run")

@@ -214,20 +214,52 @@ def test_fp32_mixed_error_and_conservation(cfsb, workloads):
     # and the FP64 path converges to the exact solution
     exact = workloads.smooth_advection_exact(n, 0.5)
     assert np.abs(U64[0] - exact).mean() < 1e-4
+    # round-to-nearest storage (biased on this smooth, slowly moving state) is
+    # the less accurate of the two FP32 roundings
+    with cfsb.Solver(n, n, precision=cfsb.FP32_MIXED, rounding=cfsb.ROUND_NEAREST, **kw) as s:
+        s.set_state(w.U0)
+        s.advance(nsteps, dt=dt)
+        l1_rn = np.abs(s.get_state()[0] - U64[0]).mean()
+    assert l1 < l1_rn, (l1, l1_rn)
+
+
+def test_fp32_stochastic_rounding_is_reproducible(cfsb, workloads):
+    """The random bits depend on cell and step count only: two runs agree bit
+    for bit, and so do one advance(6) and six advance(1) calls (the step
+    counter carries across calls) and the stage-by-stage path."""
+    w = workloads.smooth_advection(96)
+    kw = dict(precision=cfsb.FP32_MIXED, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=(2, 2, 2, 2))
+    states = []
+    for mode in ("one", "one", "split", "stages"):
+        with cfsb.Solver(96, 96, **kw) as s:
+            s.set_state(w.U0)
+            if mode == "one":
+                s.advance(6, dt=1e-3)
+            elif mode == "split":
+                for _ in range(6):
+                    s.advance(1, dt=1e-3)
+            else:
+                for _ in range(6):
+                    s.step(1e-3)
+            states.append(s.get_state())
+    for U in states[1:]:
+        assert np.array_equal(U, states[0])
 
 
 def test_fp64_slip_cylinder_per_step(cfsb, workloads):
     """Mach-3 cylinder (2 x 1 domain, 256 x 128), slip-wall immersed boundary,
-    SSP-RK3 + Davis HLL: per-step relative L-infinity <= 1e-12 against the oracle."""
+    SSP-RK3 + Davis HLL, body positivity fallback (without it the scheme reaches
+    negative pressure behind the body within the first step): per-step relative
+    L-infinity <= 1e-12 against the oracle."""
     nx, ny = 256, 128
     w = workloads.mach3_cylinder(nx, ny)
     types, cells, donors, images, normals = cfsb.circle_setup(nx, ny, 2.0, 1.0, *w.circle, 400)
     U = w.U0.copy()  # freestream in the body too: solid cells stay inside the fluid stencils
-    cfg = ob.make_orc_config(nx, ny, lx=2.0, ly=1.0, rk=2, hll=1, bc=w.bc, bc_prim=w.bc_prim)
+    cfg = ob.make_orc_config(nx, ny, lx=2.0, ly=1.0, rk=2, hll=1, bc=w.bc, bc_prim=w.bc_prim, positivity=2)
     ib = ob.OrcIBList(cells, donors, images, normals, mode=1, types=types)
     worst = 0.0
     with cfsb.Solver(nx, ny, 2.0, 1.0, precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=w.bc,
-                     bc_prim=w.bc_prim) as s:
+                     bc_prim=w.bc_prim, positivity=cfsb.POSITIVITY_BODY) as s:
         s.build_circle(*w.circle, 400, cfsb.IB_BILINEAR_SLIP)
         for _ in range(10):
             dt = ob.orc_cfl_dt(cfg, U, 0.5, types)
@@ -239,3 +271,21 @@ def test_fp64_slip_cylinder_per_step(cfsb, workloads):
             worst = max(worst, _rel_linf(got, ref))
             U = ref
     assert worst <= 1e-12, worst
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_body_positivity_keeps_mach3_cylinder_physical(cfsb, workloads, prec):
+    """300 steps of the Mach-3 cylinder (256 x 128, CFL 0.5) with the body
+    positivity fallback stay finite with positive density and pressure."""
+    w = workloads.mach3_cylinder(256, 128)
+    with cfsb.Solver(256, 128, 2.0, 1.0, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=w.bc,
+                     bc_prim=w.bc_prim, positivity=cfsb.POSITIVITY_BODY) as s:
+        s.build_circle(*w.circle, 400, cfsb.IB_BILINEAR_SLIP)
+        types, *_ = cfsb.circle_setup(256, 128, 2.0, 1.0, *w.circle, 400)
+        s.set_state(w.U0)
+        t, _ = s.advance(300, cfl=0.5)
+        U = s.get_state()
+    f = types == 0
+    p = 0.4 * (U[3] - 0.5 * (U[1] ** 2 + U[2] ** 2) / U[0])
+    assert np.all(np.isfinite(U[:, f])) and t > 0
+    assert U[0][f].min() > 0 and p[f].min() > 0

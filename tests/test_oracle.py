@@ -147,3 +147,24 @@ def test_hll_consistency_equal_states():
             un = q / rho
             exact = np.array([q, U[1] * un + (p if d == 0 else 0), U[2] * un + (p if d == 1 else 0), (U[3] + p) * un])
             assert np.allclose(out, exact, rtol=1e-13, atol=1e-15)
+
+
+def test_positivity_fallback_on_mach3_cylinder(cfsb):
+    """The reference scheme (no fallback) reaches NaN on the Mach-3 cylinder in
+    its first step; the body fallback keeps 40 steps finite."""
+    import importlib
+    wl = importlib.import_module("2d_compressible_flow_solver_b200.workloads")
+    nx, ny = 128, 64
+    w = wl.mach3_cylinder(nx, ny)
+    types, cells, donors, images, normals = cfsb.circle_setup(nx, ny, 2.0, 1.0, *w.circle, 400)
+    ib = ob.OrcIBList(cells, donors, images, normals, mode=1, types=types)
+    f = types == 0
+    finite = {}
+    for pos, nsteps in ((0, 1), (2, 40)):
+        cfg = ob.make_orc_config(nx, ny, lx=2.0, ly=1.0, rk=2, hll=1, bc=w.bc, bc_prim=w.bc_prim, positivity=pos)
+        U = w.U0.copy()
+        for _ in range(nsteps):
+            dt = ob.orc_cfl_dt(cfg, U, 0.5, types)
+            U, _ = ob.orc_run(cfg, U, 1, 3, dt=dt, types=types, ib=ib)
+        finite[pos] = bool(np.all(np.isfinite(U[:, f])))
+    assert finite == {0: False, 2: True}
