@@ -118,6 +118,7 @@ _SIGNATURES = {
     "cfs_halo_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "cfs_halo_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_halo_unpack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "cfs_set_storage_offsets": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_conserved_totals": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_compute_dt_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -333,6 +334,17 @@ class Solver:
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""
         return int(self._lib.cfs_get_stream(self._ctx) or 0)
+
+    def set_storage_offsets(self, off=None) -> None:
+        """Fix the FP32-mixed storage offsets (4 values) for later set_state
+        calls; None returns to the state's own means."""
+        if off is None:
+            self._check(self._lib.cfs_set_storage_offsets(self._ctx, None))
+        else:
+            a = np.ascontiguousarray(off, dtype=np.float64)
+            if a.shape != (4,):
+                raise ValueError("need 4 offsets")
+            self._check(self._lib.cfs_set_storage_offsets(self._ctx, _dp(a)))
 
     def halo_bytes(self) -> int:
         n = ctypes.c_longlong(0)

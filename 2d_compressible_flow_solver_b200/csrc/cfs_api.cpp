@@ -35,6 +35,8 @@ struct cfs_ctx {
     uint8_t* types_d = nullptr;
     uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
     unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
+    bool fixed_offsets = false;   // FP32 storage offsets set by cfs_set_storage_offsets
+    float fixed_off[4] = {0, 0, 0, 0};
     bool has_types = false;
     std::vector<uint8_t> types_h;
     // immersed ghosts
@@ -439,9 +441,12 @@ int cfs_set_state(cfs_ctx* c, const double* U) {
         const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
         bool changed = false;
         for (int v = 0; v < kVars; ++v) {
-            double sum = 0.0;
-            for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
-            float off = static_cast<float>(sum / static_cast<double>(n));
+            float off = c->fixed_off[v];
+            if (!c->fixed_offsets) {
+                double sum = 0.0;
+                for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
+                off = static_cast<float>(sum / static_cast<double>(n));
+            }
             if (!std::isfinite(off)) off = 0.0f;
             changed = changed || off != c->L.off[v];
             c->L.off[v] = off;
@@ -455,6 +460,13 @@ int cfs_set_state(cfs_ctx* c, const double* U) {
     c->cur = 0;
     c->u0_idx = c->u1_idx = -1;
     c->next_stage = 0;
+    return CFS_OK;
+}
+
+int cfs_set_storage_offsets(cfs_ctx* c, const double* off4) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    c->fixed_offsets = off4 != nullptr;
+    for (int v = 0; v < kVars; ++v) c->fixed_off[v] = off4 ? static_cast<float>(off4[v]) : 0.0f;
     return CFS_OK;
 }
 

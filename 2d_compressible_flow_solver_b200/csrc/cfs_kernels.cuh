@@ -314,6 +314,18 @@ __device__ __forceinline__ double wave_sum(double rho, double mx, double my, dou
     return (fabs(u) + a) / dx + (fabs(v) + a) / dy;
 }
 
+// The same wave-speed sum for the CFL maximum fused into the last stage of the
+// throughput forms: one reciprocal and one square root, in the form's
+// arithmetic type (inv_dx = 1/dx, inv_dy = 1/dy).
+template <class C>
+__device__ __forceinline__ C wave_sum_fast(C rho, C mx, C my, C E, C g, C inv_dx, C inv_dy) {
+    const C ri = rcp_fast(rho);
+    const C u = mx * ri, v = my * ri;
+    const C p = (g - C(1)) * (E - C(0.5) * (mx * u + my * v));
+    const C a = sqrt_fast(g * p * ri);
+    return (fabs(u) + a) * inv_dx + (fabs(v) + a) * inv_dy;
+}
+
 // Writes one cell of the new state and the ghost copies it feeds: Neumann
 // ghosts copy the adjacent cell into all three layers (NeummanBoundary.cpp:31-45;
 // one ghost repeated three times in the stencil, CellInterface.cpp:147-179),

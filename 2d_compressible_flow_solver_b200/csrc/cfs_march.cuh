@@ -25,39 +25,51 @@ namespace cfs {
 constexpr int kSeg = 30;
 
 // Left- and right-biased WENO5 states of the middle cell of v0..v4
-// (Weno5th.cpp:4-28 applied to v0..v4 and to v4..v0) with shared smoothness
-// indicators and one reciprocal each.
+// (Weno5th.cpp:4-28 applied to v0..v4 and to v4..v0), rewritten on the
+// differences D1..D4 (Dk = v_k - v_{k-1}) so that both states share one set of
+// smoothness indicators and weight products and are formed as v2 plus a small
+// correction (fewer operations, and in FP32 a rounding error relative to the
+// correction instead of to the value):
+//   beta_k (13/12) d_k^2 + (1/4) e_k^2 with d = (D2-D1, D3-D2, D4-D3),
+//     e = (3 D2 - D1, D2 + D3, D4 - 3 D3); scaled by 12/13 with eps alike, which
+//     leaves the normalised weights unchanged;
+//   candidate p_k = v2 + c_k: c = ((5 D2 - 2 D1)/6, (D2 + 2 D3)/6, (4 D3 - D4)/6),
+//     mirrored c' = ((2 D4 - 5 D3)/6, -(D3 + 2 D2)/6, (D1 - 4 D2)/6);
+//   weights d_k / q_k with q_k = (eps + beta_k)^2, taken as products of the
+//     other two q times (1, 6, 3) (the linear weights 0.1, 0.6, 0.3 times 10).
 template <class C>
-__device__ __forceinline__ void weno5_pair(C v0, C v1, C v2, C v3, C v4, C eps, C& left, C& right) {
-    const C k13 = C(13.0 / 12.0), k14 = C(0.25);
-    const C d0 = v0 - C(2) * v1 + v2, e0 = v0 - C(4) * v1 + C(3) * v2;
-    const C d1 = v1 - C(2) * v2 + v3, e1 = v1 - v3;
-    const C d2 = v2 - C(2) * v3 + v4, e2 = C(3) * v2 - C(4) * v3 + v4;
-    C b0 = k13 * d0 * d0 + k14 * e0 * e0;
-    C b1 = k13 * d1 * d1 + k14 * e1 * e1;
-    C b2 = k13 * d2 * d2 + k14 * e2 * e2;
+__device__ __forceinline__ void weno5_pair_diff(C v0, C v1, C v2, C v3, C v4, C eps, C& left, C& right) {
+    const C D1 = v1 - v0, D2 = v2 - v1, D3 = v3 - v2, D4 = v4 - v3;
+    const C d0 = D2 - D1, d1 = D3 - D2, d2 = D4 - D3;
+    const C e0 = fma(C(3), D2, -D1), e1 = D2 + D3, e2 = fma(C(-3), D3, D4);
+    const C k = C(3.0 / 13.0);
+    C b0 = fma(d0, d0, k * (e0 * e0));
+    C b1 = fma(d1, d1, k * (e1 * e1));
+    C b2 = fma(d2, d2, k * (e2 * e2));
     if (sizeof(C) == 4) {
         b0 = fmin(b0, C(1e9));
         b1 = fmin(b1, C(1e9));
         b2 = fmin(b2, C(1e9));
     }
-    C q0 = eps + b0, q1 = eps + b1, q2 = eps + b2;
+    C q0 = eps + b0, q1 = eps + b1, q2 = eps + b2;  // eps: the WENO eps times 12/13
     q0 *= q0;
     q1 *= q1;
     q2 *= q2;
-    const C q01 = q0 * q1, q02 = q0 * q2, q12 = q1 * q2;
-    // left: linear weights (0.1, 0.6, 0.3) on indicators (b0, b1, b2)
-    const C aL0 = C(0.1) * q12, aL1 = C(0.6) * q02, aL2 = C(0.3) * q01;
-    const C pL0 = C(2) * v0 - C(7) * v1 + C(11) * v2;
-    const C pL1 = -v1 + C(5) * v2 + C(2) * v3;
-    const C pL2 = C(2) * v2 + C(5) * v3 - v4;
-    left = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * rcp_fast(C(6) * (aL0 + aL1 + aL2));
-    // right: the mirrored stencil's indicators are (b2, b1, b0)
-    const C aR0 = C(0.1) * q01, aR1 = C(0.6) * q02, aR2 = C(0.3) * q12;
-    const C pR0 = C(2) * v4 - C(7) * v3 + C(11) * v2;
-    const C pR1 = -v3 + C(5) * v2 + C(2) * v1;
-    const C pR2 = C(2) * v2 + C(5) * v1 - v0;
-    right = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * rcp_fast(C(6) * (aR0 + aR1 + aR2));
+    const C q01 = q0 * q1, q12 = q1 * q2, a1 = C(6) * (q0 * q2);
+    const C a2L = C(3) * q01, a2R = C(3) * q12;
+    const C c0 = fma(C(5.0 / 6.0), D2, C(-1.0 / 3.0) * D1);
+    const C c1 = fma(C(1.0 / 3.0), D3, C(1.0 / 6.0) * D2);
+    const C c2 = fma(C(2.0 / 3.0), D3, C(-1.0 / 6.0) * D4);
+    const C r0 = fma(C(1.0 / 3.0), D4, C(-5.0 / 6.0) * D3);
+    const C r1 = fma(C(-1.0 / 3.0), D2, C(-1.0 / 6.0) * D3);
+    const C r2 = fma(C(1.0 / 6.0), D1, C(-2.0 / 3.0) * D2);
+    left = fma(fma(q12, c0, fma(a1, c1, a2L * c2)), rcp_fast(q12 + a1 + a2L), v2);
+    right = fma(fma(q01, r0, fma(a1, r1, a2R * r2)), rcp_fast(q01 + a1 + a2R), v2);
+}
+
+template <class C>
+__device__ __forceinline__ void weno5_pair(C v0, C v1, C v2, C v3, C v4, C eps, C& left, C& right) {
+    weno5_pair_diff(v0, v1, v2, v3, v4, C(12.0 / 13.0) * eps, left, right);
 }
 
 // Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).
@@ -117,14 +129,14 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 }
 
 // One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
-// block column bx.  Every thread of the block calls it (it ends with a block
-// reduction when the CFL maximum is accumulated).  kPf: software prefetch -
+// block column bx.  Each warp works on its own segment; the warps of a block
+// share nothing but their slices of the row buffer.  kPf: software prefetch -
 // the next row two iterations ahead, the y halo columns one row ahead, and the
 // RK operands of the row being updated before its x reconstruction - so that
 // global-load latency overlaps a row of arithmetic.
 template <class Pol, int kWarps, bool kPf = false>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
-                                           typename Pol::C (&rbuf)[kWarps][kVars][36], double* wred) {
+                                           typename Pol::C (&rbuf)[kWarps][kVars][36]) {
     using T = typename Pol::T;
     using C = typename Pol::C;
     const Layout& L = a.L;
@@ -255,7 +267,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 const long long off = L.offset(i, j);
                 const T* u1 = static_cast<const T*>(a.u1);
                 T* out = static_cast<T*>(a.out);
-                double nv[kVars];
+                C nv[kVars];  // new state in the form's arithmetic type, for the CFL maximum
                 T sv[kVars];
                 if constexpr (Pol::kMixed) {
                     // FP32 update of the stored deviations (value - off): the RK
@@ -282,7 +294,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                             }
                         }
                         sv[v] = nd;
-                        nv[v] = double(nd) + double(L.off[v]);
+                        nv[v] = nd + L.off[v];
                         if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
                     }
                 } else {
@@ -299,14 +311,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                             val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
                         }
                         sv[v] = enc<T>(val, L, v);
-                        nv[v] = dec<T>(sv[v], L, v);
+                        nv[v] = C(dec<T>(sv[v], L, v));
                         if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
                     }
                 }
                 store_cell4<T>(out, L, a.bc, i, j, sv);
                 if (a.P && a.last_stage && a.P->use_cfl && fluid) {
-                    const double w = wave_sum(nv[0], nv[1], nv[2], nv[3], g, a.dx, a.dy);
-                    if (w > wloc) wloc = w;
+                    const C w = wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy));
+                    if (double(w) > wloc) wloc = double(w);
                 }
             }
         }
@@ -383,25 +395,20 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             }
         }
     }
+    // CFL maximum: one atomic per warp (no block barrier, so the warps of a
+    // block never wait for each other)
     if (a.P && a.last_stage && a.P->use_cfl) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) wloc = fmax(wloc, __shfl_xor_sync(0xffffffffu, wloc, o));
-        if (lane == 0) wred[wid] = wloc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double m = 0.0;
-            for (int w = 0; w < kWarps; ++w) m = fmax(m, wred[w]);
-            if (m > 0.0) atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(m)));
-        }
-        __syncthreads();
+        if (lane == 0 && wloc > 0.0)
+            atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(wloc)));
     }
 }
 
 template <class Pol, int kRows, int kWarps, int kMinBlocks, bool kPf>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ typename Pol::C rbuf[kWarps][kVars][36];
-    __shared__ double wred[kWarps];
-    march_item<Pol, kWarps, kPf>(a, blockIdx.x, blockIdx.y, kRows, rbuf, wred);
+    march_item<Pol, kWarps, kPf>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
 }
 
 // Persistent batched form: one launch runs one stage of every case of a batch.
@@ -415,7 +422,6 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
                        const int* __restrict__ item_local, const int* __restrict__ case_rows,
                        const int* __restrict__ case_items_x, int total, unsigned int* counter) {
     __shared__ typename Pol::C rbuf[kWarps][kVars][36];
-    __shared__ double wred[kWarps];
     __shared__ int s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
@@ -426,7 +432,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
         const int c = item_case[w], li = item_local[w];
         const int ix = case_items_x[c];
         const StageArgs a = args[c];
-        march_item<Pol, kWarps>(a, li % ix, li / ix, case_rows[c], rbuf, wred);
+        march_item<Pol, kWarps>(a, li % ix, li / ix, case_rows[c], rbuf);
     }
 }
 

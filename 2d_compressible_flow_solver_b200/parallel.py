@@ -8,7 +8,9 @@ its neighbour and receives the neighbour's rows into its 3 ghost rows (rows
 are contiguous in the engine's layout, so a message is 4 device copies of
 3 x pitch elements).  Per step the CFL time step is the minimum over ranks.
 Only the exchange is a collective step; everything else stays on each GPU.
-The immersed boundary is not decomposed (a slab solver has none).
+The immersed boundary is not decomposed (a slab solver has none).  In the
+FP32-mixed form every slab stores against the same offsets (the global means),
+so the stored rows a message carries mean the same on both sides.
 
 Message order (point-to-point ops match in posting order per peer): every
 rank posts send(right rows -> right), send(left rows -> left),
@@ -130,6 +132,19 @@ class SlabSolver:
         self.halo = HaloExchange(_EngineSlab(self.solver), dist, self.left, self.right, f"cuda:{device}")
 
     def set_state(self, U_local) -> None:
+        """Local conserved state [4][i1-i0][ny].  Halo messages carry stored
+        values, so every slab of an FP32-mixed grid stores against the global
+        means (one all-reduce of the local sums)."""
+        import numpy as np
+        import torch
+
+        U_local = np.ascontiguousarray(U_local, dtype=np.float64)
+        if self.world > 1:
+            sums = torch.tensor([*U_local.reshape(4, -1).sum(axis=1), float(U_local[0].size)], dtype=torch.float64,
+                                device=f"cuda:{self.device}")
+            self.dist.all_reduce(sums, op=self.dist.ReduceOp.SUM)
+            s = sums.cpu().numpy()
+            self.solver.set_storage_offsets(s[:4] / s[4])
         self.solver.set_state(U_local)
         self.halo.exchange()
 

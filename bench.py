@@ -15,9 +15,12 @@ Arms:
                      with the reference Makefile's optimisation flags) on all host
                      cores, on bounded samples of the same workload.
 
-Multi-GPU (torchrun, one rank per GPU): every rank advances its own 4096^2
-periodic domain (weak scaling); there is no exchange between ranks, so no
-collective is on the data path; timings are the max over ranks.
+Multi-GPU (torchrun, one rank per GPU, NCCL): one periodic grid of
+(4096 N) x 4096 cells on [0, N] x [0, 1] split into N slabs of 4096^2 along x
+(weak scaling, parallel.SlabSolver): after every stage each rank sends its 3
+edge rows to its two neighbours and receives their rows into its ghost rows,
+and every step takes the global minimum CFL time step.  Timings are the max
+over ranks.  The batch workload splits its cases round-robin over the ranks.
 """
 from __future__ import annotations
 
@@ -188,7 +191,35 @@ def engine_arm(args):
     autotune = importlib.import_module(f"{PKG}.autotune")
     variants = {cfsb.FP32_MIXED: autotune.best_variant("f32", n * n), cfsb.FP64: autotune.best_variant("f64", n * n)}
 
+    def timed_advance_slab(prec, steps, warm):
+        par = importlib.import_module(f"{PKG}.parallel")
+        s = par.SlabSolver(n * world, n, float(world), 1.0, dist=dist, rank=rank, world=world, device=local,
+                           bc=(cfsb.BC_PERIODIC,) * 4, precision=prec, variant=variants[prec], rk=cfsb.RK_SSP3,
+                           hll=cfsb.HLL_DAVIS)
+        # the field is 1-periodic in x, so every slab of [0, N] x [0, 1] starts
+        # from the single-domain state
+        s.set_state(w.U0)
+        stream = torch.cuda.ExternalStream(s.solver.stream, device=local)
+        if warm:
+            s.advance(warm, w.cfl)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t_sim = s.advance(steps, w.cfl)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        totals = s.solver.totals()
+        s.close()
+        return ms, t_sim, None, totals
+
     def timed_advance(prec, steps, warm):
+        if world > 1:
+            return timed_advance_slab(prec, steps, warm)
         s = cfsb.Solver(n, n, precision=prec, variant=variants[prec], **kw)
         s.set_state(w.U0)
         stream = torch.cuda.ExternalStream(s.stream, device=local)
@@ -227,7 +258,7 @@ def engine_arm(args):
         peak, peak_kind = hbm_peak()
         bytes32 = WORDS_PER_CELL_STEP * 4 * cells * K
         achieved = bytes32 / (ms32 / 1e3) / 1e9
-        launches = 3 * K + 1
+        launches = 3 * K + 1 if world == 1 else 4 * K  # slabs: 3 stages + 1 CFL launch per step
         per_launch_ms = ms32 / launches
         trf = MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH["f32"]
         result = {
@@ -239,6 +270,9 @@ def engine_arm(args):
                        "precision": "fp32-mixed (FP32 storage, stochastic rounding)", "grid": [n, n],
                        "cells_per_gpu": cells,
                        "kernel_variant": {"f32": variants[cfsb.FP32_MIXED], "f64": variants[cfsb.FP64]},
+                       "parallelism": "single grid" if world == 1 else
+                       f"{world} slabs of {n}x{n} along x, 3-row halo exchange per stage (NCCL send/recv), "
+                       "global CFL min per step",
                        "l2": "inputs larger than L2 (3 state buffers of "
                              f"{4 * 4 * cells / 1e6:.0f} MB each)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -329,27 +363,52 @@ def engine_arm(args):
 def batch_arm(args):
     """Uneven batch of independent cases (512 by default): aggregate
     Mcell-steps/s of the persistent batched engine (FP32-mixed and FP64) and of
-    a loop of plain FP64 single-grid solvers over the same cases."""
+    a loop of plain FP64 single-grid solvers over the same cases.  With N ranks
+    each rank runs the cases k with k % N == rank; rates use the max wall time
+    over ranks."""
     import torch
+    import torch.distributed as dist
 
+    rank, world, local = env_rank()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
     cfsb = importlib.import_module(PKG)
     wl = importlib.import_module(f"{PKG}.workloads")
     cases, states = wl.batch_cases(args.cases, seed=1)
+    cases, states = cases[rank::world], states[rank::world]
     K, W = args.steps, args.warmup
+
+    def job_max(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_sum(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
     out = {"workload": f"{args.cases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
                        "cylinder (slip wall), SSP-RK3, Davis HLL, body positivity fallback, per-case CFL 0.5",
            "steps": K, "warmup": W}
 
     def run_batch(prec):
-        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_BODY) as b:
+        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_BODY, device=local) as b:
             cells, items = b.info()
             for k, U in enumerate(states):
                 b.set_state(k, U)
             b.advance(W, cfl=0.5)
             torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
             t0 = time.perf_counter()
             b.advance(K, cfl=0.5)
-            wall = time.perf_counter() - t0
+            wall = job_max(time.perf_counter() - t0)
+        cells = int(job_sum(cells))
         return cells, items, cells * K / wall / 1e6, wall
 
     cells, items, v32, w32 = run_batch(cfsb.FP32_MIXED)
@@ -359,17 +418,19 @@ def batch_arm(args):
     solvers = []
     for c, U in zip(cases, states):
         s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
-                        bc=c["bc"], bc_prim=c.get("bc_prim"), positivity=cfsb.POSITIVITY_BODY)
+                        bc=c["bc"], bc_prim=c.get("bc_prim"), positivity=cfsb.POSITIVITY_BODY, device=local)
         if "circle" in c:
             s.build_circle(*c["circle"], 400, cfsb.IB_BILINEAR_SLIP)
         s.set_state(U)
         s.advance(W, cfl=0.5)
         solvers.append(s)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     t0 = time.perf_counter()
     for s in solvers:
         s.advance(K, cfl=0.5)
-    wall = time.perf_counter() - t0
+    wall = job_max(time.perf_counter() - t0)
     for s in solvers:
         s.close()
     loop64 = cells * K / wall / 1e6
@@ -378,8 +439,12 @@ def batch_arm(args):
                 "batched_fp32_over_batched_fp64": round(v32 / v64, 2),
                 "batched_fp32_hbm_frac": round(v32 * 1e6 * WORDS_PER_CELL_STEP * 4 / 1e9 / peak, 4),
                 "timing": "host wall clock around cfs_batch_advance / the per-case cfs_advance loop (each call "
-                          "waits for its stream)"})
-    print(json.dumps(out), flush=True)
+                          "waits for its stream), max over ranks", "n_gpus": world})
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # ----------------------------------------------------------- reference arm

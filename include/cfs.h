@@ -221,10 +221,19 @@ int cfs_advance(cfs_ctx* ctx, int nsteps, double cfl, double dt, double* t_elaps
  * cfs_halo_bytes: size of one side's message (3 rows x 4 variables, ghost
  * columns included, the state's storage type).  pack: the 3 interior rows next
  * to `side` of the current state -> dev_dst (device memory).  unpack: dev_src ->
- * the 3 ghost rows of `side`.  Both are ordered on the context's stream. */
+ * the 3 ghost rows of `side`.  Both are ordered on the context's stream.
+ * Messages carry stored values: in CFS_FP32_MIXED every context of one
+ * decomposed grid must store against the same offsets (cfs_set_storage_offsets). */
 int cfs_halo_bytes(cfs_ctx* ctx, long long* bytes);
 int cfs_halo_pack(cfs_ctx* ctx, int side, void* dev_dst);
 int cfs_halo_unpack(cfs_ctx* ctx, int side, const void* dev_src);
+
+/* CFS_FP32_MIXED stores each variable as (value - offset) in FP32.  By default
+ * cfs_set_state takes the offsets from the state (each variable's mean, rounded
+ * to FP32).  This call fixes them (FP32-rounded) for the following
+ * cfs_set_state calls; off = NULL returns to the default.  No effect on the
+ * FP64 forms.  (No reference counterpart.) */
+int cfs_set_storage_offsets(cfs_ctx* ctx, const double* off4);
 
 /* Waits for the context's stream. */
 int cfs_synchronize(cfs_ctx* ctx);
