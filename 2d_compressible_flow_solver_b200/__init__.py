@@ -24,7 +24,8 @@ __all__ = [
     "FP64", "FP32_MIXED", "FP64_EXACT", "RK_TVD2", "RK_TVD3_REFERENCE", "RK_SSP3",
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
-    "VISCOUS_OFF", "VISCOUS_NS",
+    "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "ROUND_STOCHASTIC",
+    "ROUND_NEAREST", "variants",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -158,7 +159,7 @@ def load_library() -> ctypes.CDLL:
 
 
 def variants() -> list[tuple[int, int, int, int]]:
-    """(rows, warps, min_blocks, prefetch) of every stage-kernel variant, index v-1."""
+    """(rows, warps, min_blocks, load schedule) of every stage-kernel variant, index v-1."""
     lib = load_library()
     out = []
     for v in range(1, lib.cfs_variant_count() + 1):

@@ -322,7 +322,7 @@ int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks, int* prefetc
     if (rows) *rows = cfs::kVariants[v - 1].rows;
     if (warps) *warps = cfs::kVariants[v - 1].warps;
     if (min_blocks) *min_blocks = cfs::kVariants[v - 1].min_blocks;
-    if (prefetch) *prefetch = cfs::kVariants[v - 1].prefetch ? 1 : 0;
+    if (prefetch) *prefetch = cfs::kVariants[v - 1].load;
     return CFS_OK;
 }
 

@@ -288,21 +288,19 @@ __device__ __forceinline__ unsigned int cell_hash(int i, int j, unsigned int ste
     return fmix32(static_cast<unsigned int>(i) * 0x9e3779b1u ^ fmix32(static_cast<unsigned int>(j) ^ (step_seed * 0x632be5abu)));
 }
 
-// The float next to f (finite) in the direction of sign(dir).
-__device__ __forceinline__ float float_step(float f, double dir) {
-    if (f == 0.0f) return dir > 0 ? 1.401298464e-45f : -1.401298464e-45f;
-    const unsigned int b = __float_as_uint(f);
-    return __uint_as_float((f > 0.0f) == (dir > 0) ? b + 1u : b - 1u);
-}
-
-// x rounded to float stochastically with the 8 random bits u8.
+// x rounded to float stochastically with the 8 random bits u8: round to
+// nearest of x + (u - 1/2) g, with u = (u8 + 1/2)/256 and g the float spacing
+// of the binade of RN(x).  For x between neighbouring floats f < x < f + g this
+// picks f + g with probability (x - f)/g.  Just below a power of two the
+// spacing halves, so there the choice is only approximately unbiased; tiny and
+// non-finite values round to nearest.
 __device__ __forceinline__ float round_stochastic(double x, unsigned int u8) {
     const float f = __double2float_rn(x);
-    const double e = x - double(f);  // exact
-    if (!(fabs(e) > 0.0) || !isfinite(f)) return f;
-    const float n = float_step(f, e);
-    const double gap = fabs(double(n) - double(f));
-    return (double(u8) + 0.5) * (1.0 / 256.0) * gap < fabs(e) ? n : f;
+    const unsigned int eb = __float_as_uint(f) & 0x7f800000u;
+    if (eb <= (24u << 23) || eb == 0x7f800000u) return f;
+    const float g = __uint_as_float(eb - (23u << 23));
+    const float noise = (static_cast<float>(u8) - 127.5f) * (1.0f / 256.0f) * g;
+    return __double2float_rn(x + static_cast<double>(noise));
 }
 
 // (|u| + a)/dx + (|v| + a)/dy of one cell, FP64, in the order of the CFL

@@ -32,12 +32,12 @@ cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const doub
 // Stage-kernel variants of the throughput forms (march_kernel template shapes).
 struct MarchVariant {
     int rows, warps, min_blocks;
-    bool prefetch;  // software-prefetching form of the row march
+    int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead
 };
-constexpr int kNumVariants = 10;
+constexpr int kNumVariants = 14;
 constexpr MarchVariant kVariants[kNumVariants] = {
-    {64, 4, 1, false}, {64, 4, 4, false}, {64, 4, 5, false}, {32, 4, 5, false}, {128, 4, 4, false},
-    {64, 8, 2, false}, {64, 4, 4, true},  {32, 4, 5, true},  {64, 4, 3, true},  {64, 8, 2, true},
+    {64, 4, 1, 0}, {64, 4, 4, 0}, {64, 4, 5, 0}, {32, 4, 5, 0}, {128, 4, 4, 0}, {64, 8, 2, 0}, {64, 4, 4, 2},
+    {32, 4, 5, 2}, {64, 4, 3, 2}, {64, 8, 2, 2}, {64, 4, 4, 1}, {32, 4, 5, 1}, {64, 8, 2, 1}, {32, 4, 4, 1},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).

@@ -72,14 +72,72 @@ __device__ __forceinline__ void weno5_pair(C v0, C v1, C v2, C v3, C v4, C eps, 
     weno5_pair_diff(v0, v1, v2, v3, v4, C(12.0 / 13.0) * eps, left, right);
 }
 
-// Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).
+// The same pair for two variables at once in packed FP32 (sm_100 FFMA2 /
+// FADD2 / FMUL2: two independent FP32 operations per instruction, each rounded
+// as its scalar form), for the FP32-mixed form, whose row loop is bound by
+// instruction issue.  The reciprocals stay scalar.
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, p2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, float2 v3, float2 v4, float eps,
+                                              float2& left, float2& right) {
+    const float2 D1 = sub2(v1, v0), D2 = sub2(v2, v1), D3 = sub2(v3, v2), D4 = sub2(v4, v3);
+    const float2 d0 = sub2(D2, D1), d1 = sub2(D3, D2), d2 = sub2(D4, D3);
+    const float2 e0 = fma2(p2(3.0f), D2, mul2(p2(-1.0f), D1)), e1 = add2(D2, D3), e2 = fma2(p2(-3.0f), D3, D4);
+    const float2 k = p2(float(3.0 / 13.0));
+    float2 b0 = fma2(d0, d0, mul2(k, mul2(e0, e0)));
+    float2 b1 = fma2(d1, d1, mul2(k, mul2(e1, e1)));
+    float2 b2 = fma2(d2, d2, mul2(k, mul2(e2, e2)));
+    b0 = make_float2(fminf(b0.x, 1e9f), fminf(b0.y, 1e9f));
+    b1 = make_float2(fminf(b1.x, 1e9f), fminf(b1.y, 1e9f));
+    b2 = make_float2(fminf(b2.x, 1e9f), fminf(b2.y, 1e9f));
+    const float2 es = p2(float(12.0 / 13.0) * eps);
+    float2 q0 = add2(es, b0), q1 = add2(es, b1), q2 = add2(es, b2);
+    q0 = mul2(q0, q0);
+    q1 = mul2(q1, q1);
+    q2 = mul2(q2, q2);
+    const float2 q01 = mul2(q0, q1), q12 = mul2(q1, q2), a1 = mul2(p2(6.0f), mul2(q0, q2));
+    const float2 a2L = mul2(p2(3.0f), q01), a2R = mul2(p2(3.0f), q12);
+    const float2 c0 = fma2(p2(float(5.0 / 6.0)), D2, mul2(p2(float(-1.0 / 3.0)), D1));
+    const float2 c1 = fma2(p2(float(1.0 / 3.0)), D3, mul2(p2(float(1.0 / 6.0)), D2));
+    const float2 c2 = fma2(p2(float(2.0 / 3.0)), D3, mul2(p2(float(-1.0 / 6.0)), D4));
+    const float2 r0 = fma2(p2(float(1.0 / 3.0)), D4, mul2(p2(float(-5.0 / 6.0)), D3));
+    const float2 r1 = fma2(p2(float(-1.0 / 3.0)), D2, mul2(p2(float(-1.0 / 6.0)), D3));
+    const float2 r2 = fma2(p2(float(1.0 / 6.0)), D1, mul2(p2(float(-2.0 / 3.0)), D2));
+    const float2 sL = add2(add2(q12, a1), a2L), sR = add2(add2(q01, a1), a2R);
+    const float2 iL = make_float2(rcp_fast(sL.x), rcp_fast(sL.y)), iR = make_float2(rcp_fast(sR.x), rcp_fast(sR.y));
+    left = fma2(fma2(q12, c0, fma2(a1, c1, mul2(a2L, c2))), iL, v2);
+    right = fma2(fma2(q01, r0, fma2(a1, r1, mul2(a2R, r2))), iR, v2);
+}
+
+// Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).  The
+// FP32-mixed form pairs (rho, rho u) and (rho v, E) in packed instructions.
 template <class Pol>
 __device__ __forceinline__ void cell_states(const typename Pol::C st[5][kVars], typename Pol::C eps, double g,
                                             Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
-    weno5_pair(st[0][0], st[1][0], st[2][0], st[3][0], st[4][0], eps, L.r, R.r);
-    weno5_pair(st[0][1], st[1][1], st[2][1], st[3][1], st[4][1], eps, L.mx, R.mx);
-    weno5_pair(st[0][2], st[1][2], st[2][2], st[3][2], st[4][2], eps, L.my, R.my);
-    weno5_pair(st[0][3], st[1][3], st[2][3], st[3][3], st[4][3], eps, L.E, R.E);
+    if constexpr (Pol::kMixed) {
+        float2 l, r;
+        weno5_pair_x2(make_float2(st[0][0], st[0][1]), make_float2(st[1][0], st[1][1]), make_float2(st[2][0], st[2][1]),
+                      make_float2(st[3][0], st[3][1]), make_float2(st[4][0], st[4][1]), eps, l, r);
+        L.r = l.x;
+        L.mx = l.y;
+        R.r = r.x;
+        R.mx = r.y;
+        weno5_pair_x2(make_float2(st[0][2], st[0][3]), make_float2(st[1][2], st[1][3]), make_float2(st[2][2], st[2][3]),
+                      make_float2(st[3][2], st[3][3]), make_float2(st[4][2], st[4][3]), eps, l, r);
+        L.my = l.x;
+        L.E = l.y;
+        R.my = r.x;
+        R.E = r.y;
+    } else {
+        weno5_pair(st[0][0], st[1][0], st[2][0], st[3][0], st[4][0], eps, L.r, R.r);
+        weno5_pair(st[0][1], st[1][1], st[2][1], st[3][1], st[4][1], eps, L.mx, R.mx);
+        weno5_pair(st[0][2], st[1][2], st[2][2], st[3][2], st[4][2], eps, L.my, R.my);
+        weno5_pair(st[0][3], st[1][3], st[2][3], st[3][3], st[4][3], eps, L.E, R.E);
+    }
     finish_state<Pol>(L, g);
     finish_state<Pol>(R, g);
 }
@@ -130,11 +188,15 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 
 // One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
 // block column bx.  Each warp works on its own segment; the warps of a block
-// share nothing but their slices of the row buffer.  kPf: software prefetch -
-// the next row two iterations ahead, the y halo columns one row ahead, and the
-// RK operands of the row being updated before its x reconstruction - so that
-// global-load latency overlaps a row of arithmetic.
-template <class Pol, int kWarps, bool kPf = false>
+// share nothing but their slices of the row buffer.  kLoad, where global loads
+// are issued (the trade is latency hidden against registers held):
+//   0 at their use;
+//   1 early in the iteration: the next row, the y halo columns and the RK
+//     operands right after the row's x reconstruction, ahead of the update and
+//     the y work that precede their use;
+//   2 ahead: the next row two iterations ahead, the halo columns one row ahead,
+//     the RK operands before the x reconstruction.
+template <class Pol, int kWarps, int kLoad = 0>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][kVars][36]) {
     using T = typename Pol::T;
@@ -226,8 +288,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     };
 
     C win[5][kVars];
-    C nxt[kVars];   // kPf: the row after win[4]
-    C hal[kVars];   // kPf: halo columns of the next y row
+    C nxt[kVars];   // kLoad 1, 2: the row after win[4]
+    C hal[kVars];   // kLoad 1, 2: halo columns of the next y row
     Face5<C> Lx{};                             // left x-state of the previous row
     C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
     C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
@@ -235,18 +297,23 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     if (active_warp) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) load_row(i0 - 3 + k, win[k]);
-        if constexpr (kPf) {
+        if constexpr (kLoad == 2) {
             load_row(i0 + 2, nxt);
             load_halo(i0, hal);
         }
     }
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
-        if constexpr (kPf) {
+        if constexpr (kLoad == 2) {
             if (r - 1 >= i0 && owner) load_update(r - 1);
         }
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
         cell_states<Pol>(win, eps, g, Lr, Rr);
+        if constexpr (kLoad == 1) {
+            if (r < i1) load_row(r + 3, nxt);
+            if (r - 1 >= i0 && owner) load_update(r - 1);
+            if (r >= i0 && r < i1) load_halo(r, hal);
+        }
         C FX[kVars] = {C(0), C(0), C(0), C(0)};
         if (r >= i0) {
             Face5<C> Lf = Lx;
@@ -262,7 +329,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             // ---- update of row r-1 (its upper x-face is r - 1/2)
             const int i = r - 1;
             if (i >= i0 && owner) {
-                if constexpr (!kPf) load_update(i);
+                if constexpr (kLoad == 0) load_update(i);
                 const bool fluid = pf_fluid;
                 const long long off = L.offset(i, j);
                 const T* u1 = static_cast<const T*>(a.u1);
@@ -327,7 +394,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             C* rb = &rbuf[wid][0][0];
 #pragma unroll
             for (int v = 0; v < kVars; ++v) rb[v * 36 + lane + 2] = win[2][v];
-            if constexpr (!kPf) load_halo(r, hal);
+            if constexpr (kLoad == 0) load_halo(r, hal);
             if (lane < 2 || lane >= 30) {
                 const int slot = lane < 2 ? lane : lane + 4;
 #pragma unroll
@@ -385,11 +452,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             for (int k = 0; k < 4; ++k)
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[k][v] = win[k + 1][v];
-            if constexpr (kPf) {
+            if constexpr (kLoad == 2) {
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[4][v] = nxt[v];
                 if (r + 4 <= i1 + 2) load_row(r + 4, nxt);
                 if (r + 1 < i1) load_halo(r + 1, hal);
+            } else if constexpr (kLoad == 1) {
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) win[4][v] = nxt[v];
             } else {
                 load_row(r + 3, win[4]);
             }
@@ -405,10 +475,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     }
 }
 
-template <class Pol, int kRows, int kWarps, int kMinBlocks, bool kPf>
+template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ typename Pol::C rbuf[kWarps][kVars][36];
-    march_item<Pol, kWarps, kPf>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+    march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
 }
 
 // Persistent batched form: one launch runs one stage of every case of a batch.

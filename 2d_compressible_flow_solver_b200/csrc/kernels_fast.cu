@@ -6,23 +6,23 @@
 
 namespace cfs {
 
-template <class Pol, int R, int W, int B, bool Pf>
+template <class Pol, int R, int W, int B, int Ld>
 cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     const int nseg = (a.L.ny + kSeg - 1) / kSeg;
     const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
-    march_kernel<Pol, R, W, B, Pf><<<grid, 32 * W, 0, s>>>(a);
+    march_kernel<Pol, R, W, B, Ld><<<grid, 32 * W, 0, s>>>(a);
     return cudaGetLastError();
 }
 
 template <class Pol, int K>
 cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
     constexpr MarchVariant v = kVariants[K];
-    return launch_march<Pol, v.rows, v.warps, v.min_blocks, v.prefetch>(a, s);
+    return launch_march<Pol, v.rows, v.warps, v.min_blocks, v.load>(a, s);
 }
 
 template <class Pol>
 cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
-    static_assert(kNumVariants == 10, "variant table and dispatch disagree");
+    static_assert(kNumVariants == 14, "variant table and dispatch disagree");
     switch (v) {
         case 1: return launch_march_k<Pol, 0>(a, s);
         case 2: return launch_march_k<Pol, 1>(a, s);
@@ -34,6 +34,10 @@ cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
         case 8: return launch_march_k<Pol, 7>(a, s);
         case 9: return launch_march_k<Pol, 8>(a, s);
         case 10: return launch_march_k<Pol, 9>(a, s);
+        case 11: return launch_march_k<Pol, 10>(a, s);
+        case 12: return launch_march_k<Pol, 11>(a, s);
+        case 13: return launch_march_k<Pol, 12>(a, s);
+        case 14: return launch_march_k<Pol, 13>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

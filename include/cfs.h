@@ -122,8 +122,9 @@ typedef struct cfs_ctx cfs_ctx;
 
 /* Number of stage-kernel variants of the throughput forms, and the shape of
  * variant v (1-based): rows marched per warp, warps per block, minimum resident
- * blocks per SM requested from the compiler, and whether the row march
- * prefetches its loads a row ahead (1) or loads at the point of use (0).
+ * blocks per SM requested from the compiler, and the row march's load schedule
+ * (0: loads at their use; 1: issued early in each row's iteration; 2: two rows
+ * ahead).
  * Returns CFS_ERR_INVALID for an unknown v. */
 int cfs_variant_count(void);
 int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks, int* prefetch);
