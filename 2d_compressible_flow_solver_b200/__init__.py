@@ -24,7 +24,7 @@ __all__ = [
     "FP64", "FP32_MIXED", "FP64_EXACT", "RK_TVD2", "RK_TVD3_REFERENCE", "RK_SSP3",
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
-    "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "ROUND_STOCHASTIC",
+    "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "POSITIVITY_FLOOR", "ROUND_STOCHASTIC",
     "ROUND_NEAREST", "variants",
 ]
 
@@ -39,7 +39,7 @@ BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC, BC_HALO = 0, 1, 2, 3
 CELL_FLUID, CELL_SOLID, CELL_IMMERSED_GHOST = 0, 1, 2
 IB_REFERENCE, IB_BILINEAR_SLIP = 0, 1
 VISCOUS_OFF, VISCOUS_NS = 0, 1
-POSITIVITY_OFF, POSITIVITY_FACE, POSITIVITY_BODY = 0, 1, 2
+POSITIVITY_OFF, POSITIVITY_FACE, POSITIVITY_BODY, POSITIVITY_FLOOR = 0, 1, 2, 3
 ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)

@@ -112,7 +112,7 @@ int validate(const cfs_config* g, std::string& msg) {
         }
     if (g->viscous != CFS_VISCOUS_OFF && g->viscous != CFS_VISCOUS_NS) { msg = "unknown viscous mode"; return CFS_ERR_INVALID; }
     if (g->variant < 0 || g->variant > cfs::kNumVariants) { msg = "unknown kernel variant"; return CFS_ERR_INVALID; }
-    if (g->positivity < CFS_POSITIVITY_OFF || g->positivity > CFS_POSITIVITY_BODY) {
+    if (g->positivity < CFS_POSITIVITY_OFF || g->positivity > CFS_POSITIVITY_FLOOR) {
         msg = "unknown positivity mode";
         return CFS_ERR_INVALID;
     }
@@ -150,7 +150,7 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.positivity = c->cfg.positivity;
     a.rounding = c->cfg.rounding;
     a.seed = c->steps_done;
-    a.lowo = c->cfg.positivity == CFS_POSITIVITY_BODY && c->has_types ? c->lowo_d : nullptr;
+    a.lowo = c->cfg.positivity >= CFS_POSITIVITY_BODY && c->has_types ? c->lowo_d : nullptr;
     return a;
 }
 
@@ -499,7 +499,7 @@ int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
     CFS_CUDA(c, cudaMemcpy(c->types_d, types, n, cudaMemcpyHostToDevice));
     c->types_h.assign(types, types + n);
     c->has_types = true;
-    if (c->cfg.positivity == CFS_POSITIVITY_BODY) {
+    if (c->cfg.positivity >= CFS_POSITIVITY_BODY) {
         const std::vector<uint8_t> f = cfs::low_order_faces(types, c->cfg.nx, c->cfg.ny, c->cfg.bc);
         if (!c->lowo_d) CFS_CUDA(c, cudaMalloc(&c->lowo_d, f.size()));
         CFS_CUDA(c, cudaMemcpy(c->lowo_d, f.data(), f.size(), cudaMemcpyHostToDevice));

@@ -225,7 +225,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         !(common->weno_eps > 0))
         return bfail(nullptr, CFS_ERR_INVALID, "bad common configuration");
     if (common->viscous != CFS_VISCOUS_OFF) return bfail(nullptr, CFS_ERR_INVALID, "batches are inviscid");
-    if (common->positivity < CFS_POSITIVITY_OFF || common->positivity > CFS_POSITIVITY_BODY)
+    if (common->positivity < CFS_POSITIVITY_OFF || common->positivity > CFS_POSITIVITY_FLOOR)
         return bfail(nullptr, CFS_ERR_INVALID, "unknown positivity mode");
     if (common->rounding != CFS_ROUND_STOCHASTIC && common->rounding != CFS_ROUND_NEAREST)
         return bfail(nullptr, CFS_ERR_INVALID, "unknown rounding mode");
@@ -293,7 +293,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
             c.types = ib.types;
             c.types_off = static_cast<long long>(types_bytes);
             types_bytes += c.types.size();
-            if (common->positivity == CFS_POSITIVITY_BODY) {
+            if (common->positivity >= CFS_POSITIVITY_BODY) {
                 c.lowo = cfs::low_order_faces(c.types.data(), d.nx, d.ny, d.bc);
                 c.lowo_off = static_cast<long long>(lowo_bytes);
                 lowo_bytes += c.lowo.size();

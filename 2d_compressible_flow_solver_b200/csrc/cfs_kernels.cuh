@@ -303,6 +303,34 @@ __device__ __forceinline__ float round_stochastic(double x, unsigned int u8) {
     return __double2float_rn(x + static_cast<double>(noise));
 }
 
+// Positivity floors of CFS_POSITIVITY_FLOOR (no reference counterpart): a new
+// state with rho <= kRhoFloor or p <= kPFloor (or a NaN) is raised to them --
+// rho to its floor with the velocity kept, then E so that p reaches its floor;
+// a NaN state becomes the floor state at rest.
+constexpr double kRhoFloor = 1e-6, kPFloor = 1e-6;
+constexpr int kPosFloor = 3;
+
+__device__ __forceinline__ void floor_state(double s[kVars], double g) {
+    double rho = s[0], mx = s[1], my = s[2], E = s[3];
+    if (!(rho == rho) || !(mx == mx) || !(my == my) || !(E == E)) {
+        rho = kRhoFloor;
+        mx = my = 0.0;
+        E = kPFloor / (g - 1);
+    }
+    if (!(rho > kRhoFloor)) {
+        const double f = rho > 0 ? kRhoFloor / rho : 0.0;
+        mx *= f;
+        my *= f;
+        rho = kRhoFloor;
+    }
+    const double ke = 0.5 * (mx * mx + my * my) / rho;
+    if (!((g - 1) * (E - ke) > kPFloor)) E = kPFloor / (g - 1) + ke;
+    s[0] = rho;
+    s[1] = mx;
+    s[2] = my;
+    s[3] = E;
+}
+
 // (|u| + a)/dx + (|v| + a)/dy of one cell, FP64, in the order of the CFL
 // reduction every caller shares.
 __device__ __forceinline__ double wave_sum(double rho, double mx, double my, double E, double g, double dx, double dy) {

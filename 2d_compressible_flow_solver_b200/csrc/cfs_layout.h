@@ -91,7 +91,7 @@ struct StageArgs {
     int first_stage;       // 1: reset P->wmax[1-parity], advance P->t
     const void* rv;        // optional viscous RHS (rho u, rho v, E) [3][nx][ny], storage type
     int variant;           // throughput-form kernel variant (1-based; 0 = default)
-    int positivity;        // 0 off, 1 face-state fallback, 2 also first order near the body
+    int positivity;        // 0 off, 1 face-state fallback, 2 also first order near the body, 3 also floors
     const uint8_t* lowo;   // positivity 2: [nx+1][ny+1] face flags, bit 0 x-face (i-1/2, j),
                            // bit 1 y-face (i, j-1/2): stencil holds a non-fluid cell
     int rounding;          // FP32 storage: 0 stochastic, 1 to nearest

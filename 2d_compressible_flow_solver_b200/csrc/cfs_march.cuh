@@ -382,6 +382,21 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
                     }
                 }
+                if (a.positivity >= kPosFloor && fluid) {
+                    const C pr = (C(g) - C(1)) * (nv[3] - C(0.5) * (nv[1] * nv[1] + nv[2] * nv[2]) / nv[0]);
+                    if (!(nv[0] > C(kRhoFloor)) || !(pr > C(kPFloor))) {
+                        double s[kVars];
+#pragma unroll
+                        for (int v = 0; v < kVars; ++v)
+                            s[v] = Pol::kMixed ? double(sv[v]) + double(L.off[v]) : double(nv[v]);
+                        floor_state(s, g);
+#pragma unroll
+                        for (int v = 0; v < kVars; ++v) {
+                            sv[v] = Pol::kMixed ? T(s[v] - double(L.off[v])) : T(s[v]);
+                            nv[v] = C(s[v]);
+                        }
+                    }
+                }
                 store_cell4<T>(out, L, a.bc, i, j, sv);
                 if (a.P && a.last_stage && a.P->use_cfl && fluid) {
                     const C w = wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy));

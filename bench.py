@@ -393,11 +393,11 @@ def batch_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
     out = {"workload": f"{args.cases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
-                       "cylinder (slip wall), SSP-RK3, Davis HLL, body positivity fallback, per-case CFL 0.5",
+                       "cylinder (slip wall), SSP-RK3, Davis HLL, positivity fallbacks with floors, per-case CFL 0.5",
            "steps": K, "warmup": W}
 
     def run_batch(prec):
-        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_BODY, device=local) as b:
+        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR, device=local) as b:
             cells, items = b.info()
             for k, U in enumerate(states):
                 b.set_state(k, U)
@@ -418,7 +418,7 @@ def batch_arm(args):
     solvers = []
     for c, U in zip(cases, states):
         s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
-                        bc=c["bc"], bc_prim=c.get("bc_prim"), positivity=cfsb.POSITIVITY_BODY, device=local)
+                        bc=c["bc"], bc_prim=c.get("bc_prim"), positivity=cfsb.POSITIVITY_FLOOR, device=local)
         if "circle" in c:
             s.build_circle(*c["circle"], 400, cfsb.IB_BILINEAR_SLIP)
         s.set_state(U)
@@ -445,6 +445,93 @@ def batch_arm(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ report arm
+def _errors(a, b):
+    """L1 / L-infinity of rho and E between two states."""
+    return {"rho_L1": float(np.abs(a[0] - b[0]).mean()), "rho_Linf": float(np.abs(a[0] - b[0]).max()),
+            "E_L1": float(np.abs(a[3] - b[3]).mean()), "E_Linf": float(np.abs(a[3] - b[3]).max())}
+
+
+def report_arm(args):
+    """Accuracy and conservation of the FP32-mixed form against FP64 on the
+    configurations beside the headline: four-quadrant Riemann problems (256^2,
+    200 steps, the reference's scheme: TVD3 as written + its HLL, where the FP64
+    form is also compared with the exact form, the reference's arithmetic), the
+    Mach-3 cylinder (2048 x 1024, 3000 steps, slip wall, positivity fallbacks with floors), the
+    Navier-Stokes shear layer (1024^2, 5000 steps) and the uneven batch (512
+    cases, 100 steps).  Open boundaries (quadrants, cylinder): drift is the
+    FP32-vs-FP64 difference of the totals; periodic shear layer: the change of
+    each form's totals.  One JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    cfsb = importlib.import_module(PKG)
+    wl = importlib.import_module(f"{PKG}.workloads")
+    out = {"report": "FP32-mixed vs FP64 at t_end per configuration"}
+
+    def run(w, prec, steps, cfl, extra, circle=None, ib_mode=None):
+        with cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, bc=w.bc, bc_prim=w.bc_prim, **extra) as s:
+            if circle is not None:
+                s.build_circle(*circle, 400, ib_mode)
+            s.set_state(w.U0)
+            m0 = s.totals()
+            t0 = time.perf_counter()
+            t, _ = s.advance(steps, cfl=cfl)
+            wall = time.perf_counter() - t0
+            return s.get_state(), m0, s.totals(), t, wall
+
+    def compare(name, w, steps, cfl, extra, circle=None, ib_mode=None, exact=False, periodic=False):
+        r64 = run(w, cfsb.FP64, steps, cfl, extra, circle, ib_mode)
+        r32 = run(w, cfsb.FP32_MIXED, steps, cfl, extra, circle, ib_mode)
+        row = {"grid": [w.nx, w.ny], "steps": steps, "t_end_fp64": r64[3], "t_end_fp32": r32[3],
+               "fp32_vs_fp64": _errors(r32[0], r64[0]),
+               "finite": bool(np.all(np.isfinite(r64[0])) and np.all(np.isfinite(r32[0]))),
+               "mcell_steps_per_s": {"fp64": round(w.nx * w.ny * steps / r64[4] / 1e6, 1),
+                                     "fp32": round(w.nx * w.ny * steps / r32[4] / 1e6, 1)}}
+        if periodic:
+            row["drift_fp32"] = {"mass": float(abs(r32[2][0] - r32[1][0]) / abs(r32[1][0])),
+                                 "energy": float(abs(r32[2][3] - r32[1][3]) / abs(r32[1][3]))}
+            row["drift_fp64"] = {"mass": float(abs(r64[2][0] - r64[1][0]) / abs(r64[1][0])),
+                                 "energy": float(abs(r64[2][3] - r64[1][3]) / abs(r64[1][3]))}
+        else:
+            row["totals_fp32_vs_fp64"] = {"mass": float(abs(r32[2][0] - r64[2][0]) / abs(r64[2][0])),
+                                          "energy": float(abs(r32[2][3] - r64[2][3]) / abs(r64[2][3]))}
+        if exact:
+            rx = run(w, cfsb.FP64_EXACT, steps, cfl, extra, circle, ib_mode)
+            row["fp64_vs_exact"] = _errors(r64[0], rx[0])
+            row["exact_finite"] = bool(np.all(np.isfinite(rx[0])))
+        out[name] = row
+
+    w1 = wl.riemann_quadrants(256, 256, seed=1)
+    compare("quadrants_256_reference_scheme", w1, 200, 0.5,
+            dict(rk=cfsb.RK_TVD3_REFERENCE, hll=cfsb.HLL_REFERENCE), exact=True)
+    w3 = wl.mach3_cylinder(2048, 1024)
+    compare("mach3_cylinder_2048x1024", w3, 3000, 0.5,
+            dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, positivity=cfsb.POSITIVITY_FLOOR),
+            circle=w3.circle, ib_mode=cfsb.IB_BILINEAR_SLIP)
+    w4 = wl.shear_layer(1024)
+    compare("shear_layer_1024_ns", w4, 5000, 0.5,
+            dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, viscous=cfsb.VISCOUS_NS, mu=w4.meta["mu"], prandtl=0.72,
+                 mach=1.0), periodic=True)
+    cases, states = wl.batch_cases(args.cases, seed=1)
+    res = {}
+    for prec in (cfsb.FP64, cfsb.FP32_MIXED):
+        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR) as b:
+            for k, U in enumerate(states):
+                b.set_state(k, U)
+            b.advance(100, cfl=0.5)
+            res[prec] = [b.get_state(k) for k in range(len(cases))]
+    worst = {"rho_L1": 0.0, "rho_Linf": 0.0, "E_L1": 0.0, "E_Linf": 0.0}
+    finite = True
+    for a, b in zip(res[cfsb.FP32_MIXED], res[cfsb.FP64]):
+        e = _errors(a, b)
+        finite = finite and bool(np.all(np.isfinite(a)) and np.all(np.isfinite(b)))
+        for k in worst:
+            worst[k] = max(worst[k], e[k])
+    out["batch_512_cases_100_steps"] = {"worst_case_fp32_vs_fp64": worst, "finite": finite}
+    print(json.dumps(out), flush=True)
 
 
 # ----------------------------------------------------------- reference arm
@@ -487,14 +574,17 @@ def main():
     ap.add_argument("--n", type=int, default=4096, help="grid edge (cells) per GPU")
     ap.add_argument("--accuracy-n", type=int, default=1024, help="grid of the FP32-vs-FP64 check (0 = skip)")
     ap.add_argument("--cpu-sample", type=int, default=384, help="grid edge of one CPU-baseline sample")
-    ap.add_argument("--workload", choices=["smooth", "batch"], default="smooth",
-                    help="smooth: the headline 4096^2 line; batch: the uneven-batch comparison (one JSON line)")
+    ap.add_argument("--workload", choices=["smooth", "batch", "report"], default="smooth",
+                    help="smooth: the headline 4096^2 line; batch: the uneven-batch comparison; report: "
+                         "FP32-vs-FP64 accuracy and drift on the other configurations (one JSON line each)")
     ap.add_argument("--cases", type=int, default=512, help="cases of the batch workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "batch":
         batch_arm(args)
+    elif args.workload == "report":
+        report_arm(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

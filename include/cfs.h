@@ -85,8 +85,13 @@ enum cfs_positivity {
     CFS_POSITIVITY_OFF = 0,   /* reconstructed states used as they come (the reference) */
     CFS_POSITIVITY_FACE = 1,  /* a face state with rho <= 0 or p <= 0 (or NaN) is replaced by the
                                  value of the cell next to the face on its side (first order) */
-    CFS_POSITIVITY_BODY = 2   /* FACE, and both states of every face whose 6-cell stencil holds an
+    CFS_POSITIVITY_BODY = 2,  /* FACE, and both states of every face whose 6-cell stencil holds an
                                  immersed-ghost or solid cell are first order */
+    CFS_POSITIVITY_FLOOR = 3  /* BODY, and a fluid cell whose new state has rho <= 1e-6 or p <= 1e-6
+                                 (or a NaN) is raised to those floors: rho to its floor with the
+                                 velocity kept, then E so that p reaches its floor; a cell with a NaN
+                                 becomes the floor state at rest.  Not conservative where it acts
+                                 (near-vacuum cells) */
 };
 
 /* Rounding of the FP32 state storage of CFS_FP32_MIXED (no reference

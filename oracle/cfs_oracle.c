@@ -499,7 +499,7 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
             for (int k = 0; k < 6; ++k) {
                 const int ii = face_slot(a, k, nx, c->bc[0] == ORC_BC_PERIODIC, c->bc[1] == ORC_BC_PERIODIC);
                 for (int q = 0; q < NV; ++q) s[k][q] = cval(c, U, q, ii, j);
-                if (c->positivity == ORC_POS_BODY && types && ii >= 0 && ii < nx && types[(size_t)ii * ny + j]) lowo = 1;
+                if (c->positivity >= ORC_POS_BODY && types && ii >= 0 && ii < nx && types[(size_t)ii * ny + j]) lowo = 1;
             }
             face_flux(c, s, 0, F, lowo);
             for (int q = 0; q < NV; ++q) FX[(size_t)q * nfx + (size_t)a * ny + j] = F[q];
@@ -512,7 +512,7 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
             for (int k = 0; k < 6; ++k) {
                 const int jj = face_slot(a, k, ny, c->bc[2] == ORC_BC_PERIODIC, c->bc[3] == ORC_BC_PERIODIC);
                 for (int q = 0; q < NV; ++q) s[k][q] = cval(c, U, q, i, jj);
-                if (c->positivity == ORC_POS_BODY && types && jj >= 0 && jj < ny && types[(size_t)i * ny + jj]) lowo = 1;
+                if (c->positivity >= ORC_POS_BODY && types && jj >= 0 && jj < ny && types[(size_t)i * ny + jj]) lowo = 1;
             }
             face_flux(c, s, 1, F, lowo);
             for (int q = 0; q < NV; ++q) FY[(size_t)q * nfy + (size_t)i * (ny + 1) + a] = F[q];
@@ -538,6 +538,31 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
  * TVD3rdRK::advance (TVD3rdRK.cpp:3-48, coef TVD3rdRK.h:14-18; stage 2 uses the
  * saved stage-1 input U1).  ORC_RK_SSP3 stage 2 uses the current state instead
  * (Shu-Osher; no reference counterpart). */
+/* ORC_POS_FLOOR (no reference counterpart): a fluid cell whose new state has
+ * rho <= ORC_RHO_FLOOR or p <= ORC_P_FLOOR (or a NaN) is raised to the floors:
+ * rho to its floor with the velocity kept, then E so that p is at least its
+ * floor; a cell with a NaN becomes the floor state at rest. */
+static void floor_cell(const orc_config* c, double* U, size_t n, size_t k) {
+    double rho = U[k], mx = U[n + k], my = U[2 * n + k], E = U[3 * n + k];
+    if (!(rho == rho) || !(mx == mx) || !(my == my) || !(E == E)) {
+        rho = ORC_RHO_FLOOR;
+        mx = my = 0.0;
+        E = ORC_P_FLOOR / (c->gamma - 1);
+    }
+    if (!(rho > ORC_RHO_FLOOR)) {
+        const double s = rho > 0 ? ORC_RHO_FLOOR / rho : 0.0;
+        mx *= s;
+        my *= s;
+        rho = ORC_RHO_FLOOR;
+    }
+    const double ke = 0.5 * (mx * mx + my * my) / rho;
+    if (!((c->gamma - 1) * (E - ke) > ORC_P_FLOOR)) E = ORC_P_FLOOR / (c->gamma - 1) + ke;
+    U[k] = rho;
+    U[n + k] = mx;
+    U[2 * n + k] = my;
+    U[3 * n + k] = E;
+}
+
 int orc_stage(const orc_config* c, const uint8_t* types, const orc_ib* ib, int stage,
               double dt, double* U, double* U0, double* U1, double* rhs_out) {
     const size_t n = ncell(c);
@@ -570,6 +595,7 @@ int orc_stage(const orc_config* c, const uint8_t* types, const orc_ib* ib, int s
                 U[e] = (1.0 / 3.0) * U0[e] + (2.0 / 3.0) * U[e] + (2.0 / 3.0) * dt * r;
             }
         }
+        if (c->positivity >= ORC_POS_FLOOR) floor_cell(c, U, n, (size_t)k);
     }
     if (!rhs_out) free(R);
     return 0;

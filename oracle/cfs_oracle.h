@@ -20,7 +20,9 @@ enum { ORC_HLL_REFERENCE = 0, ORC_HLL_DAVIS = 1 };
 enum { ORC_BC_NEUMANN = 0, ORC_BC_DIRICHLET = 1, ORC_BC_PERIODIC = 2 };
 enum { ORC_CELL_FLUID = 0, ORC_CELL_SOLID = 1, ORC_CELL_GHOST = 2 };
 enum { ORC_IB_REFERENCE = 0, ORC_IB_BILINEAR_SLIP = 1 };
-enum { ORC_POS_OFF = 0, ORC_POS_FACE = 1, ORC_POS_BODY = 2 };
+enum { ORC_POS_OFF = 0, ORC_POS_FACE = 1, ORC_POS_BODY = 2, ORC_POS_FLOOR = 3 };
+#define ORC_RHO_FLOOR 1e-6
+#define ORC_P_FLOOR 1e-6
 
 typedef struct {
     int nx, ny;

@@ -168,3 +168,25 @@ def test_positivity_fallback_on_mach3_cylinder(cfsb):
             U, _ = ob.orc_run(cfg, U, 1, 3, dt=dt, types=types, ib=ib)
         finite[pos] = bool(np.all(np.isfinite(U[:, f])))
     assert finite == {0: False, 2: True}
+
+
+def test_floors_carry_a_near_vacuum(workloads):
+    """Two halves moving apart at +-4 (rho 1, p 0.4): without floors the oracle
+    reaches NaN within 10 steps; with them (ORC_POS_FLOOR) 40 steps stay finite
+    and the pressure floor is reached."""
+    X, _ = workloads.cell_centres(64, 48, 1.0, 1.0)
+    U0 = workloads.conserved(np.ones((64, 48)), np.where(X < 0.5, -4.0, 4.0), 0.0, 0.4)
+    out = {}
+    for pos in (2, 3):
+        cfg = ob.make_orc_config(64, 48, rk=2, hll=1, positivity=pos)
+        U = U0.copy()
+        pmin = np.inf
+        for _ in range(40):
+            U, _ = ob.orc_run(cfg, U, 1, 3, dt=ob.orc_cfl_dt(cfg, U, 0.5))
+            with np.errstate(invalid="ignore"):
+                pmin = min(pmin, float(np.nanmin(0.4 * (U[3] - 0.5 * (U[1] ** 2 + U[2] ** 2) / U[0]))))
+            if not np.all(np.isfinite(U)):
+                break
+        out[pos] = (bool(np.all(np.isfinite(U))), pmin)
+    assert out[2][0] is False
+    assert out[3][0] is True and out[3][1] <= 1.0000001e-6
