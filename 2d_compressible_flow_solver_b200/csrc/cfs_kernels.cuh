@@ -274,7 +274,7 @@ __device__ __forceinline__ double rk_update(int rk, int stage, double dt, double
 // nearness.  Round-to-nearest biases the error of a smooth, slowly moving
 // state (neighbouring cells and steps round the same way), so it grows with
 // the step count; stochastic rounding leaves an unbiased random walk.
-// Random bits: MurmurHash3's 32-bit finaliser (public domain) of cell and step.
+// Random bits: MurmurHash3's 32-bit finaliser (public domain) of a mix of cell and step.
 __device__ __forceinline__ unsigned int fmix32(unsigned int h) {
     h ^= h >> 16;
     h *= 0x85ebca6bu;
@@ -284,8 +284,11 @@ __device__ __forceinline__ unsigned int fmix32(unsigned int h) {
     return h;
 }
 
+// One finaliser over a linear mix of cell and step (odd multipliers, so
+// neighbouring cells and steps enter far apart).
 __device__ __forceinline__ unsigned int cell_hash(int i, int j, unsigned int step_seed) {
-    return fmix32(static_cast<unsigned int>(i) * 0x9e3779b1u ^ fmix32(static_cast<unsigned int>(j) ^ (step_seed * 0x632be5abu)));
+    return fmix32(static_cast<unsigned int>(i) * 0x9e3779b1u + static_cast<unsigned int>(j) * 0x85ebca77u +
+                  step_seed * 0xc2b2ae3du);
 }
 
 // x rounded to float stochastically with the 8 random bits u8: round to
@@ -304,24 +307,18 @@ __device__ __forceinline__ float round_stochastic(double x, unsigned int u8) {
 }
 
 // Positivity floors of CFS_POSITIVITY_FLOOR (no reference counterpart): a new
-// state with rho <= kRhoFloor or p <= kPFloor (or a NaN) is raised to them --
-// rho to its floor with the velocity kept, then E so that p reaches its floor;
-// a NaN state becomes the floor state at rest.
+// state with rho <= kRhoFloor (or a NaN) becomes the floor state at rest (the
+// velocity of a near-zero density is not kept: it would blow up); one with
+// p <= kPFloor gets E raised so that p reaches its floor, momentum kept.
 constexpr double kRhoFloor = 1e-6, kPFloor = 1e-6;
 constexpr int kPosFloor = 3;
 
 __device__ __forceinline__ void floor_state(double s[kVars], double g) {
     double rho = s[0], mx = s[1], my = s[2], E = s[3];
-    if (!(rho == rho) || !(mx == mx) || !(my == my) || !(E == E)) {
+    if (!(rho > kRhoFloor) || !(mx == mx) || !(my == my) || !(E == E)) {
         rho = kRhoFloor;
         mx = my = 0.0;
         E = kPFloor / (g - 1);
-    }
-    if (!(rho > kRhoFloor)) {
-        const double f = rho > 0 ? kRhoFloor / rho : 0.0;
-        mx *= f;
-        my *= f;
-        rho = kRhoFloor;
     }
     const double ke = 0.5 * (mx * mx + my * my) / rho;
     if (!((g - 1) * (E - ke) > kPFloor)) E = kPFloor / (g - 1) + ke;

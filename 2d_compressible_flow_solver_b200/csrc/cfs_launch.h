@@ -34,10 +34,11 @@ struct MarchVariant {
     int rows, warps, min_blocks;
     int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead
 };
-constexpr int kNumVariants = 14;
+constexpr int kNumVariants = 16;
 constexpr MarchVariant kVariants[kNumVariants] = {
     {64, 4, 1, 0}, {64, 4, 4, 0}, {64, 4, 5, 0}, {32, 4, 5, 0}, {128, 4, 4, 0}, {64, 8, 2, 0}, {64, 4, 4, 2},
     {32, 4, 5, 2}, {64, 4, 3, 2}, {64, 8, 2, 2}, {64, 4, 4, 1}, {32, 4, 5, 1}, {64, 8, 2, 1}, {32, 4, 4, 1},
+    {32, 4, 6, 0}, {32, 8, 3, 0},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).

@@ -162,6 +162,34 @@ __device__ __forceinline__ void boundary_face_states(const typename Pol::C c[kVa
     finish_state<Pol>(R, g);
 }
 
+// One column's 4 variables to / from the shared row buffer in vector accesses.
+template <class C>
+__device__ __forceinline__ void put_slot(C (&slot)[kVars], const C v[kVars]) {
+    if constexpr (sizeof(C) == 4) {
+        *reinterpret_cast<float4*>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        reinterpret_cast<double2*>(slot)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(slot)[1] = make_double2(v[2], v[3]);
+    }
+}
+
+template <class C>
+__device__ __forceinline__ void get_slot(const C (&slot)[kVars], C v[kVars]) {
+    if constexpr (sizeof(C) == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(slot);
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else {
+        const double2 a = reinterpret_cast<const double2*>(slot)[0], b = reinterpret_cast<const double2*>(slot)[1];
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+}
+
 // Positivity fallbacks (no reference counterpart).  A face state is admissible
 // when rho > 0 and p > 0 (NaN fails); otherwise, or when the face is flagged
 // low order, it becomes the value of the cell next to the face on its side.
@@ -198,7 +226,7 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 //     the RK operands before the x reconstruction.
 template <class Pol, int kWarps, int kLoad = 0>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
-                                           typename Pol::C (&rbuf)[kWarps][kVars][36]) {
+                                           typename Pol::C (&rbuf)[kWarps][36][kVars]) {
     using T = typename Pol::T;
     using C = typename Pol::C;
     const Layout& L = a.L;
@@ -406,21 +434,16 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
         // ---- y work of row r
         if (r >= i0 && r < i1) {
-            C* rb = &rbuf[wid][0][0];
-#pragma unroll
-            for (int v = 0; v < kVars; ++v) rb[v * 36 + lane + 2] = win[2][v];
+            // slot-major row buffer: the 4 variables of a column are one
+            // 16-byte (FP32) or two 16-byte (FP64) shared accesses
+            C(*rb)[kVars] = rbuf[wid];
+            put_slot<C>(rb[lane + 2], win[2]);
             if constexpr (kLoad == 0) load_halo(r, hal);
-            if (lane < 2 || lane >= 30) {
-                const int slot = lane < 2 ? lane : lane + 4;
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) rb[v * 36 + slot] = hal[v];
-            }
+            if (lane < 2 || lane >= 30) put_slot<C>(rb[lane < 2 ? lane : lane + 4], hal);
             __syncwarp();
             C st[5][kVars];
 #pragma unroll
-            for (int k = 0; k < 5; ++k)
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) st[k][v] = rb[v * 36 + lane + k];
+            for (int k = 0; k < 5; ++k) get_slot<C>(rb[lane + k], st[k]);
             Face5<C> Ly, Ry;
             cell_states<Pol>(st, eps, g, Ly, Ry);
             // right state of the cell above (lane + 1)
@@ -492,7 +515,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 
 template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
-    __shared__ typename Pol::C rbuf[kWarps][kVars][36];
+    __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
     march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
 }
 
@@ -506,7 +529,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
     batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ item_case,
                        const int* __restrict__ item_local, const int* __restrict__ case_rows,
                        const int* __restrict__ case_items_x, int total, unsigned int* counter) {
-    __shared__ typename Pol::C rbuf[kWarps][kVars][36];
+    __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
     __shared__ int s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));

@@ -22,7 +22,7 @@ cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
 
 template <class Pol>
 cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
-    static_assert(kNumVariants == 14, "variant table and dispatch disagree");
+    static_assert(kNumVariants == 16, "variant table and dispatch disagree");
     switch (v) {
         case 1: return launch_march_k<Pol, 0>(a, s);
         case 2: return launch_march_k<Pol, 1>(a, s);
@@ -38,6 +38,8 @@ cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
         case 12: return launch_march_k<Pol, 11>(a, s);
         case 13: return launch_march_k<Pol, 12>(a, s);
         case 14: return launch_march_k<Pol, 13>(a, s);
+        case 15: return launch_march_k<Pol, 14>(a, s);
+        case 16: return launch_march_k<Pol, 15>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

