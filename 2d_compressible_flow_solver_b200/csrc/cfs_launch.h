@@ -32,13 +32,14 @@ cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const doub
 // Stage-kernel variants of the throughput forms (march_kernel template shapes).
 struct MarchVariant {
     int rows, warps, min_blocks;
-    int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead
+    int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead,
+               // 3 rows staged in shared memory by cp.async (FP32 form; FP64 runs 0)
 };
-constexpr int kNumVariants = 16;
+constexpr int kNumVariants = 20;
 constexpr MarchVariant kVariants[kNumVariants] = {
     {64, 4, 1, 0}, {64, 4, 4, 0}, {64, 4, 5, 0}, {32, 4, 5, 0}, {128, 4, 4, 0}, {64, 8, 2, 0}, {64, 4, 4, 2},
     {32, 4, 5, 2}, {64, 4, 3, 2}, {64, 8, 2, 2}, {64, 4, 4, 1}, {32, 4, 5, 1}, {64, 8, 2, 1}, {32, 4, 4, 1},
-    {32, 4, 6, 0}, {32, 8, 3, 0},
+    {32, 4, 6, 0}, {32, 8, 3, 0}, {32, 4, 5, 3}, {32, 4, 4, 3}, {64, 4, 4, 3}, {32, 4, 6, 3},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).

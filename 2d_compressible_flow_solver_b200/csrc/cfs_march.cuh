@@ -162,6 +162,28 @@ __device__ __forceinline__ void boundary_face_states(const typename Pol::C c[kVa
     finish_state<Pol>(R, g);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80+): 4 bytes each, zero
+// filled without reading when `valid` is false (gmem must still be a valid
+// address); completion per thread in commit groups.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Ring of staged rows of the FP32 row march (load schedule 3), per warp: kRingRows
+// rows of its 36 columns (the segment and 2 halo columns each side), stored
+// values, and the same rows of U^0 for its 32 lanes.
+constexpr int kRingRows = 8, kRingDist = 2;
+constexpr int kRingRowWords = 36 * kVars, kRingU0Words = 32 * kVars;
+constexpr int kRingWords = kRingRows * (kRingRowWords + kRingU0Words);
+
 // One column's 4 variables to / from the shared row buffer in vector accesses.
 template <class C>
 __device__ __forceinline__ void put_slot(C (&slot)[kVars], const C v[kVars]) {
@@ -223,12 +245,21 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 //     operands right after the row's x reconstruction, ahead of the update and
 //     the y work that precede their use;
 //   2 ahead: the next row two iterations ahead, the halo columns one row ahead,
-//     the RK operands before the x reconstruction.
+//     the RK operands before the x reconstruction;
+//   3 (FP32 form; the FP64 form uses 0) staged: every row of the segment (with
+//     its halo columns) and of U^0 is copied asynchronously (cp.async) into a
+//     per-warp shared ring `ring` kRingDist rows ahead of its use; the x and y
+//     stencils, the stored value and U^0 of the update are read from the ring,
+//     so no row window is held in registers and load latency overlaps rows of
+//     arithmetic.
 template <class Pol, int kWarps, int kLoad = 0>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
-                                           typename Pol::C (&rbuf)[kWarps][36][kVars]) {
+                                           typename Pol::C (&rbuf)[kWarps][36][kVars],
+                                           typename Pol::T* ring = nullptr) {
     using T = typename Pol::T;
     using C = typename Pol::C;
+    constexpr bool kRing = kLoad == 3 && sizeof(T) == 4;
+    constexpr int kL = (kLoad == 3 && !kRing) ? 0 : kLoad;  // effective schedule
     const Layout& L = a.L;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int seg = bx * kWarps + wid;
@@ -315,6 +346,40 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
     };
 
+    // Load schedule 3: this warp's ring (rows and U^0 rows, see kRingWords).
+    T* const rw = kRing ? ring + wid * kRingWords : nullptr;
+    T* const ru0 = kRing ? rw + kRingRows * kRingRowWords : nullptr;
+    auto ring_row = [&](int q) -> T* { return rw + (q & (kRingRows - 1)) * kRingRowWords; };
+    auto ring_u0 = [&](int q) -> T* { return ru0 + (q & (kRingRows - 1)) * kRingU0Words; };
+    // Issue the copies of row q (the lane's column; halo lanes also their
+    // halo column) and, for an updated row, of its U^0; one commit group per
+    // row (empty past the last row needed, so group counts stay uniform).
+    auto issue_row = [&](int q) {
+        if constexpr (kRing) {
+            if (q <= i1 + 2) {
+                T* dst = ring_row(q);
+                const long long off = L.offset(q, col_ok ? j : 0);
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) cp_async4(dst + (lane + 2) * kVars + v, in + v * L.plane + off, col_ok);
+                if (lane < 2 || lane >= 30) {
+                    const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
+                    const bool ok = hc <= L.ny + kGhost - 1;
+                    const long long hoff = L.offset(q, ok ? hc : 0);
+                    const int slot = lane < 2 ? lane : lane + 4;
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) cp_async4(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
+                }
+                if (a.stage >= 1 && owner && q >= i0 && q < i1) {
+                    T* du = ring_u0(q);
+                    const T* u0p = static_cast<const T*>(a.u0);
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) cp_async4(du + lane * kVars + v, u0p + v * L.plane + off, true);
+                }
+            }
+            cp_async_commit();
+        }
+    };
+
     C win[5][kVars];
     C nxt[kVars];   // kLoad 1, 2: the row after win[4]
     C hal[kVars];   // kLoad 1, 2: halo columns of the next y row
@@ -322,22 +387,38 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
     C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
     double wloc = 0.0;
-    if (active_warp) {
+    if (active_warp && kRing) {
+        for (int q = i0 - 3; q <= i0 + 1 + kRingDist; ++q) issue_row(q);
+    } else if (active_warp) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) load_row(i0 - 3 + k, win[k]);
-        if constexpr (kLoad == 2) {
+        if constexpr (kL == 2) {
             load_row(i0 + 2, nxt);
             load_halo(i0, hal);
         }
     }
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
-        if constexpr (kLoad == 2) {
+        if constexpr (kRing) {
+            // every lane is done with the previous iteration's slots; the slot
+            // now refilled held row r+3+kRingDist-kRingRows, last read at r-1
+            __syncwarp();
+            issue_row(r + 3 + kRingDist);
+            cp_async_wait<kRingDist + 1>();  // this lane's copies of rows <= r+2 have landed
+            __syncwarp();                    // ... and every lane's
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const T* src = ring_row(r - 2 + k) + (lane + 2) * kVars;
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) win[k][v] = decc<T, C>(src[v], L, v);
+            }
+        }
+        if constexpr (kL == 2) {
             if (r - 1 >= i0 && owner) load_update(r - 1);
         }
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
         cell_states<Pol>(win, eps, g, Lr, Rr);
-        if constexpr (kLoad == 1) {
+        if constexpr (kL == 1) {
             if (r < i1) load_row(r + 3, nxt);
             if (r - 1 >= i0 && owner) load_update(r - 1);
             if (r >= i0 && r < i1) load_halo(r, hal);
@@ -357,7 +438,18 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             // ---- update of row r-1 (its upper x-face is r - 1/2)
             const int i = r - 1;
             if (i >= i0 && owner) {
-                if constexpr (kLoad == 0) load_update(i);
+                if constexpr (kRing) {
+                    pf_fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+                    const T* cs = ring_row(i) + (lane + 2) * kVars;
+                    const T* us = ring_u0(i) + lane * kVars;
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) {
+                        pf_cur[v] = cs[v];
+                        pf_u0[v] = a.stage >= 1 ? us[v] : T(0);
+                    }
+                } else if constexpr (kL == 0) {
+                    load_update(i);
+                }
                 const bool fluid = pf_fluid;
                 const long long off = L.offset(i, j);
                 const T* u1 = static_cast<const T*>(a.u1);
@@ -436,14 +528,22 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         if (r >= i0 && r < i1) {
             // slot-major row buffer: the 4 variables of a column are one
             // 16-byte (FP32) or two 16-byte (FP64) shared accesses
-            C(*rb)[kVars] = rbuf[wid];
-            put_slot<C>(rb[lane + 2], win[2]);
-            if constexpr (kLoad == 0) load_halo(r, hal);
-            if (lane < 2 || lane >= 30) put_slot<C>(rb[lane < 2 ? lane : lane + 4], hal);
-            __syncwarp();
             C st[5][kVars];
+            if constexpr (kRing) {
+                const T* row = ring_row(r);
 #pragma unroll
-            for (int k = 0; k < 5; ++k) get_slot<C>(rb[lane + k], st[k]);
+                for (int k = 0; k < 5; ++k)
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) st[k][v] = decc<T, C>(row[(lane + k) * kVars + v], L, v);
+            } else {
+                C(*rb)[kVars] = rbuf[wid];
+                put_slot<C>(rb[lane + 2], win[2]);
+                if constexpr (kL == 0) load_halo(r, hal);
+                if (lane < 2 || lane >= 30) put_slot<C>(rb[lane < 2 ? lane : lane + 4], hal);
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 5; ++k) get_slot<C>(rb[lane + k], st[k]);
+            }
             Face5<C> Ly, Ry;
             cell_states<Pol>(st, eps, g, Ly, Ry);
             // right state of the cell above (lane + 1)
@@ -485,17 +585,17 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
         for (int v = 0; v < kVars; ++v) FXp[v] = FX[v];
         Lx = Lr;
-        if (r < i1) {
+        if (!kRing && r < i1) {
 #pragma unroll
             for (int k = 0; k < 4; ++k)
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[k][v] = win[k + 1][v];
-            if constexpr (kLoad == 2) {
+            if constexpr (kL == 2) {
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[4][v] = nxt[v];
                 if (r + 4 <= i1 + 2) load_row(r + 4, nxt);
                 if (r + 1 < i1) load_halo(r + 1, hal);
-            } else if constexpr (kLoad == 1) {
+            } else if constexpr (kL == 1) {
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) win[4][v] = nxt[v];
             } else {
@@ -503,6 +603,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             }
         }
     }
+    if constexpr (kRing) cp_async_wait_all();  // no copy into the ring outlives the item
     // CFL maximum: one atomic per warp (no block barrier, so the warps of a
     // block never wait for each other)
     if (a.P && a.last_stage && a.P->use_cfl) {
@@ -516,7 +617,12 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
-    march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+    if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
+        __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
+        march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
+    } else {
+        march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+    }
 }
 
 // Persistent batched form: one launch runs one stage of every case of a batch.

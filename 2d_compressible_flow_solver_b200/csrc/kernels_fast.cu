@@ -22,7 +22,7 @@ cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
 
 template <class Pol>
 cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
-    static_assert(kNumVariants == 16, "variant table and dispatch disagree");
+    static_assert(kNumVariants == 20, "variant table and dispatch disagree");
     switch (v) {
         case 1: return launch_march_k<Pol, 0>(a, s);
         case 2: return launch_march_k<Pol, 1>(a, s);
@@ -40,6 +40,10 @@ cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
         case 14: return launch_march_k<Pol, 13>(a, s);
         case 15: return launch_march_k<Pol, 14>(a, s);
         case 16: return launch_march_k<Pol, 15>(a, s);
+        case 17: return launch_march_k<Pol, 16>(a, s);
+        case 18: return launch_march_k<Pol, 17>(a, s);
+        case 19: return launch_march_k<Pol, 18>(a, s);
+        case 20: return launch_march_k<Pol, 19>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
