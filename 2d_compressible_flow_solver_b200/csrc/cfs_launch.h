@@ -43,12 +43,13 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).
-constexpr int kDefaultVariantF32 = 6;
-constexpr int kDefaultVariantF64 = 6;
+constexpr int kDefaultVariantF32 = 17;
+constexpr int kDefaultVariantF64 = 18;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
 constexpr int kBatchWarps = 4;
 constexpr int kBatchMinBlocksF32 = 5;
+constexpr int kBatchLoadF32 = 3;  // FP32 batches stage rows in the shared ring
 constexpr int kBatchMinBlocksF64 = 4;
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_items_x, int total, unsigned int* counter,

@@ -630,12 +630,14 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const St
 // counter, largest cases first, until none are left.  args[c] holds case c's
 // stage arguments (its own layout, boundaries, buffers, dt slot); rows[c] is
 // the row chunk the autotuner chose for its size.
-template <class Pol, int kWarps, int kMinBlocks>
+template <class Pol, int kWarps, int kMinBlocks, int kLoad = 0>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
     batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ item_case,
                        const int* __restrict__ item_local, const int* __restrict__ case_rows,
                        const int* __restrict__ case_items_x, int total, unsigned int* counter) {
     __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
+    constexpr bool kRing = kLoad == 3 && sizeof(typename Pol::T) == 4;
+    __shared__ __align__(16) typename Pol::T ring[kRing ? kWarps * kRingWords : 1];
     __shared__ int s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
@@ -646,7 +648,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
         const int c = item_case[w], li = item_local[w];
         const int ix = case_items_x[c];
         const StageArgs a = args[c];
-        march_item<Pol, kWarps>(a, li % ix, li / ix, case_rows[c], rbuf);
+        march_item<Pol, kWarps, kLoad>(a, li % ix, li / ix, case_rows[c], rbuf, kRing ? ring : nullptr);
     }
 }
 

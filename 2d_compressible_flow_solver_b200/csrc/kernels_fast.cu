@@ -61,7 +61,7 @@ cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_ca
                                int grid, cudaStream_t s) {
     if (total <= 0) return cudaSuccess;
     if (p == kF32Mixed)
-        batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32><<<grid, 32 * kBatchWarps, 0, s>>>(
+        batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32><<<grid, 32 * kBatchWarps, 0, s>>>(
             args, item_case, item_local, case_rows, case_items_x, total, counter);
     else
         batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64><<<grid, 32 * kBatchWarps, 0, s>>>(
@@ -72,7 +72,7 @@ cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_ca
 int batch_blocks_per_sm(Prec p) {
     int n = 0;
     if (p == kF32Mixed)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32>,
                                                       32 * kBatchWarps, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64>,
