@@ -115,19 +115,33 @@ __device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, f
 
 // Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).  The
 // FP32-mixed form pairs (rho, rho u) and (rho v, E) in packed instructions.
+// With `off` the stencil holds stored deviations (value - off[v]): WENO5 is
+// translation invariant (the difference form sees only differences), so the
+// states are reconstructed from the deviations and the offsets added once.
 template <class Pol>
 __device__ __forceinline__ void cell_states(const typename Pol::C st[5][kVars], typename Pol::C eps, double g,
-                                            Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+                                            Face5<typename Pol::C>& L, Face5<typename Pol::C>& R,
+                                            const float* off = nullptr) {
     if constexpr (Pol::kMixed) {
         float2 l, r;
         weno5_pair_x2(make_float2(st[0][0], st[0][1]), make_float2(st[1][0], st[1][1]), make_float2(st[2][0], st[2][1]),
                       make_float2(st[3][0], st[3][1]), make_float2(st[4][0], st[4][1]), eps, l, r);
+        if (off) {
+            const float2 o = make_float2(off[0], off[1]);
+            l = add2(l, o);
+            r = add2(r, o);
+        }
         L.r = l.x;
         L.mx = l.y;
         R.r = r.x;
         R.mx = r.y;
         weno5_pair_x2(make_float2(st[0][2], st[0][3]), make_float2(st[1][2], st[1][3]), make_float2(st[2][2], st[2][3]),
                       make_float2(st[3][2], st[3][3]), make_float2(st[4][2], st[4][3]), eps, l, r);
+        if (off) {
+            const float2 o = make_float2(off[2], off[3]);
+            l = add2(l, o);
+            r = add2(r, o);
+        }
         L.my = l.x;
         L.E = l.y;
         R.my = r.x;
@@ -406,10 +420,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             cp_async_wait<kRingDist + 1>();  // this lane's copies of rows <= r+2 have landed
             __syncwarp();                    // ... and every lane's
 #pragma unroll
-            for (int k = 0; k < 5; ++k) {
+            for (int k = 0; k < 5; ++k) {  // stored deviations; offsets added after the reconstruction
                 const T* src = ring_row(r - 2 + k) + (lane + 2) * kVars;
 #pragma unroll
-                for (int v = 0; v < kVars; ++v) win[k][v] = decc<T, C>(src[v], L, v);
+                for (int v = 0; v < kVars; ++v) win[k][v] = C(src[v]);
             }
         }
         if constexpr (kL == 2) {
@@ -417,7 +431,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
-        cell_states<Pol>(win, eps, g, Lr, Rr);
+        cell_states<Pol>(win, eps, g, Lr, Rr, kRing ? L.off : nullptr);
         if constexpr (kL == 1) {
             if (r < i1) load_row(r + 3, nxt);
             if (r - 1 >= i0 && owner) load_update(r - 1);
@@ -427,12 +441,25 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         if (r >= i0) {
             Face5<C> Lf = Lx;
             Face5<C> Rf = Rr;
-            if (r == 0 && lo_x) boundary_face_states<Pol>(win[2], win[1], true, eps, g, Lf, Rf);
-            else if (r == L.nx && hi_x) boundary_face_states<Pol>(win[1], win[2], false, eps, g, Lf, Rf);
+            // cell values of rows r-1 and r (decoded from the ring's deviations)
+            auto full = [&](const C w[kVars], C out[kVars]) {
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) out[v] = kRing ? w[v] + C(L.off[v]) : w[v];
+            };
+            if ((r == 0 && lo_x) || (r == L.nx && hi_x)) {
+                C c1[kVars], c2[kVars];
+                full(win[1], c1);
+                full(win[2], c2);
+                if (r == 0) boundary_face_states<Pol>(c2, c1, true, eps, g, Lf, Rf);
+                else boundary_face_states<Pol>(c1, c2, false, eps, g, Lf, Rf);
+            }
             if (a.positivity) {
                 const bool low = a.lowo && j >= 0 && j < L.ny && r <= L.nx &&
                                  (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j] & 1);
-                positivity_fix<Pol>(low, win[1], win[2], g, Lf, Rf);
+                C c1[kVars], c2[kVars];
+                full(win[1], c1);
+                full(win[2], c2);
+                positivity_fix<Pol>(low, c1, c2, g, Lf, Rf);
             }
             hll_flux<Pol>(Lf, Rf, 0, a.hll, g, FX);
             // ---- update of row r-1 (its upper x-face is r - 1/2)
@@ -534,7 +561,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                 for (int k = 0; k < 5; ++k)
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) st[k][v] = decc<T, C>(row[(lane + k) * kVars + v], L, v);
+                    for (int v = 0; v < kVars; ++v) st[k][v] = C(row[(lane + k) * kVars + v]);  // deviations
             } else {
                 C(*rb)[kVars] = rbuf[wid];
                 put_slot<C>(rb[lane + 2], win[2]);
@@ -545,7 +572,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 for (int k = 0; k < 5; ++k) get_slot<C>(rb[lane + k], st[k]);
             }
             Face5<C> Ly, Ry;
-            cell_states<Pol>(st, eps, g, Ly, Ry);
+            cell_states<Pol>(st, eps, g, Ly, Ry, kRing ? L.off : nullptr);
+            if constexpr (kRing) {  // full values of the stencil's middle cells, for the rare paths below
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) {
+                    st[2][v] += C(L.off[v]);
+                    st[3][v] += C(L.off[v]);
+                }
+            }
             // right state of the cell above (lane + 1)
             Face5<C> Rn;
             Rn.r = __shfl_down_sync(0xffffffffu, Ry.r, 1);
