@@ -266,7 +266,12 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 //     stencils, the stored value and U^0 of the update are read from the ring,
 //     so no row window is held in registers and load latency overlaps rows of
 //     arithmetic.
-template <class Pol, int kWarps, int kLoad = 0>
+//
+// kLean: the caller has checked that this item needs none of the rare paths
+// (no physical-boundary face in its rows or columns, no positivity fallback, no
+// cell types, no RHS copy, no viscous RHS); they are compiled out, which keeps
+// the row loop small in the instruction cache.
+template <class Pol, int kWarps, int kLoad = 0, bool kLean = false>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][36][kVars],
                                            typename Pol::T* ring = nullptr) {
@@ -310,10 +315,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     const float cdt = float(cdtd);
     const bool sr = Pol::kMixed && a.rounding == 0;
     const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
-    const bool lo_x = a.bc[0] == kNeumann || a.bc[0] == kDirichlet;
-    const bool hi_x = a.bc[1] == kNeumann || a.bc[1] == kDirichlet;
-    const bool lo_y = a.bc[2] == kNeumann || a.bc[2] == kDirichlet;
-    const bool hi_y = a.bc[3] == kNeumann || a.bc[3] == kDirichlet;
+    const bool lo_x = !kLean && (a.bc[0] == kNeumann || a.bc[0] == kDirichlet);
+    const bool hi_x = !kLean && (a.bc[1] == kNeumann || a.bc[1] == kDirichlet);
+    const bool lo_y = !kLean && (a.bc[2] == kNeumann || a.bc[2] == kDirichlet);
+    const bool hi_y = !kLean && (a.bc[3] == kNeumann || a.bc[3] == kDirichlet);
+    const uint8_t* const types = kLean ? nullptr : a.types;
+    const int positivity = kLean ? 0 : a.positivity;
+    double* const rhs_out = kLean ? nullptr : a.rhs;
+    const T* const rv_in = kLean ? nullptr : static_cast<const T*>(a.rv);
     if (a.P && a.first_stage && bx == 0 && by == 0 && threadIdx.x == 0) {
         a.P->wmax[1 - a.parity] = 0ull;
         a.P->t += dt;
@@ -352,7 +361,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     T pf_cur[kVars], pf_u0[kVars];
     auto load_update = [&](int i) {
         const long long off = L.offset(i, j);
-        pf_fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+        pf_fluid = types ? (types[static_cast<long long>(i) * L.ny + j] == 0) : true;
 #pragma unroll
         for (int v = 0; v < kVars; ++v) {
             pf_cur[v] = Pol::kMixed ? in[v * L.plane + off] : T(0);
@@ -453,7 +462,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 if (r == 0) boundary_face_states<Pol>(c2, c1, true, eps, g, Lf, Rf);
                 else boundary_face_states<Pol>(c1, c2, false, eps, g, Lf, Rf);
             }
-            if (a.positivity) {
+            if (positivity) {
                 const bool low = a.lowo && j >= 0 && j < L.ny && r <= L.nx &&
                                  (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j] & 1);
                 C c1[kVars], c2[kVars];
@@ -466,7 +475,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             const int i = r - 1;
             if (i >= i0 && owner) {
                 if constexpr (kRing) {
-                    pf_fluid = a.types ? (a.types[static_cast<long long>(i) * L.ny + j] == 0) : true;
+                    pf_fluid = types ? (types[static_cast<long long>(i) * L.ny + j] == 0) : true;
                     const T* cs = ring_row(i) + (lane + 2) * kVars;
                     const T* us = ring_u0(i) + lane * kVars;
 #pragma unroll
@@ -493,8 +502,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
-                        if (a.rv && v >= 1)
-                            rvf += static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
+                        if (rv_in && v >= 1)
+                            rvf += rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
                         const float cur = pf_cur[v];
                         float nd = cur;
                         if (fluid) {
@@ -509,14 +518,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         }
                         sv[v] = nd;
                         nv[v] = nd + L.off[v];
-                        if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
+                        if (rhs_out) rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
                     }
                 } else {
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         double rv = -double(FX[v] - FXp[v]) * inv_dx + double(RY[v]);
-                        if (a.rv && v >= 1)
-                            rv += double(static_cast<const T*>(a.rv)[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
+                        if (rv_in && v >= 1)
+                            rv += double(rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
                         const double cur = double(win[1][v]);
                         double val = cur;
                         if (fluid) {
@@ -526,10 +535,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         }
                         sv[v] = enc<T>(val, L, v);
                         nv[v] = C(dec<T>(sv[v], L, v));
-                        if (a.rhs) a.rhs[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
+                        if (rhs_out) rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
                     }
                 }
-                if (a.positivity >= kPosFloor && fluid) {
+                if (positivity >= kPosFloor && fluid) {
                     const C pr = (C(g) - C(1)) * (nv[3] - C(0.5) * (nv[1] * nv[1] + nv[2] * nv[2]) / nv[0]);
                     if (!(nv[0] > C(kRhoFloor)) || !(pr > C(kPFloor))) {
                         double s[kVars];
@@ -601,7 +610,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 for (int v = 0; v < kVars; ++v) { cc[v] = st[2][v]; gg[v] = st[3][v]; }
                 boundary_face_states<Pol>(cc, gg, false, eps, g, Ly, Rn);
             }
-            if (a.positivity) {
+            if (positivity) {
                 const bool low = a.lowo && j >= -1 && j < L.ny &&
                                  (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j + 1] & 2);
                 positivity_fix<Pol>(low, st[2], st[3], g, Ly, Rn);
@@ -648,14 +657,28 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     }
 }
 
+// True when the work item (block column bx, rows [by*rows, by*rows + rows))
+// needs none of the rare paths of the row march (see march_item's kLean).
+template <int kWarps>
+__device__ __forceinline__ bool lean_item(const StageArgs& a, int bx, int by, int rows) {
+    if (a.positivity || a.rhs || a.rv || a.types) return false;
+    auto phys = [&](int s) { return a.bc[s] == kNeumann || a.bc[s] == kDirichlet; };
+    const int i0 = by * rows, i1 = min(i0 + rows, a.L.nx);
+    const int f0 = bx * kWarps * kSeg, f1 = (bx * kWarps + kWarps - 1) * kSeg + 31;  // y faces of the item
+    return !(phys(0) && i0 == 0) && !(phys(1) && i1 == a.L.nx) && !(phys(2) && f0 == 0) && !(phys(3) && f1 >= a.L.ny);
+}
+
 template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
+    const bool lean = lean_item<kWarps>(a, blockIdx.x, blockIdx.y, kRows);  // uniform per block
     if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
-        march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
+        if (lean) march_item<Pol, kWarps, kLoad, true>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
+        else march_item<Pol, kWarps, kLoad, false>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
     } else {
-        march_item<Pol, kWarps, kLoad>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+        if (lean) march_item<Pol, kWarps, kLoad, true>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+        else march_item<Pol, kWarps, kLoad, false>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
     }
 }
 
@@ -682,7 +705,11 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
         const int c = item_case[w], li = item_local[w];
         const int ix = case_items_x[c];
         const StageArgs a = args[c];
-        march_item<Pol, kWarps, kLoad>(a, li % ix, li / ix, case_rows[c], rbuf, kRing ? ring : nullptr);
+        const int bx = li % ix, by = li / ix, rows = case_rows[c];
+        if (lean_item<kWarps>(a, bx, by, rows))
+            march_item<Pol, kWarps, kLoad, true>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
+        else
+            march_item<Pol, kWarps, kLoad, false>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
     }
 }
 
