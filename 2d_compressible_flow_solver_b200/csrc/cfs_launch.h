@@ -43,7 +43,7 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).
-constexpr int kDefaultVariantF32 = 20;
+constexpr int kDefaultVariantF32 = 17;
 constexpr int kDefaultVariantF64 = 18;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
