@@ -53,7 +53,7 @@ WORDS_PER_CELL_STEP = 32
 # dram__bytes_write.sum, averaged over the 3 stage launches of a step) from the
 # ncu capture of the tuned FP32 march kernel at 4096^2 summarised in
 # profiles/march_kernel_f32_smooth4096_traffic.md.
-MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 42.1, "f64": None}
+MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
 
 
 def env_rank():
