@@ -113,6 +113,35 @@ __device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, f
     right = fma2(fma2(q01, r0, fma2(a1, r1, mul2(a2R, r2))), iR, v2);
 }
 
+// finish_state of a cell's two states at once (FP32-mixed: packed
+// instructions; a state whose kinetic energy exceeds 90 % of E takes the scalar
+// path with its FP64 pressure).
+template <class Pol>
+__device__ __forceinline__ void finish_pair(Face5<typename Pol::C>& L, Face5<typename Pol::C>& R, double g) {
+    if constexpr (Pol::kMixed) {
+        const float2 mx = make_float2(L.mx, R.mx), my = make_float2(L.my, R.my), E = make_float2(L.E, R.E);
+        const float2 ri = make_float2(rcp_fast(L.r), rcp_fast(R.r));
+        const float2 ke = mul2(mul2(p2(0.5f), fma2(mx, mx, mul2(my, my))), ri);
+        if (ke.x > 0.9f * L.E || ke.y > 0.9f * R.E) {
+            finish_state<Pol>(L, g);
+            finish_state<Pol>(R, g);
+            return;
+        }
+        const float2 p = mul2(p2(float(g - 1)), sub2(E, ke));
+        const float2 a2 = mul2(mul2(p2(float(g)), p), ri);
+        const float2 a = mul2(a2, make_float2(rsqrtf(a2.x), rsqrtf(a2.y)));
+        L.ri = ri.x;
+        R.ri = ri.y;
+        L.p = p.x;
+        R.p = p.y;
+        L.a = a.x;
+        R.a = a.y;
+    } else {
+        finish_state<Pol>(L, g);
+        finish_state<Pol>(R, g);
+    }
+}
+
 // Both states of one cell from a 5-cell stencil st[k][v] (k = 0..4).  The
 // FP32-mixed form pairs (rho, rho u) and (rho v, E) in packed instructions.
 // With `off` the stencil holds stored deviations (value - off[v]): WENO5 is
@@ -152,8 +181,7 @@ __device__ __forceinline__ void cell_states(const typename Pol::C st[5][kVars], 
         weno5_pair(st[0][2], st[1][2], st[2][2], st[3][2], st[4][2], eps, L.my, R.my);
         weno5_pair(st[0][3], st[1][3], st[2][3], st[3][3], st[4][3], eps, L.E, R.E);
     }
-    finish_state<Pol>(L, g);
-    finish_state<Pol>(R, g);
+    finish_pair<Pol>(L, R, g);
 }
 
 // Reference boundary face between an interior cell value c and a ghost value g
@@ -313,7 +341,13 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         x1_u1 = a.rk == kRkTvd3Ref;
     }
     const float cdt = float(cdtd);
-    const bool sr = Pol::kMixed && a.rounding == 0;
+    // Stochastic rounding of the state that ends each step (the last stage);
+    // the intermediate stage states are rounded to nearest: they are
+    // temporaries, and rounding them stochastically too gives no measurable
+    // gain in accuracy (smooth advection, 128^2 to t = 0.5: density L1 error
+    // against FP64 6.4e-8 either way, 2.8e-7 with round-to-nearest throughout).
+    const bool last_of_step = a.rk == kRkTvd2 ? a.stage == 1 : a.stage == 2;
+    const bool sr = Pol::kMixed && a.rounding == 0 && last_of_step;
     const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
     const bool lo_x = !kLean && (a.bc[0] == kNeumann || a.bc[0] == kDirichlet);
     const bool hi_x = !kLean && (a.bc[1] == kNeumann || a.bc[1] == kDirichlet);

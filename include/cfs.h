@@ -96,9 +96,10 @@ enum cfs_positivity {
 /* Rounding of the FP32 state storage of CFS_FP32_MIXED (no reference
  * counterpart; the FP64 forms round to nearest). */
 enum cfs_rounding {
-    CFS_ROUND_STOCHASTIC = 0,  /* the new state is formed exactly in FP64 and rounded to one of its two
-                                  neighbouring floats with probability by nearness (random bits hashed
-                                  from cell and step): an unbiased error that does not build up */
+    CFS_ROUND_STOCHASTIC = 0,  /* the state that ends each RK step is formed exactly in FP64 and rounded
+                                  to one of its two neighbouring floats with probability by nearness
+                                  (random bits hashed from cell and step): an unbiased error that does
+                                  not build up; intermediate stage states round to nearest */
     CFS_ROUND_NEAREST = 1      /* FP32 FMA update, round to nearest */
 };
 
