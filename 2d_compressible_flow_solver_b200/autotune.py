@@ -81,17 +81,24 @@ def tune(sizes, precisions, out: Path):
 
 def best_variant(precision: str, cells: int, table_path: Path = TABLE) -> int:
     """Best measured variant for a grid of about `cells` cells (nearest tuned
-    size by cell count); 0 (the library default) when no table exists."""
+    size by cell count), as an index of the library's current variant table
+    (the table records each variant's shape, so a table tuned against another
+    build still maps); 0 (the library default) when no table exists or its best
+    shape is not in the library."""
     try:
         doc = json.loads(table_path.read_text())
         rows = doc["table"][precision]
+        shapes = doc["variants"]
     except (OSError, KeyError, ValueError):
         return 0
     sizes = sorted(int(k) for k in rows)
     if not sizes:
         return 0
     near = min(sizes, key=lambda n: abs(n * n - cells))
-    return int(rows[str(near)]["best"])
+    shape = tuple(shapes.get(str(rows[str(near)]["best"]), ()))
+    cfsb, _ = _pkg()
+    current = [tuple(v) for v in cfsb.variants()]
+    return current.index(shape) + 1 if shape in current else 0
 
 
 def main():

@@ -34,6 +34,8 @@ struct cfs_ctx {
     void* rv = nullptr;   // viscous RHS [3][nx][ny] (Navier-Stokes form only)
     uint8_t* types_d = nullptr;
     uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
+    uint8_t* cflags_d = nullptr;  // [nx+2][ny+2] per-cell flags of the row march (with cell types)
+    void* bflux = nullptr;        // boundary-face fluxes of the row march (physical sides)
     unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
     bool fixed_offsets = false;   // FP32 storage offsets set by cfs_set_storage_offsets
     float fixed_off[4] = {0, 0, 0, 0};
@@ -151,6 +153,8 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.rounding = c->cfg.rounding;
     a.seed = c->steps_done;
     a.lowo = c->cfg.positivity >= CFS_POSITIVITY_BODY && c->has_types ? c->lowo_d : nullptr;
+    a.cflags = c->has_types ? c->cflags_d : nullptr;
+    a.bflux = c->bflux;
     return a;
 }
 
@@ -393,6 +397,12 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
         if (cudaMalloc(&c->rv, vb) != cudaSuccess) { c->err = "device allocation of the viscous RHS failed"; return bail(CFS_ERR_NOMEM); }
         cudaMemsetAsync(c->rv, 0, vb, c->stream);
     }
+    bool physical = false;
+    for (int s = 0; s < 4; ++s) physical = physical || cfg->bc[s] == CFS_BC_NEUMANN || cfg->bc[s] == CFS_BC_DIRICHLET;
+    if (physical && c->prec != cfs::kF64Exact) {
+        const size_t bb = static_cast<size_t>(cfs::bflux_count(c->L)) * c->L.elem_bytes;
+        if (cudaMalloc(&c->bflux, bb) != cudaSuccess) { c->err = "device allocation of the boundary fluxes failed"; return bail(CFS_ERR_NOMEM); }
+    }
     if (cfg->keep_rhs) {
         if (cudaMalloc(&c->rhs, hb) != cudaSuccess) { c->err = "device allocation of the RHS buffer failed"; return bail(CFS_ERR_NOMEM); }
         cudaMemsetAsync(c->rhs, 0, hb, c->stream);
@@ -419,6 +429,8 @@ int cfs_destroy(cfs_ctx* c) {
     cudaFree(c->rv);
     cudaFree(c->types_d);
     cudaFree(c->lowo_d);
+    cudaFree(c->cflags_d);
+    cudaFree(c->bflux);
     cudaFree(c->ib_cell);
     cudaFree(c->ib_donor);
     cudaFree(c->ib_perm);
@@ -499,11 +511,15 @@ int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
     CFS_CUDA(c, cudaMemcpy(c->types_d, types, n, cudaMemcpyHostToDevice));
     c->types_h.assign(types, types + n);
     c->has_types = true;
+    std::vector<uint8_t> f;
     if (c->cfg.positivity >= CFS_POSITIVITY_BODY) {
-        const std::vector<uint8_t> f = cfs::low_order_faces(types, c->cfg.nx, c->cfg.ny, c->cfg.bc);
+        f = cfs::low_order_faces(types, c->cfg.nx, c->cfg.ny, c->cfg.bc);
         if (!c->lowo_d) CFS_CUDA(c, cudaMalloc(&c->lowo_d, f.size()));
         CFS_CUDA(c, cudaMemcpy(c->lowo_d, f.data(), f.size(), cudaMemcpyHostToDevice));
     }
+    const std::vector<uint8_t> cf = cfs::cell_flags(types, f.empty() ? nullptr : f.data(), c->cfg.nx, c->cfg.ny);
+    if (!c->cflags_d) CFS_CUDA(c, cudaMalloc(&c->cflags_d, cf.size()));
+    CFS_CUDA(c, cudaMemcpy(c->cflags_d, cf.data(), cf.size(), cudaMemcpyHostToDevice));
     return CFS_OK;
 }
 

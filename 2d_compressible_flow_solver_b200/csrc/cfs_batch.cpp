@@ -31,6 +31,9 @@ struct BatchCase {
     std::vector<uint8_t> types;
     std::vector<uint8_t> lowo;   // CFS_POSITIVITY_BODY face flags, [nx+1][ny+1]
     long long lowo_off = -1;
+    std::vector<uint8_t> cflags;  // row-march cell flags, [nx+2][ny+2] (cases with cell types)
+    long long cflags_off = -1;
+    long long bflux_off = -1;     // bytes from the arena start to the boundary-face fluxes
     int ib_n = 0, ib_mode = 0;
     int ib_first = 0;       // first immersed-ghost index in the flattened lists
 };
@@ -47,6 +50,10 @@ struct cfs_batch {
     char* arena = nullptr;
     uint8_t* types_d = nullptr;
     uint8_t* lowo_d = nullptr;
+    uint8_t* cflags_d = nullptr;
+    bool any_bflux = false;  // some case has a physical side
+    int feat = 0;            // row-march features of the batch (kFeatPos, kFeatEdge)
+    int max_edge = 0;        // largest nx or ny of the cases
     int total_ig = 0;
     int* ib_cell = nullptr;
     int* ib_donor = nullptr;
@@ -120,6 +127,8 @@ int upload_args(cfs_batch* b) {
                 a.positivity = b->common.positivity;
                 a.rounding = b->common.rounding;
                 a.lowo = c.lowo_off >= 0 ? b->lowo_d + c.lowo_off : nullptr;
+                a.cflags = c.cflags_off >= 0 ? b->cflags_d + c.cflags_off : nullptr;
+                a.bflux = c.bflux_off >= 0 ? b->arena + c.bflux_off : nullptr;
                 a.stage = s;
                 // buffer roles of a step that starts in S0 (as cfs_advance)
                 int in = 0, out = 1, u0 = 0, u1 = -1;
@@ -175,9 +184,12 @@ int enqueue_batch_step(cfs_batch* b, int parity) {
         if (b->total_ig > 0)
             CFSB_CUDA(b, cfs::launch_batch_ib_fill(b->elem, b->dib + static_cast<size_t>(in) * b->n, b->ig_case,
                                                    b->ig_local, b->total_ig, b->stream));
+        if (b->any_bflux)
+            CFSB_CUDA(b, cfs::launch_batch_boundary_flux(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->n,
+                                                         b->max_edge, b->stream));
         CFSB_CUDA(b, cfs::launch_batch_stage(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->item_case,
                                              b->item_local, b->case_rows, b->case_items_x, b->total_items,
-                                             b->counters + slot, b->grid, b->stream));
+                                             b->counters + slot, b->grid, b->feat, b->stream));
     }
     return CFS_OK;
 }
@@ -195,6 +207,7 @@ int cfs_batch_destroy(cfs_batch* b) {
     cudaFree(b->arena);
     cudaFree(b->types_d);
     cudaFree(b->lowo_d);
+    cudaFree(b->cflags_d);
     cudaFree(b->ib_cell);
     cudaFree(b->ib_donor);
     cudaFree(b->ib_perm);
@@ -248,7 +261,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         return bail(CFS_ERR_CUDA, "stream creation failed");
 
     // --- per-case layout, boundaries, immersed boundary (host)
-    size_t arena = 0, types_bytes = 0, lowo_bytes = 0, max_cells = 0;
+    size_t arena = 0, types_bytes = 0, lowo_bytes = 0, cflags_bytes = 0, max_cells = 0;
     std::vector<int32_t> h_cell, h_donor, h_perm, h_igc, h_igl;
     std::vector<double> h_img, h_fac;
     for (int ci = 0; ci < ncases; ++ci) {
@@ -283,6 +296,15 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         c.state_off = arena;
         arena += static_cast<size_t>(3) * static_cast<size_t>(c.L.bytes());
         arena = (arena + 255) & ~static_cast<size_t>(255);
+        bool physical = false;
+        for (int s = 0; s < 4; ++s) physical = physical || d.bc[s] == CFS_BC_NEUMANN || d.bc[s] == CFS_BC_DIRICHLET;
+        if (physical) {
+            c.bflux_off = static_cast<long long>(arena);
+            arena += static_cast<size_t>(cfs::bflux_count(c.L)) * b->elem;
+            arena = (arena + 255) & ~static_cast<size_t>(255);
+            b->any_bflux = true;
+        }
+        b->max_edge = std::max(b->max_edge, std::max(d.nx, d.ny));
         max_cells = std::max(max_cells, static_cast<size_t>(d.nx) * d.ny);
         b->total_cells += static_cast<long long>(d.nx) * d.ny;
         if (d.circle) {
@@ -298,6 +320,9 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
                 c.lowo_off = static_cast<long long>(lowo_bytes);
                 lowo_bytes += c.lowo.size();
             }
+            c.cflags = cfs::cell_flags(c.types.data(), c.lowo.empty() ? nullptr : c.lowo.data(), d.nx, d.ny);
+            c.cflags_off = static_cast<long long>(cflags_bytes);
+            cflags_bytes += c.cflags.size();
             c.ib_n = static_cast<int>(ib.cell.size());
             c.ib_mode = d.ib_mode;
             c.ib_first = static_cast<int>(h_cell.size());
@@ -345,6 +370,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     if (!dalloc(reinterpret_cast<void**>(&b->arena), arena)) return bail(CFS_ERR_NOMEM, "state arena allocation failed");
     if (!dalloc(reinterpret_cast<void**>(&b->types_d), types_bytes) ||
         !dalloc(reinterpret_cast<void**>(&b->lowo_d), lowo_bytes) ||
+        !dalloc(reinterpret_cast<void**>(&b->cflags_d), cflags_bytes) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_cell), sizeof(int) * h_cell.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_donor), sizeof(int) * h_donor.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->ib_perm), sizeof(int) * h_perm.size()) ||
@@ -370,6 +396,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         if (c.types_off >= 0) ok = ok && h2d(b->types_d + c.types_off, c.types.data(), c.types.size());
     for (const BatchCase& c : b->cases)
         if (c.lowo_off >= 0) ok = ok && h2d(b->lowo_d + c.lowo_off, c.lowo.data(), c.lowo.size());
+    for (const BatchCase& c : b->cases)
+        if (c.cflags_off >= 0) ok = ok && h2d(b->cflags_d + c.cflags_off, c.cflags.data(), c.cflags.size());
     ok = ok && h2d(b->ib_cell, h_cell.data(), sizeof(int) * h_cell.size()) &&
          h2d(b->ib_donor, h_donor.data(), sizeof(int) * h_donor.size()) &&
          h2d(b->ib_perm, h_perm.data(), sizeof(int) * h_perm.size()) &&
@@ -387,6 +415,9 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
             if (cfs::launch_ghost_fill(b->elem, state_buf(b, b->cases[ci], k), b->cases[ci].L, b->cases[ci].sides,
                                        b->stream) != cudaSuccess)
                 return bail(CFS_ERR_CUDA, "ghost fill failed");
+    bool flags = false;
+    for (const BatchCase& c : b->cases) flags = flags || c.cflags_off >= 0;
+    b->feat = (common->positivity ? cfs::kFeatPos : 0) | (b->any_bflux || flags ? cfs::kFeatEdge : 0);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, common->device);
     b->grid = sms * cfs::batch_blocks_per_sm(b->prec);
@@ -450,14 +481,9 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
         p.dt_fixed = dt;
     }
     CFSB_CUDA(b, cudaMemcpyAsync(b->P, hp.data(), sizeof(cfs::DevParams) * b->n, cudaMemcpyHostToDevice, b->stream));
-    if (cfl > 0) {
-        for (int ci = 0; ci < b->n; ++ci) {
-            const BatchCase& c = b->cases[ci];
-            CFSB_CUDA(b, cfs::launch_wmax(b->elem, state_buf(b, c, 0), c.L,
-                                          c.types_off >= 0 ? b->types_d + c.types_off : nullptr, b->common.gamma, c.dx,
-                                          c.dy, reinterpret_cast<unsigned long long*>(b->P + ci), b->stream));
-        }
-    }
+    // first step's CFL maxima: the stage-0 arguments of parity 0 read S0 and
+    // point at each case's parameters
+    if (cfl > 0) CFSB_CUDA(b, cfs::launch_batch_wmax(b->elem, b->dargs, b->n, b->stream));
     if (nsteps >= 2 && !b->graph2) {
         cudaGraph_t g = nullptr;
         CFSB_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));

@@ -775,6 +775,28 @@ __global__ void __launch_bounds__(NT) wmax_kernel(const T* U, const Layout L, co
     if (threadIdx.x == 0 && m > 0.0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
 }
 
+// Batched form: blockIdx.y = case; the state is args[c].in, the maximum goes
+// to args[c].P->wmax[0].
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) batch_wmax_kernel(const StageArgs* __restrict__ args) {
+    __shared__ double red[NT / 32];
+    const StageArgs& a = args[blockIdx.y];
+    const T* U = static_cast<const T*>(a.in);
+    const Layout& L = a.L;
+    double m = 0.0;
+    const long long n = static_cast<long long>(L.nx) * L.ny;
+    for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
+        if (a.types && a.types[k] != 0) continue;
+        const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
+        const long long off = L.offset(i, j);
+        const double w = wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1), dec<T>(U[2 * L.plane + off], L, 2),
+                                  dec<T>(U[3 * L.plane + off], L, 3), a.gamma, a.dx, a.dy);
+        if (w > m) m = w;
+    }
+    m = block_max<NT>(m, red);
+    if (threadIdx.x == 0 && m > 0.0) atomicMax(&a.P->wmax[0], static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+
 // Sums of rho, m_x, m_y, E over fluid cells (FP64 accumulation).
 template <class T, int NT>
 __global__ void __launch_bounds__(NT) totals_kernel(const T* U, const Layout L, const uint8_t* types, double* out) {

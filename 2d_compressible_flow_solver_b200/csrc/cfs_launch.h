@@ -1,6 +1,7 @@
-// Host-callable launchers of the kernels in cfs_kernels.cuh.  Each policy's
-// kernels live in the translation unit whose compile flags they need:
-// kernels_exact.cu (-fmad=false) and kernels_fast.cu (FMA on).
+// Host-callable launchers of the kernels in cfs_kernels.cuh and cfs_march.cuh.
+// Each policy's kernels live in the translation unit whose compile flags they
+// need: kernels_exact.cu (-fmad=false), kernels_fast.cu and march_inst.cu (FMA
+// on; the latter once per form and feature set).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -18,6 +19,8 @@ cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_ib_fill(int elem_bytes, const IbArgs& a, cudaStream_t s);
 cudaError_t launch_wmax(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double g, double dx,
                         double dy, unsigned long long* out, cudaStream_t s);
+// CFL maxima of every case of a batch: args[c].in into args[c].P->wmax[0].
+cudaError_t launch_batch_wmax(int elem_bytes, const StageArgs* args, int ncases, cudaStream_t s);
 cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
                           cudaStream_t s);
 cudaError_t launch_pack(int elem_bytes, const double* src, void* dst, const Layout& L, cudaStream_t s);
@@ -35,16 +38,15 @@ struct MarchVariant {
     int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead,
                // 3 rows staged in shared memory by cp.async (FP32 form; FP64 runs 0)
 };
-constexpr int kNumVariants = 20;
+constexpr int kNumVariants = 10;
 constexpr MarchVariant kVariants[kNumVariants] = {
-    {64, 4, 1, 0}, {64, 4, 4, 0}, {64, 4, 5, 0}, {32, 4, 5, 0}, {128, 4, 4, 0}, {64, 8, 2, 0}, {64, 4, 4, 2},
-    {32, 4, 5, 2}, {64, 4, 3, 2}, {64, 8, 2, 2}, {64, 4, 4, 1}, {32, 4, 5, 1}, {64, 8, 2, 1}, {32, 4, 4, 1},
-    {32, 4, 6, 0}, {32, 8, 3, 0}, {32, 4, 5, 3}, {32, 4, 4, 3}, {64, 4, 4, 3}, {32, 4, 6, 3},
+    {64, 4, 1, 0}, {32, 4, 5, 0}, {64, 8, 2, 0}, {32, 4, 4, 1}, {64, 8, 2, 1},
+    {32, 4, 5, 2}, {32, 4, 5, 3}, {32, 4, 4, 3}, {64, 4, 4, 3}, {32, 4, 6, 3},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).
-constexpr int kDefaultVariantF32 = 17;
-constexpr int kDefaultVariantF64 = 18;
+constexpr int kDefaultVariantF32 = 7;
+constexpr int kDefaultVariantF64 = 8;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
 constexpr int kBatchWarps = 4;
@@ -53,7 +55,9 @@ constexpr int kBatchLoadF32 = 3;  // FP32 batches stage rows in the shared ring
 constexpr int kBatchMinBlocksF64 = 4;
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
-                               int grid, cudaStream_t s);
+                               int grid, int feat, cudaStream_t s);  // feat: kFeatPos | kFeatEdge bits
+// Boundary-face fluxes of every case (grid: max_edge = the largest nx or ny).
+cudaError_t launch_batch_boundary_flux(Prec p, const StageArgs* args, int ncases, int max_edge, cudaStream_t s);
 cudaError_t launch_batch_ib_fill(int elem_bytes, const IbArgs* args, const int* cases, const int* local, int total,
                                  cudaStream_t s);
 int batch_blocks_per_sm(Prec p);
@@ -62,6 +66,23 @@ int batch_blocks_per_sm(Prec p);
 cudaError_t launch_stage_exact(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s);
+// Row march of one form and feature set (march_inst.cu, kFeat* bits), variant v (1-based).
+cudaError_t launch_march_f64_0(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_1(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_2(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_3(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_4(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_5(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_6(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f64_7(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_0(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_1(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_2(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_3(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_4(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_5(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_6(const StageArgs& a, int v, cudaStream_t s);
+cudaError_t launch_march_f32_7(const StageArgs& a, int v, cudaStream_t s);
 cudaError_t launch_viscous_f64(const ViscArgs& a, cudaStream_t s);
 cudaError_t launch_viscous_f32(const ViscArgs& a, cudaStream_t s);
 cudaError_t launch_weno_faces_exact(int n, const double* st, double* l, double* r, double g, double eps, cudaStream_t s);

@@ -96,7 +96,40 @@ struct StageArgs {
                            // bit 1 y-face (i, j-1/2): stencil holds a non-fluid cell
     int rounding;          // FP32 storage: 0 stochastic, 1 to nearest
     unsigned int seed;     // stochastic-rounding step counter when P is null
+    const uint8_t* cflags; // throughput forms: per-cell flag bytes (kCell* bits) of cells
+                           // i = -1..nx, j = -1..ny, [nx+2][ny+2]; null = all fluid, no low-order faces
+    void* bflux;           // throughput forms: fluxes through the physical boundary faces
+                           // (bflux_side_offset), arithmetic type of the form
 };
+
+// Bits of StageArgs::cflags.  The x-faces of cell (i, j) are (i-1/2, j) (lo)
+// and (i+1/2, j) (hi), its y-faces (i, j-1/2) and (i, j+1/2); a low-order face
+// has a non-fluid cell in its reconstruction stencil (CFS_POSITIVITY_BODY).
+constexpr uint8_t kCellSolid = 1;   // non-fluid cell: keeps its state
+constexpr uint8_t kCellLowXlo = 2;
+constexpr uint8_t kCellLowXhi = 4;
+constexpr uint8_t kCellLowYlo = 8;
+constexpr uint8_t kCellLowYhi = 16;
+
+// Boundary-face flux layout (StageArgs::bflux): sides 0 (face i = 0) and 1
+// (i = nx) hold [4][ny], sides 2 (j = 0) and 3 (j = ny) hold [4][nx].
+CFS_HD long long bflux_side_offset(const Layout& L, int s) {
+    return s == 0 ? 0 : s == 1 ? 4LL * L.ny : s == 2 ? 8LL * L.ny : 8LL * L.ny + 4LL * L.nx;
+}
+CFS_HD long long bflux_count(const Layout& L) { return 8LL * (L.nx + L.ny); }
+
+// Sides whose faces take the reference's boundary stencil.
+CFS_HD bool physical_side(const StageArgs& a, int s) { return a.bc[s] == kNeumann || a.bc[s] == kDirichlet; }
+
+// Row-march instantiation features, chosen per launch:
+constexpr int kFeatPos = 1;    // positivity fallbacks and floors (StageArgs::positivity != 0)
+constexpr int kFeatExtra = 2;  // RHS copy (StageArgs::rhs) and viscous RHS (StageArgs::rv)
+constexpr int kFeatEdge = 4;   // physical sides (boundary-face fluxes) or cell flags (StageArgs::cflags)
+CFS_HD int march_features(const StageArgs& a) {
+    bool edge = a.cflags != nullptr;
+    for (int s = 0; s < 4; ++s) edge = edge || physical_side(a, s);
+    return (a.positivity ? kFeatPos : 0) | ((a.rhs || a.rv) ? kFeatExtra : 0) | (edge ? kFeatEdge : 0);
+}
 
 // Viscous (Navier-Stokes) RHS of one state: (dFv/dx + dGv/dy) for the momentum
 // and energy equations, written to rv[3][nx][ny].

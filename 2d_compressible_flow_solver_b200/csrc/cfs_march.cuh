@@ -254,28 +254,111 @@ __device__ __forceinline__ void get_slot(const C (&slot)[kVars], C v[kVars]) {
     }
 }
 
-// Positivity fallbacks (no reference counterpart).  A face state is admissible
-// when rho > 0 and p > 0 (NaN fails); otherwise, or when the face is flagged
-// low order, it becomes the value of the cell next to the face on its side.
+// Positivity fallback of one cell's two reconstructed states in one direction
+// (no reference counterpart).  A state is admissible when rho > 0 and p > 0
+// (NaN fails); a state that is not, or that lies on a face flagged low order
+// (a non-fluid cell in the face's stencil), becomes the cell's own value (first
+// order).  `c` is the cell's value; the replacement is finished only when a
+// state needs it.
 template <class Pol>
 __device__ __forceinline__ bool admissible(const Face5<typename Pol::C>& s) {
     return s.r > typename Pol::C(0) && s.p > typename Pol::C(0);
 }
 
 template <class Pol>
-__device__ __forceinline__ void first_order_state(const typename Pol::C c[kVars], double g, Face5<typename Pol::C>& s) {
-    s.r = c[0];
-    s.mx = c[1];
-    s.my = c[2];
-    s.E = c[3];
-    finish_state<Pol>(s, g);
+__device__ __forceinline__ void fix_states(bool lowL, bool lowR, const typename Pol::C c[kVars], double g,
+                                           Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+    const bool bl = lowL || !admissible<Pol>(L), br = lowR || !admissible<Pol>(R);
+    if (bl || br) {
+        Face5<typename Pol::C> s;
+        s.r = c[0];
+        s.mx = c[1];
+        s.my = c[2];
+        s.E = c[3];
+        finish_state<Pol>(s, g);
+        if (bl) L = s;
+        if (br) R = s;
+    }
 }
 
+// The same fallback on the two states of a physical boundary face, each taking
+// the value of the cell on its side (cl left of the face, cr right of it).
 template <class Pol>
-__device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C cl[kVars], const typename Pol::C cr[kVars],
-                                               double g, Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
-    if (low || !admissible<Pol>(L)) first_order_state<Pol>(cl, g, L);
-    if (low || !admissible<Pol>(R)) first_order_state<Pol>(cr, g, R);
+__device__ __forceinline__ void fix_face(bool low, const typename Pol::C cl[kVars], const typename Pol::C cr[kVars],
+                                         double g, Face5<typename Pol::C>& L, Face5<typename Pol::C>& R) {
+    Face5<typename Pol::C> dummy = R;
+    fix_states<Pol>(low, false, cl, g, L, dummy);
+    dummy = L;
+    fix_states<Pol>(false, low, cr, g, dummy, R);
+}
+
+// Fluxes through the physical boundary faces of one stage (the reference's
+// boundary stencil [g g g | c c c], CellInterface.cpp:172-178, then the
+// positivity fallback and HLL), computed by boundary_flux_kernel before the
+// row march, which reads them (StageArgs::bflux) instead of reconstructing
+// there.
+template <class Pol>
+__device__ __forceinline__ void boundary_face_flux(const StageArgs& a, int s, int k) {
+    using T = typename Pol::T;
+    using C = typename Pol::C;
+    const Layout& L = a.L;
+    const T* in = static_cast<const T*>(a.in);
+    // interior cell (ii, jj) and ghost cell (gi, gj) of face k of side s
+    int ii, jj, gi, gj;
+    if (s < 2) {
+        jj = gj = k;
+        ii = s == 0 ? 0 : L.nx - 1;
+        gi = s == 0 ? -1 : L.nx;
+    } else {
+        ii = gi = k;
+        jj = s == 2 ? 0 : L.ny - 1;
+        gj = s == 2 ? -1 : L.ny;
+    }
+    C c[kVars], gh[kVars];
+    const long long oc = L.offset(ii, jj), og = L.offset(gi, gj);
+#pragma unroll
+    for (int v = 0; v < kVars; ++v) {
+        c[v] = decc<T, C>(in[v * L.plane + oc], L, v);
+        gh[v] = decc<T, C>(in[v * L.plane + og], L, v);
+    }
+    const bool lo = s == 0 || s == 2;
+    Face5<C> Lf, Rf;
+    boundary_face_states<Pol>(c, gh, lo, C(a.eps), a.gamma, Lf, Rf);
+    if (a.positivity) {
+        // face flags [nx+1][ny+1]: bit 0 x-face (i-1/2, j), bit 1 y-face (i, j-1/2)
+        bool low = false;
+        if (a.lowo) {
+            const long long f = s == 0 ? jj : s == 1 ? static_cast<long long>(L.nx) * (L.ny + 1) + jj
+                              : s == 2 ? static_cast<long long>(ii) * (L.ny + 1) : static_cast<long long>(ii) * (L.ny + 1) + L.ny;
+            low = a.lowo[f] & (s < 2 ? 1 : 2);
+        }
+        fix_face<Pol>(low, lo ? gh : c, lo ? c : gh, a.gamma, Lf, Rf);
+    }
+    C F[kVars];
+    hll_flux<Pol>(Lf, Rf, s < 2 ? 0 : 1, a.hll, a.gamma, F);
+    C* out = static_cast<C*>(a.bflux) + bflux_side_offset(L, s);
+    const int n = s < 2 ? L.ny : L.nx;
+#pragma unroll
+    for (int v = 0; v < kVars; ++v) out[static_cast<long long>(v) * n + k] = F[v];
+}
+
+// One thread per boundary face: blockIdx.y = side, threads over the face index.
+template <class Pol>
+__global__ void __launch_bounds__(128) boundary_flux_kernel(const StageArgs a) {
+    const int s = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!physical_side(a, s) || k >= (s < 2 ? a.L.ny : a.L.nx)) return;
+    boundary_face_flux<Pol>(a, s, k);
+}
+
+// Batched form: blockIdx.z = case (args[c]), blockIdx.y = side.
+template <class Pol>
+__global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArgs* __restrict__ args) {
+    const StageArgs& a = args[blockIdx.z];
+    const int s = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!a.bflux || !physical_side(a, s) || k >= (s < 2 ? a.L.ny : a.L.nx)) return;
+    boundary_face_flux<Pol>(a, s, k);
 }
 
 // One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
@@ -295,11 +378,14 @@ __device__ __forceinline__ void positivity_fix(bool low, const typename Pol::C c
 //     so no row window is held in registers and load latency overlaps rows of
 //     arithmetic.
 //
-// kLean: the caller has checked that this item needs none of the rare paths
-// (no physical-boundary face in its rows or columns, no positivity fallback, no
-// cell types, no RHS copy, no viscous RHS); they are compiled out, which keeps
-// the row loop small in the instruction cache.
-template <class Pol, int kWarps, int kLoad = 0, bool kLean = false>
+// The row loop holds no rarely taken code of any size: physical boundary faces
+// read the fluxes of boundary_flux_kernel and cell types and low-order faces
+// come from one flag byte per cell (StageArgs::cflags), both compiled in only
+// with kFeatEdge; the positivity fallback is a select of the cell's own state
+// (kFeatPos); the RHS copy and viscous RHS come with kFeatExtra.  A loop body that outgrows the
+// instruction cache stalls every warp on instruction fetch, whatever the share
+// of the rare code actually executed.
+template <class Pol, int kWarps, int kLoad, int kFeat>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][36][kVars],
                                            typename Pol::T* ring = nullptr) {
@@ -307,6 +393,9 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     using C = typename Pol::C;
     constexpr bool kRing = kLoad == 3 && sizeof(T) == 4;
     constexpr int kL = (kLoad == 3 && !kRing) ? 0 : kLoad;  // effective schedule
+    constexpr bool kPos = (kFeat & kFeatPos) != 0;
+    constexpr bool kExtra = (kFeat & kFeatExtra) != 0;
+    constexpr bool kEdge = (kFeat & kFeatEdge) != 0;
     const Layout& L = a.L;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int seg = bx * kWarps + wid;
@@ -349,14 +438,13 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     const bool last_of_step = a.rk == kRkTvd2 ? a.stage == 1 : a.stage == 2;
     const bool sr = Pol::kMixed && a.rounding == 0 && last_of_step;
     const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
-    const bool lo_x = !kLean && (a.bc[0] == kNeumann || a.bc[0] == kDirichlet);
-    const bool hi_x = !kLean && (a.bc[1] == kNeumann || a.bc[1] == kDirichlet);
-    const bool lo_y = !kLean && (a.bc[2] == kNeumann || a.bc[2] == kDirichlet);
-    const bool hi_y = !kLean && (a.bc[3] == kNeumann || a.bc[3] == kDirichlet);
-    const uint8_t* const types = kLean ? nullptr : a.types;
-    const int positivity = kLean ? 0 : a.positivity;
-    double* const rhs_out = kLean ? nullptr : a.rhs;
-    const T* const rv_in = kLean ? nullptr : static_cast<const T*>(a.rv);
+    // physical boundary faces: fluxes precomputed (boundary_flux_kernel)
+    const bool lo_x = kEdge && physical_side(a, 0), hi_x = kEdge && physical_side(a, 1);
+    const bool lo_y = kEdge && physical_side(a, 2), hi_y = kEdge && physical_side(a, 3);
+    const C* const bfl = static_cast<const C*>(a.bflux);
+    const uint8_t* const flags = kEdge ? a.cflags : nullptr;
+    double* const rhs_out = kExtra ? a.rhs : nullptr;
+    const T* const rv_in = kExtra ? static_cast<const T*>(a.rv) : nullptr;
     if (a.P && a.first_stage && bx == 0 && by == 0 && threadIdx.x == 0) {
         a.P->wmax[1 - a.parity] = 0ull;
         a.P->t += dt;
@@ -389,13 +477,18 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             }
         }
     };
-    // RK operands of cell (i, j): fluid flag, the stored value (FP32 form), U^0.
+    // Flag byte of cell (r, j) (kCell* bits; 0 outside i = -1..nx, j = -1..ny
+    // or without flags).
+    auto load_flags = [&](int r) -> unsigned int {
+        if (flags && r >= -1 && r <= L.nx && j <= L.ny)
+            return flags[static_cast<long long>(r + 1) * (L.ny + 2) + (j + 1)];
+        return 0u;
+    };
+    // RK operands of cell (i, j): the stored value (FP32 form), U^0.
     // (U^1, read by the reference's TVD3 stage 2 only, is loaded at its use.)
-    bool pf_fluid = true;
     T pf_cur[kVars], pf_u0[kVars];
     auto load_update = [&](int i) {
         const long long off = L.offset(i, j);
-        pf_fluid = types ? (types[static_cast<long long>(i) * L.ny + j] == 0) : true;
 #pragma unroll
         for (int v = 0; v < kVars; ++v) {
             pf_cur[v] = Pol::kMixed ? in[v * L.plane + off] : T(0);
@@ -436,6 +529,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             cp_async_commit();
         }
     };
+    // full value of a stencil cell (the ring holds stored deviations)
+    auto full = [&](const C w[kVars], C out[kVars]) {
+#pragma unroll
+        for (int v = 0; v < kVars; ++v) out[v] = kRing ? w[v] + C(L.off[v]) : w[v];
+    };
 
     C win[5][kVars];
     C nxt[kVars];   // kLoad 1, 2: the row after win[4]
@@ -443,6 +541,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     Face5<C> Lx{};                             // left x-state of the previous row
     C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
     C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
+    unsigned int f_prev = 0u, f_next = 0u;     // flags of rows r-1 and r+1
     double wloc = 0.0;
     if (active_warp && kRing) {
         for (int q = i0 - 3; q <= i0 + 1 + kRingDist; ++q) issue_row(q);
@@ -454,7 +553,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             load_halo(i0, hal);
         }
     }
+    if (active_warp) f_next = load_flags(i0 - 1);
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
+        const unsigned int f_r = f_next;
+        f_next = load_flags(r + 1);
         if constexpr (kRing) {
             // every lane is done with the previous iteration's slots; the slot
             // now refilled held row r+3+kRingDist-kRingRows, last read at r-1
@@ -475,6 +577,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
         cell_states<Pol>(win, eps, g, Lr, Rr, kRing ? L.off : nullptr);
+        if constexpr (kPos) {
+            C cc[kVars];
+            full(win[2], cc);
+            fix_states<Pol>(f_r & kCellLowXhi, f_r & kCellLowXlo, cc, g, Lr, Rr);
+        }
         if constexpr (kL == 1) {
             if (r < i1) load_row(r + 3, nxt);
             if (r - 1 >= i0 && owner) load_update(r - 1);
@@ -482,34 +589,20 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
         C FX[kVars] = {C(0), C(0), C(0), C(0)};
         if (r >= i0) {
-            Face5<C> Lf = Lx;
-            Face5<C> Rf = Rr;
-            // cell values of rows r-1 and r (decoded from the ring's deviations)
-            auto full = [&](const C w[kVars], C out[kVars]) {
+            // (computed on a boundary row too and replaced there: a flux in a
+            // branch of its own would not overlap the surrounding work)
+            hll_flux<Pol>(Lx, Rr, 0, a.hll, g, FX);
+            if ((r == 0 && lo_x) || (r == L.nx && hi_x)) {  // uniform per warp
+                const C* b = bfl + bflux_side_offset(L, r == 0 ? 0 : 1);
+                if (j >= 0 && j < L.ny) {
 #pragma unroll
-                for (int v = 0; v < kVars; ++v) out[v] = kRing ? w[v] + C(L.off[v]) : w[v];
-            };
-            if ((r == 0 && lo_x) || (r == L.nx && hi_x)) {
-                C c1[kVars], c2[kVars];
-                full(win[1], c1);
-                full(win[2], c2);
-                if (r == 0) boundary_face_states<Pol>(c2, c1, true, eps, g, Lf, Rf);
-                else boundary_face_states<Pol>(c1, c2, false, eps, g, Lf, Rf);
+                    for (int v = 0; v < kVars; ++v) FX[v] = b[static_cast<long long>(v) * L.ny + j];
+                }
             }
-            if (positivity) {
-                const bool low = a.lowo && j >= 0 && j < L.ny && r <= L.nx &&
-                                 (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j] & 1);
-                C c1[kVars], c2[kVars];
-                full(win[1], c1);
-                full(win[2], c2);
-                positivity_fix<Pol>(low, c1, c2, g, Lf, Rf);
-            }
-            hll_flux<Pol>(Lf, Rf, 0, a.hll, g, FX);
             // ---- update of row r-1 (its upper x-face is r - 1/2)
             const int i = r - 1;
             if (i >= i0 && owner) {
                 if constexpr (kRing) {
-                    pf_fluid = types ? (types[static_cast<long long>(i) * L.ny + j] == 0) : true;
                     const T* cs = ring_row(i) + (lane + 2) * kVars;
                     const T* us = ring_u0(i) + lane * kVars;
 #pragma unroll
@@ -520,7 +613,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 } else if constexpr (kL == 0) {
                     load_update(i);
                 }
-                const bool fluid = pf_fluid;
+                const bool fluid = !kEdge || !(f_prev & kCellSolid);
                 const long long off = L.offset(i, j);
                 const T* u1 = static_cast<const T*>(a.u1);
                 T* out = static_cast<T*>(a.out);
@@ -532,49 +625,49 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                     // the rounding step is that of the deviation.  Stochastic
                     // rounding forms the new deviation exactly in FP64 (float
                     // products are exact there) and rounds it once.
-                    const unsigned int h = sr && fluid ? cell_hash(i, j, step_seed) : 0u;
+                    // (formed for every cell and selected: a non-fluid cell keeps its state)
+                    const unsigned int h = sr ? cell_hash(i, j, step_seed) : 0u;
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
-                        if (rv_in && v >= 1)
+                        if (kExtra && rv_in && v >= 1)
                             rvf += rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
                         const float cur = pf_cur[v];
-                        float nd = cur;
-                        if (fluid) {
-                            const float x0 = a.stage == 0 ? cur : pf_u0[v];
-                            const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
-                            if (sr) {
-                                const double tot = fma(cdtd, double(rvf), fma(double(cA), double(x0), double(cB) * double(x1)));
-                                nd = round_stochastic(tot, (h >> (8 * v)) & 255u);
-                            } else {
-                                nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
-                            }
+                        const float x0 = a.stage == 0 ? cur : pf_u0[v];
+                        const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
+                        float nd;
+                        if (sr) {
+                            const double tot = fma(cdtd, double(rvf), fma(double(cA), double(x0), double(cB) * double(x1)));
+                            nd = round_stochastic(tot, (h >> (8 * v)) & 255u);
+                        } else {
+                            nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
                         }
+                        nd = fluid ? nd : cur;
                         sv[v] = nd;
                         nv[v] = nd + L.off[v];
-                        if (rhs_out) rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
+                        if (kExtra && rhs_out)
+                            rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
                     }
                 } else {
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         double rv = -double(FX[v] - FXp[v]) * inv_dx + double(RY[v]);
-                        if (rv_in && v >= 1)
+                        if (kExtra && rv_in && v >= 1)
                             rv += double(rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
                         const double cur = double(win[1][v]);
-                        double val = cur;
-                        if (fluid) {
-                            const double u0v = a.stage >= 1 ? dec<T>(pf_u0[v], L, v) : 0.0;
-                            const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
-                            val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
-                        }
+                        const double u0v = a.stage >= 1 ? dec<T>(pf_u0[v], L, v) : 0.0;
+                        const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
+                        const double val = fluid ? rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv) : cur;
                         sv[v] = enc<T>(val, L, v);
                         nv[v] = C(dec<T>(sv[v], L, v));
-                        if (rhs_out) rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
+                        if (kExtra && rhs_out)
+                            rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? rv : 0.0;
                     }
                 }
-                if (positivity >= kPosFloor && fluid) {
-                    const C pr = (C(g) - C(1)) * (nv[3] - C(0.5) * (nv[1] * nv[1] + nv[2] * nv[2]) / nv[0]);
-                    if (!(nv[0] > C(kRhoFloor)) || !(pr > C(kPFloor))) {
+                if (kPos && a.positivity >= kPosFloor && fluid) {
+                    // p > floor, multiplied by rho > 0: (g-1)(rho E - |m|^2/2) > floor rho
+                    const C q = nv[3] * nv[0] - C(0.5) * (nv[1] * nv[1] + nv[2] * nv[2]);
+                    if (!(nv[0] > C(kRhoFloor)) || !(C(g - 1.0) * q > C(kPFloor) * nv[0])) {
                         double s[kVars];
 #pragma unroll
                         for (int v = 0; v < kVars; ++v)
@@ -588,9 +681,9 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                     }
                 }
                 store_cell4<T>(out, L, a.bc, i, j, sv);
-                if (a.P && a.last_stage && a.P->use_cfl && fluid) {
+                if (a.P && a.last_stage && a.P->use_cfl) {
                     const C w = wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy));
-                    if (double(w) > wloc) wloc = double(w);
+                    if (fluid && double(w) > wloc) wloc = double(w);
                 }
             }
         }
@@ -616,12 +709,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             }
             Face5<C> Ly, Ry;
             cell_states<Pol>(st, eps, g, Ly, Ry, kRing ? L.off : nullptr);
-            if constexpr (kRing) {  // full values of the stencil's middle cells, for the rare paths below
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) {
-                    st[2][v] += C(L.off[v]);
-                    st[3][v] += C(L.off[v]);
-                }
+            if constexpr (kPos) {
+                C cc[kVars];
+                full(st[2], cc);
+                fix_states<Pol>(f_r & kCellLowYhi, f_r & kCellLowYlo, cc, g, Ly, Ry);
             }
             // right state of the cell above (lane + 1)
             Face5<C> Rn;
@@ -633,24 +724,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             Rn.a = __shfl_down_sync(0xffffffffu, Ry.a, 1);
             Rn.ri = __shfl_down_sync(0xffffffffu, Ry.ri, 1);
             // face between column j and j+1 (face index j+1)
-            if (j + 1 == 0 && lo_y) {
-                C cc[kVars], gg[kVars];
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) { gg[v] = st[2][v]; cc[v] = st[3][v]; }
-                boundary_face_states<Pol>(cc, gg, true, eps, g, Ly, Rn);
-            } else if (j + 1 == L.ny && hi_y) {
-                C cc[kVars], gg[kVars];
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) { cc[v] = st[2][v]; gg[v] = st[3][v]; }
-                boundary_face_states<Pol>(cc, gg, false, eps, g, Ly, Rn);
-            }
-            if (positivity) {
-                const bool low = a.lowo && j >= -1 && j < L.ny &&
-                                 (a.lowo[static_cast<long long>(r) * (L.ny + 1) + j + 1] & 2);
-                positivity_fix<Pol>(low, st[2], st[3], g, Ly, Rn);
-            }
             C FY[kVars];
             hll_flux<Pol>(Ly, Rn, 1, a.hll, g, FY);
+            if ((j == -1 && lo_y) || (j == L.ny - 1 && hi_y)) {
+                const int n = L.nx;
+                const C* b = bfl + bflux_side_offset(L, j == -1 ? 2 : 3);
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) FY[v] = b[static_cast<long long>(v) * n + r];
+            }
 #pragma unroll
             for (int v = 0; v < kVars; ++v) {
                 const C below = __shfl_up_sync(0xffffffffu, FY[v], 1);
@@ -662,6 +743,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
         for (int v = 0; v < kVars; ++v) FXp[v] = FX[v];
         Lx = Lr;
+        f_prev = f_r;
         if (!kRing && r < i1) {
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -691,28 +773,14 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     }
 }
 
-// True when the work item (block column bx, rows [by*rows, by*rows + rows))
-// needs none of the rare paths of the row march (see march_item's kLean).
-template <int kWarps>
-__device__ __forceinline__ bool lean_item(const StageArgs& a, int bx, int by, int rows) {
-    if (a.positivity || a.rhs || a.rv || a.types) return false;
-    auto phys = [&](int s) { return a.bc[s] == kNeumann || a.bc[s] == kDirichlet; };
-    const int i0 = by * rows, i1 = min(i0 + rows, a.L.nx);
-    const int f0 = bx * kWarps * kSeg, f1 = (bx * kWarps + kWarps - 1) * kSeg + 31;  // y faces of the item
-    return !(phys(0) && i0 == 0) && !(phys(1) && i1 == a.L.nx) && !(phys(2) && f0 == 0) && !(phys(3) && f1 >= a.L.ny);
-}
-
-template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad>
+template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad, int kFeat>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
     __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
-    const bool lean = lean_item<kWarps>(a, blockIdx.x, blockIdx.y, kRows);  // uniform per block
     if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
-        if (lean) march_item<Pol, kWarps, kLoad, true>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
-        else march_item<Pol, kWarps, kLoad, false>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
     } else {
-        if (lean) march_item<Pol, kWarps, kLoad, true>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
-        else march_item<Pol, kWarps, kLoad, false>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
     }
 }
 
@@ -721,7 +789,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const St
 // counter, largest cases first, until none are left.  args[c] holds case c's
 // stage arguments (its own layout, boundaries, buffers, dt slot); rows[c] is
 // the row chunk the autotuner chose for its size.
-template <class Pol, int kWarps, int kMinBlocks, int kLoad = 0>
+template <class Pol, int kWarps, int kMinBlocks, int kLoad, int kFeat>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
     batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ item_case,
                        const int* __restrict__ item_local, const int* __restrict__ case_rows,
@@ -740,10 +808,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
         const int ix = case_items_x[c];
         const StageArgs a = args[c];
         const int bx = li % ix, by = li / ix, rows = case_rows[c];
-        if (lean_item<kWarps>(a, bx, by, rows))
-            march_item<Pol, kWarps, kLoad, true>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
-        else
-            march_item<Pol, kWarps, kLoad, false>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
     }
 }
 

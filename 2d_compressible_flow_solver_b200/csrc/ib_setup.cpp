@@ -3,6 +3,8 @@
 // doubles exactly (Circle.cpp uses only + - * / sqrt, cos and sin).
 #include "ib_setup.h"
 
+#include "cfs_layout.h"
+
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -275,6 +277,26 @@ std::vector<uint8_t> low_order_faces(const uint8_t* types, int nx, int ny, const
                     break;
                 }
             }
+    return f;
+}
+
+std::vector<uint8_t> cell_flags(const uint8_t* types, const uint8_t* lowo, int nx, int ny) {
+    const int w = ny + 2;
+    std::vector<uint8_t> f(static_cast<size_t>(nx + 2) * w, 0);
+    auto face = [&](int i, int j) { return lowo[static_cast<size_t>(i) * (ny + 1) + j]; };
+    for (int i = -1; i <= nx; ++i)
+        for (int j = -1; j <= ny; ++j) {
+            const bool in_i = i >= 0 && i < nx, in_j = j >= 0 && j < ny;
+            uint8_t b = 0;
+            if (in_i && in_j && types[static_cast<size_t>(i) * ny + j]) b |= kCellSolid;
+            if (lowo) {
+                if (in_j && i >= 0 && i <= nx && (face(i, j) & 1)) b |= kCellLowXlo;
+                if (in_j && i + 1 >= 0 && i + 1 <= nx && (face(i + 1, j) & 1)) b |= kCellLowXhi;
+                if (in_i && j >= 0 && j <= ny && (face(i, j) & 2)) b |= kCellLowYlo;
+                if (in_i && j + 1 >= 0 && j + 1 <= ny && (face(i, j + 1) & 2)) b |= kCellLowYhi;
+            }
+            f[static_cast<size_t>(i + 1) * w + (j + 1)] = b;
+        }
     return f;
 }
 

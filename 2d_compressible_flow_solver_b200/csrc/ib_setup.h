@@ -52,4 +52,10 @@ void ib_factors(int mode, const uint8_t* types, int nx, int ny, double dx, doubl
 // physical-boundary face is the first interior cell).  bc: cfs_bc per side.
 std::vector<uint8_t> low_order_faces(const uint8_t* types, int nx, int ny, const int bc[4]);
 
+// Per-cell flag bytes of the row march (StageArgs::cflags, kCell* bits),
+// [nx+2][ny+2] for cells i = -1..nx, j = -1..ny: the cell's own type (solid
+// bit) and, with face flags `lowo` (low_order_faces; null = none), the flags of
+// its four faces.
+std::vector<uint8_t> cell_flags(const uint8_t* types, const uint8_t* lowo, int nx, int ny);
+
 }  // namespace cfs

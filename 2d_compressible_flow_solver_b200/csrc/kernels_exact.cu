@@ -50,6 +50,18 @@ cudaError_t launch_wmax(int elem_bytes, const void* U, const Layout& L, const ui
     return cudaGetLastError();
 }
 
+cudaError_t launch_batch_wmax(int elem_bytes, const StageArgs* args, int ncases, cudaStream_t s) {
+    constexpr int nt = 256, per_case = 64;
+    for (int c0 = 0; c0 < ncases; c0 += 65535) {  // gridDim.y limit
+        const int nc = ncases - c0 < 65535 ? ncases - c0 : 65535;
+        if (elem_bytes == 8) batch_wmax_kernel<double, nt><<<dim3(per_case, nc), nt, 0, s>>>(args + c0);
+        else batch_wmax_kernel<float, nt><<<dim3(per_case, nc), nt, 0, s>>>(args + c0);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
                           cudaStream_t s) {
     constexpr int nt = 256;

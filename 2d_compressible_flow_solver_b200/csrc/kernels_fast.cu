@@ -6,77 +6,114 @@
 
 namespace cfs {
 
-template <class Pol, int R, int W, int B, int Ld>
-cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
-    const int nseg = (a.L.ny + kSeg - 1) / kSeg;
-    const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
-    march_kernel<Pol, R, W, B, Ld><<<grid, 32 * W, 0, s>>>(a);
+// Boundary-face fluxes of the stage (physical sides only), then the row march
+// of the stage's feature set.
+template <class Pol>
+cudaError_t launch_boundary_flux(const StageArgs& a, cudaStream_t s) {
+    if (!(physical_side(a, 0) || physical_side(a, 1) || physical_side(a, 2) || physical_side(a, 3)))
+        return cudaSuccess;
+    if (!a.bflux) return cudaErrorInvalidValue;
+    const int n = a.L.nx > a.L.ny ? a.L.nx : a.L.ny;
+    boundary_flux_kernel<Pol><<<dim3((n + 127) / 128, 4), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <class Pol, int K>
-cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
-    constexpr MarchVariant v = kVariants[K];
-    return launch_march<Pol, v.rows, v.warps, v.min_blocks, v.load>(a, s);
-}
-
-template <class Pol>
-cudaError_t launch_march_variant(const StageArgs& a, int v, cudaStream_t s) {
-    static_assert(kNumVariants == 20, "variant table and dispatch disagree");
-    switch (v) {
-        case 1: return launch_march_k<Pol, 0>(a, s);
-        case 2: return launch_march_k<Pol, 1>(a, s);
-        case 3: return launch_march_k<Pol, 2>(a, s);
-        case 4: return launch_march_k<Pol, 3>(a, s);
-        case 5: return launch_march_k<Pol, 4>(a, s);
-        case 6: return launch_march_k<Pol, 5>(a, s);
-        case 7: return launch_march_k<Pol, 6>(a, s);
-        case 8: return launch_march_k<Pol, 7>(a, s);
-        case 9: return launch_march_k<Pol, 8>(a, s);
-        case 10: return launch_march_k<Pol, 9>(a, s);
-        case 11: return launch_march_k<Pol, 10>(a, s);
-        case 12: return launch_march_k<Pol, 11>(a, s);
-        case 13: return launch_march_k<Pol, 12>(a, s);
-        case 14: return launch_march_k<Pol, 13>(a, s);
-        case 15: return launch_march_k<Pol, 14>(a, s);
-        case 16: return launch_march_k<Pol, 15>(a, s);
-        case 17: return launch_march_k<Pol, 16>(a, s);
-        case 18: return launch_march_k<Pol, 17>(a, s);
-        case 19: return launch_march_k<Pol, 18>(a, s);
-        case 20: return launch_march_k<Pol, 19>(a, s);
-        default: return cudaErrorInvalidValue;
+cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
+    const cudaError_t e = launch_boundary_flux<PolF64>(a, s);
+    if (e != cudaSuccess) return e;
+    const int v = a.variant > 0 ? a.variant : kDefaultVariantF64;
+    switch (march_features(a)) {
+        case 0: return launch_march_f64_0(a, v, s);
+        case 1: return launch_march_f64_1(a, v, s);
+        case 2: return launch_march_f64_2(a, v, s);
+        case 3: return launch_march_f64_3(a, v, s);
+        case 4: return launch_march_f64_4(a, v, s);
+        case 5: return launch_march_f64_5(a, v, s);
+        case 6: return launch_march_f64_6(a, v, s);
+        default: return launch_march_f64_7(a, v, s);
     }
 }
 
-cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
-    return launch_march_variant<PolF64>(a, a.variant > 0 ? a.variant : kDefaultVariantF64, s);
+cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
+    const cudaError_t e = launch_boundary_flux<PolF32>(a, s);
+    if (e != cudaSuccess) return e;
+    const int v = a.variant > 0 ? a.variant : kDefaultVariantF32;
+    switch (march_features(a)) {
+        case 0: return launch_march_f32_0(a, v, s);
+        case 1: return launch_march_f32_1(a, v, s);
+        case 2: return launch_march_f32_2(a, v, s);
+        case 3: return launch_march_f32_3(a, v, s);
+        case 4: return launch_march_f32_4(a, v, s);
+        case 5: return launch_march_f32_5(a, v, s);
+        case 6: return launch_march_f32_6(a, v, s);
+        default: return launch_march_f32_7(a, v, s);
+    }
 }
 
-cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
-    return launch_march_variant<PolF32>(a, a.variant > 0 ? a.variant : kDefaultVariantF32, s);
+// The batch's feature set is common to its cases: positivity, and the edge
+// code when some case has a physical side or cell types (batches keep no RHS
+// and have no viscous terms).
+template <class Pol, int kMinBlocks, int kLoad>
+cudaError_t launch_batch_march(const StageArgs* args, const int* item_case, const int* item_local,
+                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               int grid, int feat, cudaStream_t s) {
+    switch (feat) {
+        case 0:
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, 0><<<grid, 32 * kBatchWarps, 0, s>>>(
+                args, item_case, item_local, case_rows, case_items_x, total, counter);
+            break;
+        case kFeatPos:
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
+                args, item_case, item_local, case_rows, case_items_x, total, counter);
+            break;
+        case kFeatEdge:
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge><<<grid, 32 * kBatchWarps, 0, s>>>(
+                args, item_case, item_local, case_rows, case_items_x, total, counter);
+            break;
+        case kFeatEdge | kFeatPos:
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge | kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
+                args, item_case, item_local, case_rows, case_items_x, total, counter);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
-                               int grid, cudaStream_t s) {
+                               int grid, int feat, cudaStream_t s) {
     if (total <= 0) return cudaSuccess;
     if (p == kF32Mixed)
-        batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32><<<grid, 32 * kBatchWarps, 0, s>>>(
-            args, item_case, item_local, case_rows, case_items_x, total, counter);
-    else
-        batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64><<<grid, 32 * kBatchWarps, 0, s>>>(
-            args, item_case, item_local, case_rows, case_items_x, total, counter);
-    return cudaGetLastError();
+        return launch_batch_march<PolF32, kBatchMinBlocksF32, kBatchLoadF32>(args, item_case, item_local, case_rows,
+                                                                             case_items_x, total, counter, grid, feat, s);
+    return launch_batch_march<PolF64, kBatchMinBlocksF64, 0>(args, item_case, item_local, case_rows, case_items_x,
+                                                             total, counter, grid, feat, s);
+}
+
+// Boundary-face fluxes of every case of a batch (cases without physical sides
+// carry no bflux and return at once).
+cudaError_t launch_batch_boundary_flux(Prec p, const StageArgs* args, int ncases, int max_edge, cudaStream_t s) {
+    for (int c0 = 0; c0 < ncases; c0 += 65535) {  // gridDim.z limit
+        const int nc = ncases - c0 < 65535 ? ncases - c0 : 65535;
+        const dim3 grid((max_edge + 127) / 128, 4, nc);
+        if (p == kF32Mixed) batch_boundary_flux_kernel<PolF32><<<grid, 128, 0, s>>>(args + c0);
+        else batch_boundary_flux_kernel<PolF64><<<grid, 128, 0, s>>>(args + c0);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int batch_blocks_per_sm(Prec p) {
     int n = 0;
     if (p == kF32Mixed)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32>,
-                                                      32 * kBatchWarps, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32, kFeatEdge | kFeatPos>,
+            32 * kBatchWarps, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64>,
-                                                      32 * kBatchWarps, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64, 0, kFeatEdge | kFeatPos>, 32 * kBatchWarps, 0);
     return n > 0 ? n : 1;
 }
 

@@ -1,0 +1,51 @@
+// Row-march launchers of one (form, feature set): compiled once per pair, with
+//   -DCFS_MARCH_POL=PolF32|PolF64  -DCFS_MARCH_FEAT=0..7  -DCFS_MARCH_FN=<launcher name>
+// (the build gives each pair its own object, so the 160 kernels compile in
+// parallel).  The launcher runs the variant `v` of kVariants (1-based).
+#include "cfs_kernels.cuh"
+#include "cfs_launch.h"
+#include "cfs_march.cuh"
+
+#if !defined(CFS_MARCH_POL) || !defined(CFS_MARCH_FEAT) || !defined(CFS_MARCH_FN)
+#error "march_inst.cu needs CFS_MARCH_POL, CFS_MARCH_FEAT and CFS_MARCH_FN"
+#endif
+
+namespace cfs {
+namespace {
+
+template <class Pol, int R, int W, int B, int Ld, int F>
+cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
+    const int nseg = (a.L.ny + kSeg - 1) / kSeg;
+    const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
+    march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class Pol, int K, int F>
+cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
+    constexpr MarchVariant v = kVariants[K];
+    return launch_march<Pol, v.rows, v.warps, v.min_blocks, v.load, F>(a, s);
+}
+
+}  // namespace
+
+cudaError_t CFS_MARCH_FN(const StageArgs& a, int v, cudaStream_t s) {
+    using P = CFS_MARCH_POL;
+    constexpr int F = CFS_MARCH_FEAT;
+    static_assert(kNumVariants == 10, "variant table and dispatch disagree");
+    switch (v) {
+        case 1: return launch_march_k<P, 0, F>(a, s);
+        case 2: return launch_march_k<P, 1, F>(a, s);
+        case 3: return launch_march_k<P, 2, F>(a, s);
+        case 4: return launch_march_k<P, 3, F>(a, s);
+        case 5: return launch_march_k<P, 4, F>(a, s);
+        case 6: return launch_march_k<P, 5, F>(a, s);
+        case 7: return launch_march_k<P, 6, F>(a, s);
+        case 8: return launch_march_k<P, 7, F>(a, s);
+        case 9: return launch_march_k<P, 8, F>(a, s);
+        case 10: return launch_march_k<P, 9, F>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace cfs

@@ -2,20 +2,28 @@
 cfs_variant_info) computes the same stage: against variant 1, relative
 L-infinity <= 1e-12 in FP64 and <= 1e-5 in FP32-mixed after 6 steps (the
 variants are separate compilations, so FMA contraction may differ in the last
-bits).  Cases: four-quadrant Riemann problem with transmissive sides, and a
-cylinder with the slip-wall IB and the body positivity fallback."""
+bits).  Cases cover the row march's feature sets: a periodic four-quadrant
+problem (no edge code), the same with the face positivity fallback and the RHS
+copy, the four-quadrant problem with transmissive sides (boundary-face fluxes),
+and a cylinder with the slip-wall IB and the body positivity fallback (cell
+flags).  The feature sets themselves agree where they must: all-fluid cell
+types, and a positivity fallback that never triggers, change nothing."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def _run(cfsb, w, prec, variant, circle=None):
-    with cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=w.bc,
-                     bc_prim=w.bc_prim, variant=variant,
-                     positivity=cfsb.POSITIVITY_BODY if circle else cfsb.POSITIVITY_OFF) as s:
+def _run(cfsb, w, prec, variant, circle=None, bc=None, positivity=None, keep_rhs=False, types=None):
+    if positivity is None:
+        positivity = cfsb.POSITIVITY_BODY if circle else cfsb.POSITIVITY_OFF
+    with cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
+                     bc=w.bc if bc is None else bc, bc_prim=w.bc_prim, variant=variant, positivity=positivity,
+                     keep_rhs=keep_rhs) as s:
         if circle:
             s.build_circle(*circle, 400, cfsb.IB_BILINEAR_SLIP)
+        if types is not None:
+            s.set_cell_types(types)
         s.set_state(w.U0)
         s.advance(6, dt=5e-4)
         return s.get_state()
@@ -26,12 +34,32 @@ def test_variants_agree(cfsb, workloads, prec, tol):
     quad = workloads.riemann_quadrants(150, 130, seed=9)
     cyl = workloads.mach3_cylinder(192, 96)
     nvar = len(cfsb.variants())
-    assert nvar >= 20
-    for w, circle in ((quad, None), (cyl, cyl.circle)):
-        ref = _run(cfsb, w, prec, 1, circle)
+    assert nvar >= 10
+    per = (cfsb.BC_PERIODIC,) * 4
+    cases = [("periodic", quad, {"bc": per}),
+             ("periodic+face+rhs", quad, {"bc": per, "positivity": cfsb.POSITIVITY_FACE, "keep_rhs": True}),
+             ("transmissive", quad, {}),
+             ("cylinder", cyl, {"circle": cyl.circle})]
+    for name, w, kw in cases:
+        ref = _run(cfsb, w, prec, 1, **kw)
         assert np.all(np.isfinite(ref))
         scale = np.abs(ref).max()
         for v in range(2, nvar + 1):
-            got = _run(cfsb, w, prec, v, circle)
+            got = _run(cfsb, w, prec, v, **kw)
             err = np.abs(got - ref).max() / scale
-            assert err <= tol, (w.name, v, cfsb.variants()[v - 1], err)
+            assert err <= tol, (name, v, cfsb.variants()[v - 1], err)
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-5)])
+def test_feature_sets_agree(cfsb, workloads, prec, tol):
+    w = workloads.smooth_advection(96)
+    per = (cfsb.BC_PERIODIC,) * 4
+    ref = _run(cfsb, w, prec, 0, bc=per)
+    scale = np.abs(ref).max()
+    for kw in ({"types": np.zeros((w.nx, w.ny), np.uint8)},
+               {"positivity": cfsb.POSITIVITY_FACE},
+               {"positivity": cfsb.POSITIVITY_FLOOR, "types": np.zeros((w.nx, w.ny), np.uint8)},
+               {"keep_rhs": True}):
+        got = _run(cfsb, w, prec, 0, bc=per, **kw)
+        err = np.abs(got - ref).max() / scale
+        assert err <= tol, (kw.keys(), err)
