@@ -480,10 +480,17 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     // Flag byte of cell (r, j) (kCell* bits; 0 outside i = -1..nx, j = -1..ny
     // or without flags).
     auto load_flags = [&](int r) -> unsigned int {
-        if (flags && r >= -1 && r <= L.nx && j <= L.ny)
-            return flags[static_cast<long long>(r + 1) * (L.ny + 2) + (j + 1)];
-        return 0u;
+        unsigned int f = 0u;
+        if (flags && r >= -1 && r <= L.nx) {  // uniform per warp
+            if (j <= L.ny) f = flags[static_cast<long long>(r + 1) * (L.ny + 2) + (j + 1)];
+        }
+        return f;
     };
+    // this lane reconstructs the ghost column of a physical y side (its y-face
+    // flux is the boundary flux); warp-uniform screen for the rare lanes
+    const bool ybnd = (j == -1 && lo_y) || (j == L.ny - 1 && hi_y);
+    const bool warp_ybnd = __any_sync(0xffffffffu, ybnd);
+    const C* const bfy = ybnd ? bfl + bflux_side_offset(L, j == -1 ? 2 : 3) : nullptr;
     // RK operands of cell (i, j): the stored value (FP32 form), U^0.
     // (U^1, read by the reference's TVD3 stage 2 only, is loaded at its use.)
     T pf_cur[kVars], pf_u0[kVars];
@@ -726,11 +733,9 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             // face between column j and j+1 (face index j+1)
             C FY[kVars];
             hll_flux<Pol>(Ly, Rn, 1, a.hll, g, FY);
-            if ((j == -1 && lo_y) || (j == L.ny - 1 && hi_y)) {
-                const int n = L.nx;
-                const C* b = bfl + bflux_side_offset(L, j == -1 ? 2 : 3);
+            if (warp_ybnd && ybnd) {
 #pragma unroll
-                for (int v = 0; v < kVars; ++v) FY[v] = b[static_cast<long long>(v) * n + r];
+                for (int v = 0; v < kVars; ++v) FY[v] = bfy[static_cast<long long>(v) * L.nx + r];
             }
 #pragma unroll
             for (int v = 0; v < kVars; ++v) {
