@@ -568,6 +568,57 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------ modes arm
+MODES = {  # name: (side kind, positivity, cylinder)
+    "periodic": ("BC_PERIODIC", "POSITIVITY_OFF", False),
+    "transmissive": ("BC_NEUMANN", "POSITIVITY_OFF", False),
+    "periodic_floors": ("BC_PERIODIC", "POSITIVITY_FLOOR", False),
+    "transmissive_floors_cylinder": ("BC_NEUMANN", "POSITIVITY_FLOOR", True),
+}
+
+
+def modes_arm(args):
+    """Throughput of the row march's feature sets on one grid: a seeded
+    four-quadrant state on n^2 cells (default 2048^2), SSP-RK3, Davis HLL, CFL
+    0.5, with periodic or transmissive sides, without or with the positivity
+    fallbacks and floors, and with a slip-wall cylinder (r = 0.1 at the centre)
+    in the last mode.  Each form, each mode: W warm-up steps, K timed steps with
+    CUDA events on the engine's stream.  `--mode` runs one mode (FP32 only), for
+    a profiler.  One JSON line."""
+    import torch
+
+    cfsb = importlib.import_module(PKG)
+    wl = importlib.import_module(f"{PKG}.workloads")
+    n = args.modes_n
+    w = wl.riemann_quadrants(n, n, seed=3)
+
+    def rate(prec, mode):
+        side, pos, cyl = MODES[mode]
+        with cfsb.Solver(n, n, 1.0, 1.0, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
+                         bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos)) as s:
+            if cyl:
+                s.build_circle(0.1, 0.5, 0.5, 400, cfsb.IB_BILINEAR_SLIP)
+            s.set_state(w.U0)
+            s.advance(args.warmup, cfl=0.5)
+            stream = torch.cuda.ExternalStream(s.stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.advance(args.steps, cfl=0.5)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return round(n * n * args.steps / (e0.elapsed_time(e1) / 1e3) / 1e6, 1)
+
+    out = {"workload": f"row-march feature sets, four-quadrant state {n}^2, SSP-RK3, Davis HLL, CFL 0.5",
+           "steps": args.steps, "warmup": args.warmup, "unit": UNIT}
+    if args.mode:
+        out[args.mode] = {"fp32": rate(cfsb.FP32_MIXED, args.mode)}
+    else:
+        for mode in MODES:
+            out[mode] = {"fp32": rate(cfsb.FP32_MIXED, mode), "fp64": rate(cfsb.FP64, mode)}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,10 +628,13 @@ def main():
     ap.add_argument("--n", type=int, default=4096, help="grid edge (cells) per GPU")
     ap.add_argument("--accuracy-n", type=int, default=1024, help="grid of the FP32-vs-FP64 check (0 = skip)")
     ap.add_argument("--cpu-sample", type=int, default=384, help="grid edge of one CPU-baseline sample")
-    ap.add_argument("--workload", choices=["smooth", "batch", "report"], default="smooth",
+    ap.add_argument("--workload", choices=["smooth", "batch", "report", "modes"], default="smooth",
                     help="smooth: the headline 4096^2 line; batch: the uneven-batch comparison; report: "
-                         "FP32-vs-FP64 accuracy and drift on the other configurations (one JSON line each)")
+                         "FP32-vs-FP64 accuracy and drift on the other configurations; modes: the row march's "
+                         "feature sets on one grid (one JSON line each)")
     ap.add_argument("--cases", type=int, default=512, help="cases of the batch workload")
+    ap.add_argument("--modes-n", type=int, default=2048, help="grid edge of the modes workload")
+    ap.add_argument("--mode", choices=list(MODES), default=None, help="modes workload: run this mode only (FP32)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -588,6 +642,8 @@ def main():
         batch_arm(args)
     elif args.workload == "report":
         report_arm(args)
+    elif args.workload == "modes":
+        modes_arm(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:
