@@ -25,7 +25,7 @@ __all__ = [
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
     "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "POSITIVITY_FLOOR", "ROUND_STOCHASTIC",
-    "ROUND_NEAREST", "variants",
+    "ROUND_NEAREST", "variants", "fp_peaks",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -124,6 +124,7 @@ _SIGNATURES = {
     "cfs_compute_dt_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_void_p, _c_double_p]),
+    "cfs_fp_peaks": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "cfs_batch_create": (ctypes.c_int, [ctypes.POINTER(CfsConfig), ctypes.c_int, ctypes.c_void_p,
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "cfs_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -167,6 +168,16 @@ def variants() -> list[tuple[int, int, int, int]]:
         lib.cfs_variant_info(v, ctypes.byref(r), ctypes.byref(w), ctypes.byref(b), ctypes.byref(p))
         out.append((r.value, w.value, b.value, p.value))
     return out
+
+
+def fp_peaks(device: int = 0) -> dict:
+    """Measured CUDA-core peaks of a device (cfs_fp_peaks), TFLOP/s."""
+    lib = load_library()
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    rc = lib.cfs_fp_peaks(int(device), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    if rc != 0:
+        raise CfsError(rc, lib.cfs_last_error(None).decode())
+    return {"fp32_ffma": a.value, "fp32_ffma2": b.value, "fp64_dfma": c.value}
 
 
 def exported_symbols() -> list[str]:

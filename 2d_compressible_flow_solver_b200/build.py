@@ -33,6 +33,7 @@ CU_UNITS = [
     ("kernels_exact.cu", "kernels_exact.cu", ["-fmad=false"]),
     ("kernels_fast.cu", "kernels_fast.cu", []),
     ("cfl_static.cu", "cfl_static.cu", ["-fmad=false"]),
+    ("fp_peaks.cu", "fp_peaks.cu", []),
 ] + [
     (f"march_{form}_{feat}.cu", "march_inst.cu",
      [f"-DCFS_MARCH_POL={pol}", f"-DCFS_MARCH_FEAT={feat}", f"-DCFS_MARCH_FN=launch_march_{form}_{feat}"])

@@ -452,6 +452,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         a.P->seed[1 - a.parity] = a.P->seed[a.parity] + 1u;
     }
     const bool active_warp = j0 < L.ny;  // uniform per warp
+    const bool do_cfl = a.P && a.last_stage && a.P->use_cfl;  // read once: stores to `out` may alias P for the compiler
 
     auto load_row = [&](int r, C out[kVars]) {
         if (col_ok) {
@@ -549,6 +550,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     C FXp[kVars] = {C(0), C(0), C(0), C(0)};   // x-flux through the lower face of the previous row
     C RY[kVars] = {C(0), C(0), C(0), C(0)};    // y part of the previous row's RHS
     unsigned int f_prev = 0u, f_next = 0u;     // flags of rows r-1 and r+1
+    T rv_cur[3] = {T(0), T(0), T(0)}, rv_pf[3] = {T(0), T(0), T(0)};  // kExtra: viscous RHS of rows r-1, r
     double wloc = 0.0;
     if (active_warp && kRing) {
         for (int q = i0 - 3; q <= i0 + 1 + kRingDist; ++q) issue_row(q);
@@ -564,6 +566,15 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
         const unsigned int f_r = f_next;
         f_next = load_flags(r + 1);
+        if constexpr (kExtra) {  // viscous RHS of row r, a whole iteration ahead of its update
+#pragma unroll
+            for (int q = 0; q < 3; ++q) rv_cur[q] = rv_pf[q];
+            if (rv_in && owner && r >= i0 && r < i1) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                    rv_pf[q] = rv_in[static_cast<long long>(q) * L.nx * L.ny + static_cast<long long>(r) * L.ny + j];
+            }
+        }
         if constexpr (kRing) {
             // every lane is done with the previous iteration's slots; the slot
             // now refilled held row r+3+kRingDist-kRingRows, last read at r-1
@@ -637,8 +648,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
-                        if (kExtra && rv_in && v >= 1)
-                            rvf += rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j];
+                        if (kExtra && rv_in && v >= 1) rvf += rv_cur[v - 1];
                         const float cur = pf_cur[v];
                         const float x0 = a.stage == 0 ? cur : pf_u0[v];
                         const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
@@ -659,8 +669,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
                         double rv = -double(FX[v] - FXp[v]) * inv_dx + double(RY[v]);
-                        if (kExtra && rv_in && v >= 1)
-                            rv += double(rv_in[static_cast<long long>(v - 1) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j]);
+                        if (kExtra && rv_in && v >= 1) rv += double(rv_cur[v - 1]);
                         const double cur = double(win[1][v]);
                         const double u0v = a.stage >= 1 ? dec<T>(pf_u0[v], L, v) : 0.0;
                         const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
@@ -688,7 +697,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                     }
                 }
                 store_cell4<T>(out, L, a.bc, i, j, sv);
-                if (a.P && a.last_stage && a.P->use_cfl) {
+                if (do_cfl) {
                     const C w = wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy));
                     if (fluid && double(w) > wloc) wloc = double(w);
                 }
@@ -770,7 +779,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     if constexpr (kRing) cp_async_wait_all();  // no copy into the ring outlives the item
     // CFL maximum: one atomic per warp (no block barrier, so the warps of a
     // block never wait for each other)
-    if (a.P && a.last_stage && a.P->use_cfl) {
+    if (do_cfl) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) wloc = fmax(wloc, __shfl_xor_sync(0xffffffffu, wloc, o));
         if (lane == 0 && wloc > 0.0)

@@ -569,11 +569,12 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------ modes arm
-MODES = {  # name: (side kind, positivity, cylinder)
-    "periodic": ("BC_PERIODIC", "POSITIVITY_OFF", False),
-    "transmissive": ("BC_NEUMANN", "POSITIVITY_OFF", False),
-    "periodic_floors": ("BC_PERIODIC", "POSITIVITY_FLOOR", False),
-    "transmissive_floors_cylinder": ("BC_NEUMANN", "POSITIVITY_FLOOR", True),
+MODES = {  # name: (side kind, positivity, cylinder, Navier-Stokes shear layer instead of quadrants)
+    "periodic": ("BC_PERIODIC", "POSITIVITY_OFF", False, False),
+    "transmissive": ("BC_NEUMANN", "POSITIVITY_OFF", False, False),
+    "periodic_floors": ("BC_PERIODIC", "POSITIVITY_FLOOR", False, False),
+    "transmissive_floors_cylinder": ("BC_NEUMANN", "POSITIVITY_FLOOR", True, False),
+    "periodic_navier_stokes": ("BC_PERIODIC", "POSITIVITY_OFF", False, True),
 }
 
 
@@ -582,20 +583,23 @@ def modes_arm(args):
     four-quadrant state on n^2 cells (default 2048^2), SSP-RK3, Davis HLL, CFL
     0.5, with periodic or transmissive sides, without or with the positivity
     fallbacks and floors, and with a slip-wall cylinder (r = 0.1 at the centre)
-    in the last mode.  Each form, each mode: W warm-up steps, K timed steps with
-    CUDA events on the engine's stream.  `--mode` runs one mode (FP32 only), for
-    a profiler.  One JSON line."""
+    in one mode; the last mode is the periodic Navier-Stokes shear layer (mu =
+    1/2000, Pr 0.72) on the same grid.  Each form, each mode: W warm-up steps, K
+    timed steps with CUDA events on the engine's stream.  `--mode` runs one mode
+    (FP32 only), for a profiler.  One JSON line."""
     import torch
 
     cfsb = importlib.import_module(PKG)
     wl = importlib.import_module(f"{PKG}.workloads")
     n = args.modes_n
-    w = wl.riemann_quadrants(n, n, seed=3)
+    quads = wl.riemann_quadrants(n, n, seed=3)
 
     def rate(prec, mode):
-        side, pos, cyl = MODES[mode]
+        side, pos, cyl, ns = MODES[mode]
+        w = wl.shear_layer(n) if ns else quads
+        extra = dict(viscous=cfsb.VISCOUS_NS, mu=w.meta["mu"], prandtl=0.72, mach=1.0) if ns else {}
         with cfsb.Solver(n, n, 1.0, 1.0, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
-                         bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos)) as s:
+                         bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos), **extra) as s:
             if cyl:
                 s.build_circle(0.1, 0.5, 0.5, 400, cfsb.IB_BILINEAR_SLIP)
             s.set_state(w.U0)

@@ -302,6 +302,15 @@ int cfs_batch_info(const cfs_batch* b, long long* cells, int* items);
 int cfs_compute_dt_static(const double* U, const uint8_t* types, int nx, int ny, double lx, double ly,
                           double gamma, double cfl, void* stream, double* dt);
 
+/* Measured arithmetic peaks of a device's CUDA cores (a diagnostic with no
+ * counterpart in the reference): FP32 FFMA, packed FP32 FFMA2 and FP64 DFMA
+ * throughput in TFLOP/s (2 flops per fused multiply-add), from independent
+ * multiply-add chains filling every SM, best of three timed launches.  The
+ * stage kernels are bound by instruction issue and these pipes, so this is
+ * the denominator of their floating-point roofline.  Takes a few ms and 2.4 MB
+ * of device memory.  Errors: cfs_last_error(NULL). */
+int cfs_fp_peaks(int device, double* fp32_tflops, double* fp32x2_tflops, double* fp64_tflops);
+
 /* Unit-level entry points (device batch, host buffers), mirroring one plugin
  * call each, for parity tests:
  * cfs_weno5_faces: Weno5th::comLeftPhase + comRightPhase (Weno5th.cpp:57-81) on
