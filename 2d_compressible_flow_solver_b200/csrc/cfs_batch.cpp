@@ -27,7 +27,7 @@ struct BatchCase {
     double dx = 0, dy = 0;
     size_t state_off = 0;   // bytes from the arena start to S0 (S1, S2 follow)
     long long types_off = -1;
-    int rows = 32, nseg = 0, items_x = 0, items_y = 0;
+    int rows = 32, nseg = 0, items_y = 0;  // row chunk, 30-column segments, row chunks
     std::vector<uint8_t> types;
     std::vector<uint8_t> lowo;   // CFS_POSITIVITY_BODY face flags, [nx+1][ny+1]
     long long lowo_off = -1;
@@ -69,7 +69,7 @@ struct cfs_batch {
     int* item_case = nullptr;
     int* item_local = nullptr;
     int* case_rows = nullptr;
-    int* case_items_x = nullptr;
+    int* case_nseg = nullptr;
     unsigned int* counters = nullptr;  // [parity][stage]
     double* staging = nullptr;
     int grid = 0;
@@ -188,7 +188,7 @@ int enqueue_batch_step(cfs_batch* b, int parity) {
             CFSB_CUDA(b, cfs::launch_batch_boundary_flux(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->n,
                                                          b->max_edge, b->stream));
         CFSB_CUDA(b, cfs::launch_batch_stage(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->item_case,
-                                             b->item_local, b->case_rows, b->case_items_x, b->total_items,
+                                             b->item_local, b->case_rows, b->case_nseg, b->total_items,
                                              b->counters + slot, b->grid, b->feat, b->stream));
     }
     return CFS_OK;
@@ -221,7 +221,7 @@ int cfs_batch_destroy(cfs_batch* b) {
     cudaFree(b->item_case);
     cudaFree(b->item_local);
     cudaFree(b->case_rows);
-    cudaFree(b->case_items_x);
+    cudaFree(b->case_nseg);
     cudaFree(b->counters);
     cudaFree(b->staging);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -291,7 +291,6 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         c.rows = d.rows > 0 ? d.rows : cfs::kVariants[(b->prec == cfs::kF32Mixed ? cfs::kDefaultVariantF32
                                                                                    : cfs::kDefaultVariantF64) - 1].rows;
         c.nseg = (d.ny + 29) / 30;
-        c.items_x = (c.nseg + cfs::kBatchWarps - 1) / cfs::kBatchWarps;
         c.items_y = (d.nx + c.rows - 1) / c.rows;
         c.state_off = arena;
         arena += static_cast<size_t>(3) * static_cast<size_t>(c.L.bytes());
@@ -351,17 +350,18 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         return static_cast<long long>(b->cases[x].desc.nx) * b->cases[x].desc.ny >
                static_cast<long long>(b->cases[y].desc.nx) * b->cases[y].desc.ny;
     });
+    // one work unit per (segment, row chunk): a warp's share of a stage
     std::vector<int> it_case, it_local, c_rows(ncases), c_ix(ncases);
     for (int ci : order) {
         const BatchCase& c = b->cases[ci];
-        for (int li = 0; li < c.items_x * c.items_y; ++li) {
+        for (int li = 0; li < c.nseg * c.items_y; ++li) {
             it_case.push_back(ci);
             it_local.push_back(li);
         }
     }
     for (int ci = 0; ci < ncases; ++ci) {
         c_rows[ci] = b->cases[ci].rows;
-        c_ix[ci] = b->cases[ci].items_x;
+        c_ix[ci] = b->cases[ci].nseg;
     }
     b->total_items = static_cast<int>(it_case.size());
 
@@ -384,7 +384,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         !dalloc(reinterpret_cast<void**>(&b->item_case), sizeof(int) * it_case.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->item_local), sizeof(int) * it_local.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->case_rows), sizeof(int) * ncases) ||
-        !dalloc(reinterpret_cast<void**>(&b->case_items_x), sizeof(int) * ncases) ||
+        !dalloc(reinterpret_cast<void**>(&b->case_nseg), sizeof(int) * ncases) ||
         !dalloc(reinterpret_cast<void**>(&b->counters), sizeof(unsigned int) * 6) ||
         !dalloc(reinterpret_cast<void**>(&b->staging), sizeof(double) * kVars * max_cells))
         return bail(CFS_ERR_NOMEM, "batch device allocation failed");
@@ -407,7 +407,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
          h2d(b->ig_local, h_igl.data(), sizeof(int) * h_igl.size()) &&
          h2d(b->item_case, it_case.data(), sizeof(int) * it_case.size()) &&
          h2d(b->item_local, it_local.data(), sizeof(int) * it_local.size()) &&
-         h2d(b->case_rows, c_rows.data(), sizeof(int) * ncases) && h2d(b->case_items_x, c_ix.data(), sizeof(int) * ncases) &&
+         h2d(b->case_rows, c_rows.data(), sizeof(int) * ncases) && h2d(b->case_nseg, c_ix.data(), sizeof(int) * ncases) &&
          cudaMemset(b->P, 0, sizeof(cfs::DevParams) * ncases) == cudaSuccess;
     if (!ok) return bail(CFS_ERR_CUDA, "batch upload failed");
     for (int ci = 0; ci < ncases; ++ci)

@@ -54,7 +54,7 @@ constexpr int kBatchMinBlocksF32 = 5;
 constexpr int kBatchLoadF32 = 3;  // FP32 batches stage rows in the shared ring
 constexpr int kBatchMinBlocksF64 = 4;
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
-                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s);  // feat: kFeatPos | kFeatEdge bits
 // Boundary-face fluxes of every case (grid: max_edge = the largest nx or ny).
 cudaError_t launch_batch_boundary_flux(Prec p, const StageArgs* args, int ncases, int max_edge, cudaStream_t s);

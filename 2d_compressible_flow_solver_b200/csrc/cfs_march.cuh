@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArg
 template <class Pol, int kWarps, int kLoad, int kFeat>
 __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][36][kVars],
-                                           typename Pol::T* ring = nullptr) {
+                                           typename Pol::T* ring, int wid) {
     using T = typename Pol::T;
     using C = typename Pol::C;
     constexpr bool kRing = kLoad == 3 && sizeof(T) == 4;
@@ -397,7 +397,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     constexpr bool kExtra = (kFeat & kFeatExtra) != 0;
     constexpr bool kEdge = (kFeat & kFeatEdge) != 0;
     const Layout& L = a.L;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int seg = bx * kWarps + wid;
     const int j0 = seg * kSeg;
     const int i0 = by * rows;
@@ -445,7 +445,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     const uint8_t* const flags = kEdge ? a.cflags : nullptr;
     double* const rhs_out = kExtra ? a.rhs : nullptr;
     const T* const rv_in = kExtra ? static_cast<const T*>(a.rv) : nullptr;
-    if (a.P && a.first_stage && bx == 0 && by == 0 && threadIdx.x == 0) {
+    if (a.P && a.first_stage && seg == 0 && by == 0 && lane == 0) {
         a.P->wmax[1 - a.parity] = 0ull;
         a.P->t += dt;
         a.P->dt_last = dt;
@@ -792,37 +792,38 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const St
     __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
     if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring, threadIdx.x >> 5);
     } else {
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, nullptr, threadIdx.x >> 5);
     }
 }
 
 // Persistent batched form: one launch runs one stage of every case of a batch.
-// Each block pulls work items (case, block column, row chunk) from a global
-// counter, largest cases first, until none are left.  args[c] holds case c's
-// stage arguments (its own layout, boundaries, buffers, dt slot); rows[c] is
-// the row chunk the autotuner chose for its size.
+// Each warp pulls work units (case, segment, row chunk) from a global counter,
+// largest cases first, until none are left; warps share nothing, so a case
+// whose segment count is not a multiple of the block's warps leaves no warp
+// idle.  args[c] holds case c's stage arguments (its own layout, boundaries,
+// buffers, dt slot); rows[c] is its row chunk, nseg[c] its segment count.
 template <class Pol, int kWarps, int kMinBlocks, int kLoad, int kFeat>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
-    batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ item_case,
-                       const int* __restrict__ item_local, const int* __restrict__ case_rows,
-                       const int* __restrict__ case_items_x, int total, unsigned int* counter) {
-    __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
+    batch_march_kernel(const StageArgs* __restrict__ args, const int* __restrict__ unit_case,
+                       const int* __restrict__ unit_local, const int* __restrict__ case_rows,
+                       const int* __restrict__ case_nseg, int total, unsigned int* counter) {
+    using C = typename Pol::C;
+    __shared__ __align__(16) C rbuf[kWarps][36][kVars];
     constexpr bool kRing = kLoad == 3 && sizeof(typename Pol::T) == 4;
     __shared__ __align__(16) typename Pol::T ring[kRing ? kWarps * kRingWords : 1];
-    __shared__ int s_item;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    C(&wbuf)[1][36][kVars] = *reinterpret_cast<C(*)[1][36][kVars]>(&rbuf[wid]);
     for (;;) {
-        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
-        __syncthreads();
-        const int w = s_item;
-        __syncthreads();
-        if (w >= total) break;
-        const int c = item_case[w], li = item_local[w];
-        const int ix = case_items_x[c];
+        unsigned int w = 0u;
+        if (lane == 0) w = atomicAdd(counter, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= static_cast<unsigned int>(total)) break;
+        const int c = unit_case[w], lu = unit_local[w];
+        const int ns = case_nseg[c];
         const StageArgs a = args[c];
-        const int bx = li % ix, by = li / ix, rows = case_rows[c];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, bx, by, rows, rbuf, kRing ? ring : nullptr);
+        march_item<Pol, 1, kLoad, kFeat>(a, lu % ns, lu / ns, case_rows[c], wbuf, kRing ? ring + wid * kRingWords : nullptr, 0);
     }
 }
 

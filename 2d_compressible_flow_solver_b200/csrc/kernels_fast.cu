@@ -55,24 +55,24 @@ cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
 // and have no viscous terms).
 template <class Pol, int kMinBlocks, int kLoad>
 cudaError_t launch_batch_march(const StageArgs* args, const int* item_case, const int* item_local,
-                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s) {
     switch (feat) {
         case 0:
             batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, 0><<<grid, 32 * kBatchWarps, 0, s>>>(
-                args, item_case, item_local, case_rows, case_items_x, total, counter);
+                args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatPos:
             batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
-                args, item_case, item_local, case_rows, case_items_x, total, counter);
+                args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatEdge:
             batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge><<<grid, 32 * kBatchWarps, 0, s>>>(
-                args, item_case, item_local, case_rows, case_items_x, total, counter);
+                args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatEdge | kFeatPos:
             batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge | kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
-                args, item_case, item_local, case_rows, case_items_x, total, counter);
+                args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         default:
             return cudaErrorInvalidValue;
@@ -81,13 +81,13 @@ cudaError_t launch_batch_march(const StageArgs* args, const int* item_case, cons
 }
 
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
-                               const int* case_rows, const int* case_items_x, int total, unsigned int* counter,
+                               const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s) {
     if (total <= 0) return cudaSuccess;
     if (p == kF32Mixed)
         return launch_batch_march<PolF32, kBatchMinBlocksF32, kBatchLoadF32>(args, item_case, item_local, case_rows,
-                                                                             case_items_x, total, counter, grid, feat, s);
-    return launch_batch_march<PolF64, kBatchMinBlocksF64, 0>(args, item_case, item_local, case_rows, case_items_x,
+                                                                             case_nseg, total, counter, grid, feat, s);
+    return launch_batch_march<PolF64, kBatchMinBlocksF64, 0>(args, item_case, item_local, case_rows, case_nseg,
                                                              total, counter, grid, feat, s);
 }
 

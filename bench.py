@@ -54,6 +54,11 @@ WORDS_PER_CELL_STEP = 32
 # ncu capture of the tuned FP32 march kernel at 4096^2 summarised in
 # profiles/march_kernel_f32_smooth4096_traffic.md.
 MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
+# Floating-point operations the FP32-mixed march executes per cell-step (its
+# three stage launches; packed FFMA2 = 4, FADD2/FMUL2 = 2, FFMA/DFMA = 2, others
+# 1), from ncu's per-opcode thread-instruction counts of the periodic 2048^2 run
+# in profiles/march_kernel_f32_flops2048.md.  Data-independent on smooth states.
+MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2888.8, "fp64": 40.8}}
 
 
 def env_rank():
@@ -262,6 +267,9 @@ def engine_arm(args):
         launches = 3 * K + 1 if world == 1 else 4 * K  # slabs: 3 stages + 1 CFL launch per step
         per_launch_ms = ms32 / launches
         trf = MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH["f32"]
+        fl = MEASURED_FLOPS_PER_CELL_STEP["f32"]
+        fp_peak = cfsb.fp_peaks(local)
+        fp_achieved = (fl["fp32"] + fl["fp64"]) * cells * K / (ms32 / 1e3) / 1e12
         result = {
             "metric": METRIC, "value": round(v32, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": round(ms32 / K, 4), "higher_is_better": True, "scaling": "weak",
@@ -282,7 +290,15 @@ def engine_arm(args):
                          "traffic_is": "DRAM bytes per stage launch (ncu dram__bytes_read+write, 4096^2, "
                                        "profiles/march_kernel_f32_smooth4096_traffic.md)",
                          "algorithmic_bytes_per_cell_step": WORDS_PER_CELL_STEP * 4,
-                         "avg_stage_launch_ms": round(per_launch_ms, 4)},
+                         "avg_stage_launch_ms": round(per_launch_ms, 4),
+                         "fp_pipe": {"achieved": round(fp_achieved, 2), "unit": "TFLOP/s",
+                                     "peak": round(fp_peak["fp32_ffma"], 2),
+                                     "frac": round(fp_achieved / fp_peak["fp32_ffma"], 4),
+                                     "peak_source": "measured in this run (cfs_fp_peaks: FP32 FFMA chains; "
+                                                    f"packed FFMA2 {fp_peak['fp32_ffma2']:.1f}, "
+                                                    f"FP64 DFMA {fp_peak['fp64_dfma']:.1f} TFLOP/s)",
+                                     "flops_per_cell_step": round(fl["fp32"] + fl["fp64"], 1),
+                                     "flops_source": "ncu per-opcode counts, profiles/march_kernel_f32_flops2048.md"}},
             "fp64": {"value": round(v64, 1), "ms_per_step": round(ms64 / K, 4),
                      "roofline_frac": round(WORDS_PER_CELL_STEP * 8 * cells * K / (ms64 / 1e3) / 1e9 / peak, 4),
                      "fp32_over_fp64": round(v32 / v64, 3)},

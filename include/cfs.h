@@ -255,8 +255,8 @@ int cfs_conserved_totals(cfs_ctx* ctx, double totals[4]);
 
 /* ---- Batched cases -------------------------------------------------------
  * Hundreds of independent grids of uneven size advanced together: every stage
- * of every case runs in ONE persistent launch whose blocks pull work items
- * (case, block column, row chunk) from a device counter, largest cases first;
+ * of every case runs in ONE persistent launch whose warps pull work items
+ * (case, 30-column segment, row chunk) from a device counter, largest cases first;
  * each case keeps its own CFL time step, computed on the device; whole steps
  * are replayed from a CUDA graph.  Throughput forms only (CFS_FP32_MIXED,
  * CFS_FP64).  No reference counterpart (the reference runs one grid). */
