@@ -49,6 +49,14 @@ __device__ __forceinline__ T enc(double value, const Layout& L, int v) {
 // std::min / std::max as the reference uses them (RiemmanSolverHLL.cpp:41-42):
 // the first argument is returned unless the second compares smaller (larger),
 // so a NaN second argument is dropped.
+// Packed FP32 (sm_100 FFMA2 / FADD2 / FMUL2: two independent FP32 operations
+// per instruction, each rounded as its scalar form).
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, p2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 template <class C> __device__ __forceinline__ C min_ref(C a, C b) { return (b < a) ? b : a; }
 template <class C> __device__ __forceinline__ C max_ref(C a, C b) { return (a < b) ? b : a; }
 
@@ -220,6 +228,20 @@ __device__ __forceinline__ void hll_flux(const Face5<typename Pol::C>& L, const 
             SL = min_ref(uL - aL, uR - aR);
             SR = max_ref(uL + aL, uR + aR);
         }
+    }
+    if constexpr (Pol::kMixed) {
+        // the HLL average on (rho, m_x) and (m_y, E) in packed FP32, then the
+        // upwind cases as selects
+        const float inv = rcp_fast(SR - SL);
+        const float2 sr = p2(SR), msl = p2(-SL), slsr = p2(SL * SR), iv = p2(inv);
+        const float2 H01 = mul2(fma2(slsr, sub2(make_float2(R.r, R.mx), make_float2(L.r, L.mx)),
+                                     fma2(msl, make_float2(FR[0], FR[1]), mul2(sr, make_float2(FL[0], FL[1])))), iv);
+        const float2 H23 = mul2(fma2(slsr, sub2(make_float2(R.my, R.E), make_float2(L.my, L.E)),
+                                     fma2(msl, make_float2(FR[2], FR[3]), mul2(sr, make_float2(FL[2], FL[3])))), iv);
+        const float H[4] = {H01.x, H01.y, H23.x, H23.y};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) F[q] = SL >= 0 ? FL[q] : (SR <= 0 ? FR[q] : H[q]);
+        return;
     }
     if (SL >= 0) {
 #pragma unroll

@@ -76,11 +76,6 @@ __device__ __forceinline__ void weno5_pair(C v0, C v1, C v2, C v3, C v4, C eps, 
 // FADD2 / FMUL2: two independent FP32 operations per instruction, each rounded
 // as its scalar form), for the FP32-mixed form, whose row loop is bound by
 // instruction issue.  The reciprocals stay scalar.
-__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, p2(-1.0f), a); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 __device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, float2 v3, float2 v4, float eps,
                                               float2& left, float2& right) {
@@ -410,7 +405,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     const double g = a.gamma;
     const double dt = stage_dt(a);
     const double inv_dx = 1.0 / a.dx, inv_dy = 1.0 / a.dy;
-    const float inv_dxf = float(inv_dx);
+    const float inv_dxf = float(inv_dx), inv_dyf = float(inv_dy);
     // FP32 update coefficients of this stage: new = cA x0 + cB x1 + (c dt) R with
     // x0 = U^0 (or the current state at stage 0), x1 = U^1 (TVD3 as written,
     // stage 2) or the current state (TVD2rdRK.h:16-19, TVD3rdRK.h:14-18).
@@ -749,7 +744,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
             for (int v = 0; v < kVars; ++v) {
                 const C below = __shfl_up_sync(0xffffffffu, FY[v], 1);
-                RY[v] = C(-double(FY[v] - below) * inv_dy);
+                if constexpr (Pol::kMixed) RY[v] = (below - FY[v]) * inv_dyf;  // as the x part: FP32
+                else RY[v] = C(-double(FY[v] - below) * inv_dy);
             }
             __syncwarp();
         }
