@@ -58,7 +58,7 @@ MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
 # three stage launches; packed FFMA2 = 4, FADD2/FMUL2 = 2, FFMA/DFMA = 2, others
 # 1), from ncu's per-opcode thread-instruction counts of the periodic 2048^2 run
 # in profiles/march_kernel_f32_flops2048.md.  Data-independent on smooth states.
-MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2888.8, "fp64": 40.8}}
+MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2927.9, "fp64": 27.9}}
 
 
 def env_rank():
