@@ -106,6 +106,12 @@ _SIGNATURES = {
                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _c_uint8_p,
                                         ctypes.c_int, ctypes.POINTER(ctypes.c_int), _c_int32_p, _c_int32_p,
                                         _c_double_p, _c_double_p]),
+    "cfs_ib_build_circle_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "cfs_circle_setup_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_int, _c_uint8_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                               _c_int32_p, _c_int32_p, _c_double_p, _c_double_p]),
     "cfs_get_ib": (ctypes.c_int, [ctypes.c_void_p, _c_uint8_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                   _c_int32_p, _c_int32_p, _c_double_p]),
     "cfs_ib_fill": (ctypes.c_int, [ctypes.c_void_p]),
@@ -185,23 +191,30 @@ def exported_symbols() -> list[str]:
     return list(_SIGNATURES)
 
 
-def circle_setup(nx: int, ny: int, lx: float, ly: float, radius: float, cx: float, cy: float, npoints: int = 400):
-    """Host-only circle immersed-boundary set-up (cfs_circle_setup): returns
-    (types[nx, ny], cells[n], donors[n, 4], images[n, 2], normals[n, 2])."""
+def circle_setup(nx: int, ny: int, lx: float, ly: float, radius: float, cx: float, cy: float, npoints: int = 400,
+                 device: int | None = None):
+    """Circle immersed-boundary set-up: returns (types[nx, ny], cells[n],
+    donors[n, 4], images[n, 2], normals[n, 2]).  device=None: the host set-up
+    (cfs_circle_setup); an ordinal: the per-cell work on that GPU
+    (cfs_circle_setup_device), bit for bit the same result."""
     lib = load_library()
     types = np.empty((nx, ny), dtype=np.uint8)
     n = ctypes.c_int(0)
     args = (int(nx), int(ny), float(lx), float(ly), float(radius), float(cx), float(cy), int(npoints))
-    rc = lib.cfs_circle_setup(*args, types.ctypes.data_as(_c_uint8_p), 0, ctypes.byref(n), None, None, None, None)
+    if device is None:
+        call = lib.cfs_circle_setup
+    else:
+        def call(*a):
+            return lib.cfs_circle_setup_device(int(device), *a)
+    rc = call(*args, types.ctypes.data_as(_c_uint8_p), 0, ctypes.byref(n), None, None, None, None)
     if rc != 0:
         raise CfsError(rc, lib.cfs_last_error(None).decode())
     cells = np.empty(n.value, dtype=np.int32)
     donors = np.empty((n.value, 4), dtype=np.int32)
     images = np.empty((n.value, 2))
     normals = np.empty((n.value, 2))
-    rc = lib.cfs_circle_setup(*args, None, n.value, ctypes.byref(n), cells.ctypes.data_as(_c_int32_p),
-                              donors.ctypes.data_as(_c_int32_p), images.ctypes.data_as(_c_double_p),
-                              normals.ctypes.data_as(_c_double_p))
+    rc = call(*args, None, n.value, ctypes.byref(n), cells.ctypes.data_as(_c_int32_p),
+              donors.ctypes.data_as(_c_int32_p), images.ctypes.data_as(_c_double_p), normals.ctypes.data_as(_c_double_p))
     if rc != 0:
         raise CfsError(rc, lib.cfs_last_error(None).decode())
     return types, cells, donors, images, normals
@@ -299,8 +312,12 @@ class Solver:
                                          donors.ctypes.data_as(_c_int32_p), _dp(images),
                                          None if nrm is None else _dp(nrm)))
 
-    def build_circle(self, radius: float, cx: float, cy: float, npoints: int = 400, mode: int = IB_REFERENCE) -> None:
-        self._check(self._lib.cfs_ib_build_circle(self._ctx, radius, cx, cy, int(npoints), int(mode)))
+    def build_circle(self, radius: float, cx: float, cy: float, npoints: int = 400, mode: int = IB_REFERENCE,
+                     on_device: bool = False) -> None:
+        """Circle immersed boundary (cfs_ib_build_circle; on_device: the per-cell
+        set-up on the GPU, cfs_ib_build_circle_device, the same result)."""
+        fn = self._lib.cfs_ib_build_circle_device if on_device else self._lib.cfs_ib_build_circle
+        self._check(fn(self._ctx, radius, cx, cy, int(npoints), int(mode)))
 
     def get_ib(self):
         """Returns (types[nx, ny], cells[n], donors[n, 4], images[n, 2])."""

@@ -34,6 +34,7 @@ CU_UNITS = [
     ("kernels_fast.cu", "kernels_fast.cu", []),
     ("cfl_static.cu", "cfl_static.cu", ["-fmad=false"]),
     ("fp_peaks.cu", "fp_peaks.cu", []),
+    ("ib_device.cu", "ib_device.cu", ["-fmad=false"]),
 ] + [
     (f"march_{form}_{feat}.cu", "march_inst.cu",
      [f"-DCFS_MARCH_POL={pol}", f"-DCFS_MARCH_FEAT={feat}", f"-DCFS_MARCH_FN=launch_march_{form}_{feat}"])

@@ -550,13 +550,23 @@ int cfs_ib_build_circle(cfs_ctx* c, double radius, double cx, double cy, int npo
                       ib.normal.data());
 }
 
-int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
-                     uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy,
-                     double* normal_xy) {
-    if (nx < 1 || ny < 1 || !(lx > 0) || !(ly > 0)) return fail(nullptr, CFS_ERR_INVALID, "bad grid");
+int cfs_ib_build_circle_device(cfs_ctx* c, double radius, double cx, double cy, int npoints, int mode) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     cfs::IbList ib;
     std::string err;
-    if (!cfs::build_circle(nx, ny, lx, ly, radius, cx, cy, npoints, ib, err)) return fail(nullptr, CFS_ERR_INVALID, err);
+    if (!cfs::build_circle_device(c->cfg.nx, c->cfg.ny, c->cfg.lx, c->cfg.ly, radius, cx, cy, npoints, c->stream, ib, err))
+        return fail(c, err.rfind("device circle set-up", 0) == 0 ? CFS_ERR_CUDA : CFS_ERR_INVALID, err);
+    const int rc = cfs_set_cell_types(c, ib.types.data());
+    if (rc != CFS_OK) return rc;
+    return cfs_set_ib(c, mode, static_cast<int>(ib.cell.size()), ib.cell.data(), ib.donor.data(), ib.image.data(),
+                      ib.normal.data());
+}
+
+namespace {
+
+int circle_setup_out(const cfs::IbList& ib, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4,
+                     double* image_xy, double* normal_xy) {
     if (types) std::memcpy(types, ib.types.data(), ib.types.size());
     const int total = static_cast<int>(ib.cell.size());
     if (n) *n = total;
@@ -571,6 +581,34 @@ int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double
         }
     }
     return CFS_OK;
+}
+
+}  // namespace
+
+int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
+                     uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy,
+                     double* normal_xy) {
+    if (nx < 1 || ny < 1 || !(lx > 0) || !(ly > 0)) return fail(nullptr, CFS_ERR_INVALID, "bad grid");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_circle(nx, ny, lx, ly, radius, cx, cy, npoints, ib, err)) return fail(nullptr, CFS_ERR_INVALID, err);
+    return circle_setup_out(ib, types, max_n, n, cell, donor4, image_xy, normal_xy);
+}
+
+int cfs_circle_setup_device(int device, int nx, int ny, double lx, double ly, double radius, double cx, double cy,
+                            int npoints, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4,
+                            double* image_xy, double* normal_xy) {
+    if (nx < 1 || ny < 1 || !(lx > 0) || !(ly > 0)) return fail(nullptr, CFS_ERR_INVALID, "bad grid");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, CFS_ERR_CUDA, "no CUDA device available (the device set-up has no CPU path)");
+    if (device < 0 || device >= ndev) return fail(nullptr, CFS_ERR_INVALID, "device ordinal out of range");
+    if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, CFS_ERR_CUDA, "cudaSetDevice failed");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_circle_device(nx, ny, lx, ly, radius, cx, cy, npoints, nullptr, ib, err))
+        return fail(nullptr, err.rfind("device circle set-up", 0) == 0 ? CFS_ERR_CUDA : CFS_ERR_INVALID, err);
+    return circle_setup_out(ib, types, max_n, n, cell, donor4, image_xy, normal_xy);
 }
 
 int cfs_get_ib(cfs_ctx* c, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy) {

@@ -309,8 +309,11 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         if (d.circle) {
             cfs::IbList ib;
             std::string e;
-            if (!cfs::build_circle(d.nx, d.ny, d.lx, d.ly, d.radius, d.cx, d.cy, d.npoints > 0 ? d.npoints : 400, ib, e))
-                return bail(CFS_ERR_INVALID, "case " + std::to_string(ci) + ": " + e);
+            // per-cell set-up on the device (bit for bit the host set-up's result)
+            if (!cfs::build_circle_device(d.nx, d.ny, d.lx, d.ly, d.radius, d.cx, d.cy, d.npoints > 0 ? d.npoints : 400,
+                                          b->stream, ib, e))
+                return bail(e.rfind("device circle set-up", 0) == 0 ? CFS_ERR_CUDA : CFS_ERR_INVALID,
+                            "case " + std::to_string(ci) + ": " + e);
             c.types = ib.types;
             c.types_off = static_cast<long long>(types_bytes);
             types_bytes += c.types.size();

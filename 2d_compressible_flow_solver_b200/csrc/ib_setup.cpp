@@ -33,6 +33,61 @@ inline double norm(P2 v) { return std::sqrt(v.x * v.x + v.y * v.y); }
 
 }  // namespace
 
+void circle_polygon(double radius, double cx, double cy, int npoints, std::vector<double>& pts_xy,
+                    std::vector<double>& dir_xy) {
+    // Circle::Initialize (Circle.cpp:12-41): polygon vertices and unit segment
+    // directions (segment k runs from vertex k to vertex k+1).
+    pts_xy.assign(2 * static_cast<size_t>(npoints), 0.0);
+    dir_xy.assign(2 * static_cast<size_t>(npoints), 0.0);
+    for (int k = 0; k < npoints; ++k) {
+        const double angle = 2.0 * M_PI * static_cast<double>(k) / static_cast<double>(npoints);
+        pts_xy[2 * k] = cx + radius * std::cos(angle);
+        pts_xy[2 * k + 1] = cy + radius * std::sin(angle);
+    }
+    for (int k = 0; k < npoints; ++k) {
+        const int k1 = (k + 1) % npoints;
+        const P2 d = normalized({pts_xy[2 * k1] - pts_xy[2 * k], pts_xy[2 * k1 + 1] - pts_xy[2 * k + 1]});
+        dir_xy[2 * k] = d.x;
+        dir_xy[2 * k + 1] = d.y;
+    }
+}
+
+bool select_donors(const uint8_t* t, int nx, int ny, double dx, double dy, const std::vector<int32_t>& cells,
+                   const std::vector<double>& image, std::vector<int32_t>& donor, std::string& err) {
+    // FindNearest4FluidCellsIndexed (Circle.cpp:160-215): fluid cells of the
+    // 11 x 11 window around the image point's cell, visited i outer / j inner,
+    // sorted by squared distance with the same comparator.
+    auto centre = [&](int i, int j) { return P2{(i + 0.5) * dx, (j + 0.5) * dy}; };  // CartesianMesh.cpp:92
+    const P2 origin = centre(0, 0);
+    donor.clear();
+    donor.reserve(4 * cells.size());
+    std::vector<std::pair<double, int>> cand;
+    for (size_t g = 0; g < cells.size(); ++g) {
+        const P2 img{image[2 * g], image[2 * g + 1]};
+        const int ic = static_cast<int>((img.x - origin.x) / dx);
+        const int jc = static_cast<int>((img.y - origin.y) / dy);
+        cand.clear();
+        for (int a = ic - 5; a <= ic + 5; ++a)
+            for (int b = jc - 5; b <= jc + 5; ++b) {
+                if (a >= 0 && a < nx && b >= 0 && b < ny && t[static_cast<size_t>(a) * ny + b] == 0) {
+                    const P2 c = centre(a, b);
+                    const double ddx = c.x - img.x, ddy = c.y - img.y;
+                    cand.emplace_back(ddx * ddx + ddy * ddy, a * ny + b);
+                }
+            }
+        std::sort(cand.begin(), cand.end(),
+                  [](const std::pair<double, int>& p, const std::pair<double, int>& q) { return p.first < q.first; });
+        if (cand.size() < 4) {
+            const int i = cells[g] / ny, j = cells[g] % ny;
+            err = "immersed-ghost cell (" + std::to_string(i) + ", " + std::to_string(j) + ") has " +
+                  std::to_string(cand.size()) + " fluid donors, 4 needed";
+            return false;
+        }
+        for (int k = 0; k < 4; ++k) donor.push_back(cand[k].second);
+    }
+    return true;
+}
+
 bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
                   IbList& out, std::string& err) {
     if (npoints < 3) {
@@ -41,18 +96,8 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
     }
     const double dx = lx / nx, dy = ly / ny;  // CartesianMesh::CalCellsize (CartesianMesh.cpp:150-154)
     auto centre = [&](int i, int j) { return P2{(i + 0.5) * dx, (j + 0.5) * dy}; };  // CartesianMesh.cpp:92
-
-    // Circle::Initialize (Circle.cpp:12-41): polygon vertices and unit segment
-    // directions (segment k runs from vertex k to vertex k+1).
-    std::vector<P2> pts(npoints), dir(npoints);
-    for (int k = 0; k < npoints; ++k) {
-        const double angle = 2.0 * M_PI * static_cast<double>(k) / static_cast<double>(npoints);
-        pts[k] = {cx + radius * std::cos(angle), cy + radius * std::sin(angle)};
-    }
-    for (int k = 0; k < npoints; ++k) {
-        const P2 a = pts[k], b = pts[(k + 1) % npoints];
-        dir[k] = normalized({b.x - a.x, b.y - a.y});
-    }
+    std::vector<double> pts, dir;
+    circle_polygon(radius, cx, cy, npoints, pts, dir);
 
     // DistinguishWallandFluid (Circle.cpp:43-51): solid iff |x_c - c| <= r.
     std::vector<uint8_t>& t = out.types;
@@ -83,10 +128,8 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
         }
 
     out.cell.clear();
-    out.donor.clear();
     out.image.clear();
     out.normal.clear();
-    const P2 origin = centre(0, 0);
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j) {
             if (at(i, j) != 2) continue;
@@ -96,7 +139,7 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
             double minDistance = std::numeric_limits<double>::max();
             P2 intercept{0.0, 0.0};
             for (int k = 0; k < npoints; ++k) {
-                const P2 s = dir[k], a = pts[k];
+                const P2 s{dir[2 * k], dir[2 * k + 1]}, a{pts[2 * k], pts[2 * k + 1]};
                 const double dd = s.x * (pos.x - a.x) + s.y * (pos.y - a.y);
                 const P2 proj{dd * s.x + a.x, dd * s.y + a.y};
                 const double dist = norm({proj.x - pos.x, proj.y - pos.y});
@@ -106,37 +149,13 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
                 }
             }
             const P2 n = normalized({intercept.x - pos.x, intercept.y - pos.y});
-            const P2 img{pos.x + 2 * (minDistance * n.x), pos.y + 2 * (minDistance * n.y)};
-
-            // FindNearest4FluidCellsIndexed (Circle.cpp:160-215): fluid cells of
-            // the 11 x 11 window around the image point's cell, visited i outer /
-            // j inner, sorted by squared distance with the same comparator.
-            const int ic = static_cast<int>((img.x - origin.x) / dx);
-            const int jc = static_cast<int>((img.y - origin.y) / dy);
-            std::vector<std::pair<double, int>> cand;
-            for (int a = ic - 5; a <= ic + 5; ++a)
-                for (int b = jc - 5; b <= jc + 5; ++b) {
-                    if (a >= 0 && a < nx && b >= 0 && b < ny && at(a, b) == 0) {
-                        const P2 c = centre(a, b);
-                        const double ddx = c.x - img.x, ddy = c.y - img.y;
-                        cand.emplace_back(ddx * ddx + ddy * ddy, a * ny + b);
-                    }
-                }
-            std::sort(cand.begin(), cand.end(),
-                      [](const std::pair<double, int>& p, const std::pair<double, int>& q) { return p.first < q.first; });
-            if (cand.size() < 4) {
-                err = "immersed-ghost cell (" + std::to_string(i) + ", " + std::to_string(j) + ") has " +
-                      std::to_string(cand.size()) + " fluid donors, 4 needed";
-                return false;
-            }
             out.cell.push_back(i * ny + j);
-            for (int k = 0; k < 4; ++k) out.donor.push_back(cand[k].second);
-            out.image.push_back(img.x);
-            out.image.push_back(img.y);
+            out.image.push_back(pos.x + 2 * (minDistance * n.x));
+            out.image.push_back(pos.y + 2 * (minDistance * n.y));
             out.normal.push_back(n.x);
             out.normal.push_back(n.y);
         }
-    return true;
+    return select_donors(t.data(), nx, ny, dx, dy, out.cell, out.image, out.donor, err);
 }
 
 // Outer-product LDL^T with symmetric diagonal pivoting (largest remaining

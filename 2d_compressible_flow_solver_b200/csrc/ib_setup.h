@@ -21,6 +21,23 @@ struct IbList {
 bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
                   IbList& out, std::string& err);
 
+// The same set-up with the per-cell work on the device (ib_device.cu):
+// classification, ghost marking and image points as kernels (bit for bit the
+// host doubles: built without FMA contraction), donors on the host from the
+// read-back types (the reference's sort order).  Uses the current device and
+// `stream` (waits for it).
+bool build_circle_device(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
+                         void* stream, IbList& out, std::string& err);
+
+// Pieces shared by both: the polygon of Circle::Initialize (Circle.cpp:12-41) as
+// vertex and unit-direction arrays [2*npoints]; and the 4 nearest fluid donors
+// of each image point (FindNearest4FluidCellsIndexed, Circle.cpp:160-215),
+// false when one has fewer than 4.
+void circle_polygon(double radius, double cx, double cy, int npoints, std::vector<double>& pts_xy,
+                    std::vector<double>& dir_xy);
+bool select_donors(const uint8_t* types, int nx, int ny, double dx, double dy, const std::vector<int32_t>& cells,
+                   const std::vector<double>& image, std::vector<int32_t>& donor, std::string& err);
+
 // Pivoted LDL^T of the symmetric matrix read from the lower triangle of M
 // (Eigen's ldlt(), ImagePoint.cpp:44): fac = l10 l20 l21 l30 l31 l32 d0 d1 d2 d3.
 void ldlt4_lower(const double M[4][4], double fac[10], int perm[4]);

@@ -415,8 +415,12 @@ def batch_arm(args):
                        "cylinder (slip wall), SSP-RK3, Davis HLL, positivity fallbacks with floors, per-case CFL 0.5",
            "steps": K, "warmup": W}
 
+    create_s = {}
+
     def run_batch(prec):
+        t0 = time.perf_counter()
         with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR, device=local) as b:
+            create_s[prec] = time.perf_counter() - t0
             cells, items = b.info()
             for k, U in enumerate(states):
                 b.set_state(k, U)
@@ -433,7 +437,8 @@ def batch_arm(args):
     cells, items, v32, w32 = run_batch(cfsb.FP32_MIXED)
     _, _, v64, w64 = run_batch(cfsb.FP64)
     out.update({"cells": cells, "work_items_per_stage": items,
-                "batched_fp32": round(v32, 1), "batched_fp64": round(v64, 1)})
+                "batched_fp32": round(v32, 1), "batched_fp64": round(v64, 1),
+                "create_s_fp32": round(create_s[cfsb.FP32_MIXED], 3)})
     solvers = []
     for c, U in zip(cases, states):
         s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
@@ -534,6 +539,22 @@ def report_arm(args):
     compare("shear_layer_1024_ns", w4, 5000, 0.5,
             dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, viscous=cfsb.VISCOUS_NS, mu=w4.meta["mu"], prandtl=0.72,
                  mach=1.0), periodic=True)
+    # immersed-boundary set-up of the cylinder grid on the host and on the device
+    def best_s(fn, reps=3):
+        best = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r = fn()
+            dt = time.perf_counter() - t0
+            best = dt if best is None or dt < best else best
+        return best, r
+    geo = (w3.nx, w3.ny, w3.lx, w3.ly, *w3.circle, 400)
+    th, rh = best_s(lambda: cfsb.circle_setup(*geo))
+    td, rd = best_s(lambda: cfsb.circle_setup(*geo, device=0))
+    out["ib_setup_2048x1024"] = {"host_ms": round(th * 1e3, 2), "device_ms": round(td * 1e3, 2),
+                                 "ghost_cells": int(rh[1].size),
+                                 "identical": all(np.array_equal(a, b) for a, b in zip(rh, rd)),
+                                 "timing": "host wall clock, best of 3, both through the C ABI with host outputs"}
     cases, states = wl.batch_cases(args.cases, seed=1)
     res = {}
     for prec in (cfsb.FP64, cfsb.FP32_MIXED):

@@ -189,6 +189,20 @@ int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double
                      uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4, double* image_xy,
                      double* normal_xy);
 
+/* The same circle set-up with its per-cell work on the device (no counterpart
+ * in the reference, whose set-up is host code): classification, ghost marking
+ * and image points run as kernels built without FMA contraction, so types,
+ * ghost list, image points and normals are bit for bit those of the host
+ * set-up; the donors are chosen on the host from the read-back types (the
+ * reference's sort and tie order).  cfs_ib_build_circle_device uses the
+ * context's device and stream; cfs_circle_setup_device the given device and
+ * its default stream, with cfs_circle_setup's outputs.  Errors as
+ * cfs_ib_build_circle, plus CFS_ERR_CUDA for a device failure. */
+int cfs_ib_build_circle_device(cfs_ctx* ctx, double radius, double cx, double cy, int npoints, int mode);
+int cfs_circle_setup_device(int device, int nx, int ny, double lx, double ly, double radius, double cx, double cy,
+                            int npoints, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4,
+                            double* image_xy, double* normal_xy);
+
 /* Read-back of the immersed-boundary set-up: types[nx][ny], and for the first
  * min(n, max_n) immersed-ghost cells (i outer, j inner order) their cell
  * index, donors and image point.  *n receives the total count. */
