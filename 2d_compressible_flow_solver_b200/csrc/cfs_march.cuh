@@ -207,6 +207,17 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool val
     const int n = valid ? 4 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    const int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+// one element of the stored state, zero filled when not valid
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem, bool valid) {
+    if constexpr (sizeof(T) == 8) cp_async8(smem, gmem, valid);
+    else cp_async4(smem, gmem, valid);
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -386,8 +397,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                                            typename Pol::T* ring, int wid) {
     using T = typename Pol::T;
     using C = typename Pol::C;
-    constexpr bool kRing = kLoad == 3 && sizeof(T) == 4;
-    constexpr int kL = (kLoad == 3 && !kRing) ? 0 : kLoad;  // effective schedule
+    constexpr bool kRing = kLoad == 3;
+    constexpr int kL = kLoad;
     constexpr bool kPos = (kFeat & kFeatPos) != 0;
     constexpr bool kExtra = (kFeat & kFeatExtra) != 0;
     constexpr bool kEdge = (kFeat & kFeatEdge) != 0;
@@ -513,20 +524,20 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 T* dst = ring_row(q);
                 const long long off = L.offset(q, col_ok ? j : 0);
 #pragma unroll
-                for (int v = 0; v < kVars; ++v) cp_async4(dst + (lane + 2) * kVars + v, in + v * L.plane + off, col_ok);
+                for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + (lane + 2) * kVars + v, in + v * L.plane + off, col_ok);
                 if (lane < 2 || lane >= 30) {
                     const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
                     const bool ok = hc <= L.ny + kGhost - 1;
                     const long long hoff = L.offset(q, ok ? hc : 0);
                     const int slot = lane < 2 ? lane : lane + 4;
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) cp_async4(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
+                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
                 }
                 if (a.stage >= 1 && owner && q >= i0 && q < i1) {
                     T* du = ring_u0(q);
                     const T* u0p = static_cast<const T*>(a.u0);
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) cp_async4(du + lane * kVars + v, u0p + v * L.plane + off, true);
+                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(du + lane * kVars + v, u0p + v * L.plane + off, true);
                 }
             }
             cp_async_commit();
@@ -535,7 +546,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     // full value of a stencil cell (the ring holds stored deviations)
     auto full = [&](const C w[kVars], C out[kVars]) {
 #pragma unroll
-        for (int v = 0; v < kVars; ++v) out[v] = kRing ? w[v] + C(L.off[v]) : w[v];
+        for (int v = 0; v < kVars; ++v) out[v] = (kRing && Pol::kMixed) ? w[v] + C(L.off[v]) : w[v];
     };
 
     C win[5][kVars];
@@ -589,7 +600,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
         // ---- x reconstruction of row r
         Face5<C> Lr, Rr;
-        cell_states<Pol>(win, eps, g, Lr, Rr, kRing ? L.off : nullptr);
+        cell_states<Pol>(win, eps, g, Lr, Rr, (kRing && Pol::kMixed) ? L.off : nullptr);
         if constexpr (kPos) {
             C cc[kVars];
             full(win[2], cc);
@@ -719,7 +730,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 for (int k = 0; k < 5; ++k) get_slot<C>(rb[lane + k], st[k]);
             }
             Face5<C> Ly, Ry;
-            cell_states<Pol>(st, eps, g, Ly, Ry, kRing ? L.off : nullptr);
+            cell_states<Pol>(st, eps, g, Ly, Ry, (kRing && Pol::kMixed) ? L.off : nullptr);
             if constexpr (kPos) {
                 C cc[kVars];
                 full(st[2], cc);
@@ -789,6 +800,12 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const St
     if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring, threadIdx.x >> 5);
+    } else if constexpr (kLoad == 3) {
+        // FP64 ring: kWarps * kRingWords doubles (69.6 KB for 4 warps), above the
+        // 48 KB of static shared memory: dynamic, sized at launch
+        extern __shared__ __align__(16) unsigned char march_dyn_smem[];
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf,
+                                              reinterpret_cast<typename Pol::T*>(march_dyn_smem), threadIdx.x >> 5);
     } else {
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, nullptr, threadIdx.x >> 5);
     }
@@ -807,8 +824,11 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
                        const int* __restrict__ case_nseg, int total, unsigned int* counter) {
     using C = typename Pol::C;
     __shared__ __align__(16) C rbuf[kWarps][36][kVars];
-    constexpr bool kRing = kLoad == 3 && sizeof(typename Pol::T) == 4;
-    __shared__ __align__(16) typename Pol::T ring[kRing ? kWarps * kRingWords : 1];
+    constexpr bool kRing = kLoad == 3;
+    constexpr bool kDynRing = kRing && sizeof(typename Pol::T) == 8;  // FP64: ring in dynamic shared memory
+    __shared__ __align__(16) typename Pol::T ring_static[kRing && !kDynRing ? kWarps * kRingWords : 1];
+    extern __shared__ __align__(16) unsigned char batch_dyn_smem[];
+    typename Pol::T* const ring = kDynRing ? reinterpret_cast<typename Pol::T*>(batch_dyn_smem) : ring_static;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     C(&wbuf)[1][36][kVars] = *reinterpret_cast<C(*)[1][36][kVars]>(&rbuf[wid]);
     for (;;) {

@@ -53,25 +53,49 @@ cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
 // The batch's feature set is common to its cases: positivity, and the edge
 // code when some case has a physical side or cell types (batches keep no RHS
 // and have no viscous terms).
+// Dynamic shared memory of a batched march (the FP64 ring), 0 for the others.
+template <class Pol, int kLoad>
+constexpr size_t batch_dyn_bytes() {
+    return (kLoad == 3 && sizeof(typename Pol::T) == 8) ? static_cast<size_t>(kBatchWarps) * kRingWords * 8 : 0;
+}
+
+template <class Kernel>
+cudaError_t allow_dyn(Kernel k, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
 template <class Pol, int kMinBlocks, int kLoad>
 cudaError_t launch_batch_march(const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s) {
+    constexpr size_t dyn = batch_dyn_bytes<Pol, kLoad>();
+    cudaError_t e = cudaSuccess;
+    switch (feat) {
+        case 0: e = allow_dyn(batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, 0>, dyn); break;
+        case kFeatPos: e = allow_dyn(batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatPos>, dyn); break;
+        case kFeatEdge: e = allow_dyn(batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge>, dyn); break;
+        case kFeatEdge | kFeatPos:
+            e = allow_dyn(batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge | kFeatPos>, dyn);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
     switch (feat) {
         case 0:
-            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, 0><<<grid, 32 * kBatchWarps, 0, s>>>(
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, 0><<<grid, 32 * kBatchWarps, dyn, s>>>(
                 args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatPos:
-            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatPos><<<grid, 32 * kBatchWarps, dyn, s>>>(
                 args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatEdge:
-            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge><<<grid, 32 * kBatchWarps, 0, s>>>(
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge><<<grid, 32 * kBatchWarps, dyn, s>>>(
                 args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         case kFeatEdge | kFeatPos:
-            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge | kFeatPos><<<grid, 32 * kBatchWarps, 0, s>>>(
+            batch_march_kernel<Pol, kBatchWarps, kMinBlocks, kLoad, kFeatEdge | kFeatPos><<<grid, 32 * kBatchWarps, dyn, s>>>(
                 args, item_case, item_local, case_rows, case_nseg, total, counter);
             break;
         default:
@@ -87,8 +111,8 @@ cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_ca
     if (p == kF32Mixed)
         return launch_batch_march<PolF32, kBatchMinBlocksF32, kBatchLoadF32>(args, item_case, item_local, case_rows,
                                                                              case_nseg, total, counter, grid, feat, s);
-    return launch_batch_march<PolF64, kBatchMinBlocksF64, 0>(args, item_case, item_local, case_rows, case_nseg,
-                                                             total, counter, grid, feat, s);
+    return launch_batch_march<PolF64, kBatchMinBlocksF64, kBatchLoadF64>(args, item_case, item_local, case_rows,
+                                                                         case_nseg, total, counter, grid, feat, s);
 }
 
 // Boundary-face fluxes of every case of a batch (cases without physical sides
@@ -112,8 +136,11 @@ int batch_blocks_per_sm(Prec p) {
             &n, batch_march_kernel<PolF32, kBatchWarps, kBatchMinBlocksF32, kBatchLoadF32, kFeatEdge | kFeatPos>,
             32 * kBatchWarps, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64, 0, kFeatEdge | kFeatPos>, 32 * kBatchWarps, 0);
+    {
+        constexpr size_t dyn = batch_dyn_bytes<PolF64, kBatchLoadF64>();
+        auto k = batch_march_kernel<PolF64, kBatchWarps, kBatchMinBlocksF64, kBatchLoadF64, kFeatEdge | kFeatPos>;
+        if (allow_dyn(k, dyn) == cudaSuccess) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * kBatchWarps, dyn);
+    }
     return n > 0 ? n : 1;
 }
 

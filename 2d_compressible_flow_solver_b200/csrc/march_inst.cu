@@ -17,7 +17,23 @@ template <class Pol, int R, int W, int B, int Ld, int F>
 cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     const int nseg = (a.L.ny + kSeg - 1) / kSeg;
     const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
-    march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, 0, s>>>(a);
+    size_t dyn = 0;
+    if constexpr (Ld == 3 && sizeof(typename Pol::T) == 8) {
+        // the FP64 ring lives in dynamic shared memory; allow it once per device
+        constexpr int kMaxDev = 64;
+        static bool allowed[kMaxDev] = {};
+        dyn = static_cast<size_t>(W) * kRingWords * sizeof(double);
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= kMaxDev || !allowed[dev]) {
+            e = cudaFuncSetAttribute(march_kernel<Pol, R, W, B, Ld, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(dyn));
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < kMaxDev) allowed[dev] = true;
+        }
+    }
+    march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(a);
     return cudaGetLastError();
 }
 
