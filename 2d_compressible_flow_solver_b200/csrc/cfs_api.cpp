@@ -31,6 +31,7 @@ struct cfs_ctx {
     int next_stage = 0;   // stage the RK sequence expects next
     double* rhs = nullptr;
     double* staging = nullptr;
+    double* sums = nullptr;  // plane sums of an uploaded state (FP32 storage offsets)
     void* rv = nullptr;   // viscous RHS [3][nx][ny] (Navier-Stokes form only)
     uint8_t* types_d = nullptr;
     uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
@@ -392,6 +393,10 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
     }
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(cfg->nx) * cfg->ny;
     if (cudaMalloc(&c->staging, hb) != cudaSuccess) { c->err = "device allocation of the staging buffer failed"; return bail(CFS_ERR_NOMEM); }
+    if (cudaMalloc(&c->sums, sizeof(double) * cfs::plane_sums_scratch_doubles()) != cudaSuccess) {
+        c->err = "device allocation of the sum scratch failed";
+        return bail(CFS_ERR_NOMEM);
+    }
     if (cfg->viscous == CFS_VISCOUS_NS) {
         const size_t vb = static_cast<size_t>(3) * cfg->nx * cfg->ny * c->L.elem_bytes;
         if (cudaMalloc(&c->rv, vb) != cudaSuccess) { c->err = "device allocation of the viscous RHS failed"; return bail(CFS_ERR_NOMEM); }
@@ -426,6 +431,7 @@ int cfs_destroy(cfs_ctx* c) {
     for (void* p : c->S) cudaFree(p);
     cudaFree(c->rhs);
     cudaFree(c->staging);
+    cudaFree(c->sums);
     cudaFree(c->rv);
     cudaFree(c->types_d);
     cudaFree(c->lowo_d);
@@ -448,24 +454,27 @@ int cfs_set_state(cfs_ctx* c, const double* U) {
     if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+    CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
     if (c->L.elem_bytes == 4) {
-        // FP32 storage offsets: the FP32-rounded mean of each variable.
+        // FP32 storage offsets: the FP32-rounded mean of each variable, summed
+        // on the device from the uploaded state (a fixed summation order)
         const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
+        double sums[kVars] = {0, 0, 0, 0};
+        if (!c->fixed_offsets) {
+            CFS_CUDA(c, cfs::launch_plane_sums(c->staging, static_cast<long long>(n), c->sums, c->stream));
+            CFS_CUDA(c, cudaMemcpyAsync(sums, c->sums + cfs::plane_sums_scratch_doubles() - kVars, sizeof(sums),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+        }
         bool changed = false;
         for (int v = 0; v < kVars; ++v) {
-            float off = c->fixed_off[v];
-            if (!c->fixed_offsets) {
-                double sum = 0.0;
-                for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
-                off = static_cast<float>(sum / static_cast<double>(n));
-            }
+            float off = c->fixed_offsets ? c->fixed_off[v] : static_cast<float>(sums[v] / static_cast<double>(n));
             if (!std::isfinite(off)) off = 0.0f;
             changed = changed || off != c->L.off[v];
             c->L.off[v] = off;
         }
         if (changed) release_graph(c);
     }
-    CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
     CFS_CUDA(c, cfs::launch_pack(c->L.elem_bytes, c->staging, c->S[0], c->L, c->stream));
     for (int b = 0; b < 3; ++b) CFS_CUDA(c, cfs::launch_ghost_fill(c->L.elem_bytes, c->S[b], c->L, c->sides, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -72,6 +72,7 @@ struct cfs_batch {
     int* case_nseg = nullptr;
     unsigned int* counters = nullptr;  // [parity][stage]
     double* staging = nullptr;
+    double* sums = nullptr;  // plane sums of an uploaded case state (FP32 storage offsets)
     int grid = 0;
     long long total_cells = 0;
     bool args_dirty = true;
@@ -224,6 +225,7 @@ int cfs_batch_destroy(cfs_batch* b) {
     cudaFree(b->case_nseg);
     cudaFree(b->counters);
     cudaFree(b->staging);
+    cudaFree(b->sums);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return CFS_OK;
@@ -389,7 +391,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         !dalloc(reinterpret_cast<void**>(&b->case_rows), sizeof(int) * ncases) ||
         !dalloc(reinterpret_cast<void**>(&b->case_nseg), sizeof(int) * ncases) ||
         !dalloc(reinterpret_cast<void**>(&b->counters), sizeof(unsigned int) * 6) ||
-        !dalloc(reinterpret_cast<void**>(&b->staging), sizeof(double) * kVars * max_cells))
+        !dalloc(reinterpret_cast<void**>(&b->staging), sizeof(double) * kVars * max_cells) ||
+        !dalloc(reinterpret_cast<void**>(&b->sums), sizeof(double) * cfs::plane_sums_scratch_doubles()))
         return bail(CFS_ERR_NOMEM, "batch device allocation failed");
     auto h2d = [&](void* dst, const void* src, size_t bytes) {
         return bytes == 0 || cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
@@ -440,17 +443,22 @@ int cfs_batch_set_state(cfs_batch* b, int ci, const double* U) {
     if (!b || !U || ci < 0 || ci >= b->n) return bfail(b, CFS_ERR_INVALID, "bad case or state");
     BatchCase& c = b->cases[ci];
     const size_t n = static_cast<size_t>(c.desc.nx) * c.desc.ny;
+    CFSB_CUDA(b, cudaMemcpyAsync(b->staging, U, sizeof(double) * kVars * n, cudaMemcpyHostToDevice, b->stream));
     if (b->elem == 4) {
+        // FP32 storage offsets: the FP32-rounded means, summed on the device as
+        // a single grid's (cfs_set_state) are
+        double sums[kVars];
+        CFSB_CUDA(b, cfs::launch_plane_sums(b->staging, static_cast<long long>(n), b->sums, b->stream));
+        CFSB_CUDA(b, cudaMemcpyAsync(sums, b->sums + cfs::plane_sums_scratch_doubles() - kVars, sizeof(sums),
+                                     cudaMemcpyDeviceToHost, b->stream));
+        CFSB_CUDA(b, cudaStreamSynchronize(b->stream));
         for (int v = 0; v < kVars; ++v) {
-            double sum = 0.0;
-            for (size_t k = 0; k < n; ++k) sum += U[v * n + k];
-            float off = static_cast<float>(sum / static_cast<double>(n));
+            float off = static_cast<float>(sums[v] / static_cast<double>(n));
             if (!std::isfinite(off)) off = 0.0f;
             if (off != c.L.off[v]) b->args_dirty = true;
             c.L.off[v] = off;
         }
     }
-    CFSB_CUDA(b, cudaMemcpyAsync(b->staging, U, sizeof(double) * kVars * n, cudaMemcpyHostToDevice, b->stream));
     CFSB_CUDA(b, cfs::launch_pack(b->elem, b->staging, state_buf(b, c, 0), c.L, b->stream));
     for (int k = 0; k < 3; ++k) CFSB_CUDA(b, cfs::launch_ghost_fill(b->elem, state_buf(b, c, k), c.L, c.sides, b->stream));
     CFSB_CUDA(b, cudaStreamSynchronize(b->stream));

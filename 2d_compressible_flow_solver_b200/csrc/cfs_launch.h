@@ -21,6 +21,10 @@ cudaError_t launch_wmax(int elem_bytes, const void* U, const Layout& L, const ui
                         double dy, unsigned long long* out, cudaStream_t s);
 // CFL maxima of every case of a batch: args[c].in into args[c].P->wmax[0].
 cudaError_t launch_batch_wmax(int elem_bytes, const StageArgs* args, int ncases, cudaStream_t s);
+// Sums of the four planes of a device FP64 state [4][n], deterministic; the 4
+// sums land at scratch[plane_sums_scratch_doubles() - 4 ..].
+int plane_sums_scratch_doubles();
+cudaError_t launch_plane_sums(const double* U, long long n, double* scratch, cudaStream_t s);
 cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
                           cudaStream_t s);
 cudaError_t launch_pack(int elem_bytes, const double* src, void* dst, const Layout& L, cudaStream_t s);

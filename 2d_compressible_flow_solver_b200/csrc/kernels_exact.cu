@@ -62,6 +62,43 @@ cudaError_t launch_batch_wmax(int elem_bytes, const StageArgs* args, int ncases,
     return cudaSuccess;
 }
 
+// Sums of the four planes of a host-order FP64 state [4][n], in a fixed order
+// (the same bits on every run): kSumBlocks strided partial sums per plane,
+// each reduced as a tree in its block, then the partials added in index order.
+constexpr int kSumBlocks = 256, kSumThreads = 256;
+
+__global__ void __launch_bounds__(kSumThreads) plane_partial_sums_kernel(const double* U, long long n, double* partial) {
+    __shared__ double red[kSumThreads];
+    const int v = blockIdx.y;
+    double s = 0.0;
+    for (long long k = static_cast<long long>(blockIdx.x) * kSumThreads + threadIdx.x; k < n;
+         k += static_cast<long long>(kSumBlocks) * kSumThreads)
+        s += U[v * n + k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+        if (static_cast<int>(threadIdx.x) < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[v * kSumBlocks + blockIdx.x] = red[0];
+}
+
+__global__ void plane_final_sums_kernel(const double* partial, double* out4) {
+    const int v = threadIdx.x;
+    if (v >= kVars) return;
+    double s = 0.0;
+    for (int b = 0; b < kSumBlocks; ++b) s += partial[v * kSumBlocks + b];
+    out4[v] = s;
+}
+
+int plane_sums_scratch_doubles() { return kVars * kSumBlocks + kVars; }
+
+cudaError_t launch_plane_sums(const double* U, long long n, double* scratch, cudaStream_t s) {
+    plane_partial_sums_kernel<<<dim3(kSumBlocks, kVars), kSumThreads, 0, s>>>(U, n, scratch);
+    plane_final_sums_kernel<<<1, 32, 0, s>>>(scratch, scratch + kVars * kSumBlocks);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
                           cudaStream_t s) {
     constexpr int nt = 256;
