@@ -51,6 +51,11 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 // (2d_compressible_flow_solver_b200/tuning.json).
 constexpr int kDefaultVariantF32 = 7;
 constexpr int kDefaultVariantF64 = 8;
+// FP64 ring blocks (4 warps, 70 KB dynamic + 4.6 KB static shared memory) per
+// SM, and the register-window variant the FP64 default falls back to when the
+// ring's last wave would run nearly empty (launch_stage_f64).
+constexpr int kRingBlocksPerSmF64 = 3;
+constexpr int kWindowVariantF64 = 4;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
 constexpr int kBatchWarps = 4;

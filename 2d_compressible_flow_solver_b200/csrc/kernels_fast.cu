@@ -18,10 +18,39 @@ cudaError_t launch_boundary_flux(const StageArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// SM count of the current device (cached per device).
+int sm_count() {
+    constexpr int kMaxDev = 64;
+    static int count[kMaxDev] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 148;
+    if (count[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        count[dev] = n > 0 ? n : 148;
+    }
+    return count[dev];
+}
+
+// The FP64 default variant stages rows in a 74 KB shared ring, 3 blocks per
+// SM.  When its grid fills more than one but fewer than three such waves and
+// the last one is under half full, the register-window variant, 4 blocks per
+// SM, finishes first (Mach-3 cylinder 2048 x 1024: 2,105 against 1,832
+// Mcell-steps/s; at 1024^2, 2048^2 and 4096^2 the ring is 8-20 % faster).
+int default_variant_f64(const Layout& L) {
+    const MarchVariant& d = kVariants[kDefaultVariantF64 - 1];
+    const long long nseg = (L.ny + kSeg - 1) / kSeg;
+    const long long blocks = ((nseg + d.warps - 1) / d.warps) * ((L.nx + d.rows - 1) / d.rows);
+    const double waves = static_cast<double>(blocks) / (static_cast<double>(sm_count()) * kRingBlocksPerSmF64);
+    if (waves > 1.0 && waves < 3.0 && waves - static_cast<double>(static_cast<long long>(waves)) < 0.5)
+        return kWindowVariantF64;
+    return kDefaultVariantF64;
+}
+
 cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
     const cudaError_t e = launch_boundary_flux<PolF64>(a, s);
     if (e != cudaSuccess) return e;
-    const int v = a.variant > 0 ? a.variant : kDefaultVariantF64;
+    const int v = a.variant > 0 ? a.variant : default_variant_f64(a.L);
     switch (march_features(a)) {
         case 0: return launch_march_f64_0(a, v, s);
         case 1: return launch_march_f64_1(a, v, s);
