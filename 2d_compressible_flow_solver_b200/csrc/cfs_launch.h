@@ -51,6 +51,11 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 // (2d_compressible_flow_solver_b200/tuning.json).
 constexpr int kDefaultVariantF32 = 7;
 constexpr int kDefaultVariantF64 = 8;
+// FP32 grids with edge code (physical sides, cell types) run the same ring
+// march with 128 registers and 4 blocks per SM: 2048^2 transmissive with floors
+// and a cylinder 5,672 against 5,476 Mcell-steps/s, the 2048 x 1024 Mach-3
+// cylinder 5,237 against 5,039.
+constexpr int kEdgeVariantF32 = 8;
 // FP64 ring blocks (4 warps, 70 KB dynamic + 4.6 KB static shared memory) per
 // SM, and the register-window variant the FP64 default falls back to when the
 // ring's last wave would run nearly empty (launch_stage_f64).
@@ -59,7 +64,7 @@ constexpr int kWindowVariantF64 = 4;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.
 constexpr int kBatchWarps = 4;
-constexpr int kBatchMinBlocksF32 = 5;
+constexpr int kBatchMinBlocksF32 = 4;
 constexpr int kBatchLoadF32 = 3;  // FP32 batches stage rows in the shared ring
 constexpr int kBatchMinBlocksF64 = 4;
 // FP64 batches march without the ring: its 70 KB of dynamic shared memory per

@@ -66,7 +66,7 @@ cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
 cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
     const cudaError_t e = launch_boundary_flux<PolF32>(a, s);
     if (e != cudaSuccess) return e;
-    const int v = a.variant > 0 ? a.variant : kDefaultVariantF32;
+    const int v = a.variant > 0 ? a.variant : (march_features(a) & kFeatEdge) ? kEdgeVariantF32 : kDefaultVariantF32;
     switch (march_features(a)) {
         case 0: return launch_march_f32_0(a, v, s);
         case 1: return launch_march_f32_1(a, v, s);
