@@ -533,11 +533,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
                 }
-                if (a.stage >= 1 && owner && q >= i0 && q < i1) {
+                if (a.stage >= 1 && q >= i0 && q < i1) {  // uniform: every lane fills its slot
                     T* du = ring_u0(q);
                     const T* u0p = static_cast<const T*>(a.u0);
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(du + lane * kVars + v, u0p + v * L.plane + off, true);
+                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(du + lane * kVars + v, u0p + v * L.plane + off, col_ok);
                 }
             }
             cp_async_commit();
