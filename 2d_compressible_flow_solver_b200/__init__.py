@@ -21,6 +21,7 @@ import numpy as np
 
 __all__ = [
     "LIB_PATH", "CfsConfig", "CfsCase", "CfsError", "Solver", "Batch", "load_library", "exported_symbols", "circle_setup",
+    "polygon_setup",
     "FP64", "FP32_MIXED", "FP64_EXACT", "RK_TVD2", "RK_TVD3_REFERENCE", "RK_SSP3",
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
@@ -112,6 +113,10 @@ _SIGNATURES = {
                                                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_int, _c_uint8_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                _c_int32_p, _c_int32_p, _c_double_p, _c_double_p]),
+    "cfs_ib_build_polygon": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, ctypes.c_int]),
+    "cfs_polygon_setup": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                         _c_double_p, _c_uint8_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                         _c_int32_p, _c_int32_p, _c_double_p, _c_double_p]),
     "cfs_get_ib": (ctypes.c_int, [ctypes.c_void_p, _c_uint8_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                   _c_int32_p, _c_int32_p, _c_double_p]),
     "cfs_ib_fill": (ctypes.c_int, [ctypes.c_void_p]),
@@ -220,6 +225,30 @@ def circle_setup(nx: int, ny: int, lx: float, ly: float, radius: float, cx: floa
     return types, cells, donors, images, normals
 
 
+def polygon_setup(nx: int, ny: int, lx: float, ly: float, xy):
+    """Host set-up of a closed polygon body (cfs_polygon_setup), vertices
+    xy[npoints, 2] in order: returns (types[nx, ny], cells[n], donors[n, 4],
+    images[n, 2], normals[n, 2])."""
+    lib = load_library()
+    v = np.ascontiguousarray(np.asarray(xy, dtype=np.float64).reshape(-1, 2))
+    types = np.empty((nx, ny), dtype=np.uint8)
+    n = ctypes.c_int(0)
+    args = (int(nx), int(ny), float(lx), float(ly), int(v.shape[0]), v.ctypes.data_as(_c_double_p))
+    rc = lib.cfs_polygon_setup(*args, types.ctypes.data_as(_c_uint8_p), 0, ctypes.byref(n), None, None, None, None)
+    if rc != 0:
+        raise CfsError(rc, lib.cfs_last_error(None).decode())
+    cells = np.empty(n.value, dtype=np.int32)
+    donors = np.empty((n.value, 4), dtype=np.int32)
+    images = np.empty((n.value, 2))
+    normals = np.empty((n.value, 2))
+    rc = lib.cfs_polygon_setup(*args, None, n.value, ctypes.byref(n), cells.ctypes.data_as(_c_int32_p),
+                               donors.ctypes.data_as(_c_int32_p), images.ctypes.data_as(_c_double_p),
+                               normals.ctypes.data_as(_c_double_p))
+    if rc != 0:
+        raise CfsError(rc, lib.cfs_last_error(None).decode())
+    return types, cells, donors, images, normals
+
+
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(_c_double_p)
 
@@ -318,6 +347,11 @@ class Solver:
         set-up on the GPU, cfs_ib_build_circle_device, the same result)."""
         fn = self._lib.cfs_ib_build_circle_device if on_device else self._lib.cfs_ib_build_circle
         self._check(fn(self._ctx, radius, cx, cy, int(npoints), int(mode)))
+
+    def build_polygon(self, xy, mode: int = IB_BILINEAR_SLIP) -> None:
+        """Closed polygon body (cfs_ib_build_polygon), vertices xy[npoints, 2] in order."""
+        v = np.ascontiguousarray(np.asarray(xy, dtype=np.float64).reshape(-1, 2))
+        self._check(self._lib.cfs_ib_build_polygon(self._ctx, int(v.shape[0]), v.ctypes.data_as(_c_double_p), int(mode)))
 
     def get_ib(self):
         """Returns (types[nx, ny], cells[n], donors[n, 4], images[n, 2])."""

@@ -604,6 +604,31 @@ int cfs_circle_setup(int nx, int ny, double lx, double ly, double radius, double
     return circle_setup_out(ib, types, max_n, n, cell, donor4, image_xy, normal_xy);
 }
 
+int cfs_ib_build_polygon(cfs_ctx* c, int npoints, const double* xy, int mode) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (npoints < 3 || !xy) return fail(c, CFS_ERR_INVALID, "a polygon needs at least 3 vertices");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_polygon(c->cfg.nx, c->cfg.ny, c->cfg.lx, c->cfg.ly,
+                            std::vector<double>(xy, xy + 2 * static_cast<size_t>(npoints)), ib, err))
+        return fail(c, CFS_ERR_INVALID, err);
+    const int rc = cfs_set_cell_types(c, ib.types.data());
+    if (rc != CFS_OK) return rc;
+    return cfs_set_ib(c, mode, static_cast<int>(ib.cell.size()), ib.cell.data(), ib.donor.data(), ib.image.data(),
+                      ib.normal.data());
+}
+
+int cfs_polygon_setup(int nx, int ny, double lx, double ly, int npoints, const double* xy, uint8_t* types, int max_n,
+                      int* n, int32_t* cell, int32_t* donor4, double* image_xy, double* normal_xy) {
+    if (nx < 1 || ny < 1 || !(lx > 0) || !(ly > 0)) return fail(nullptr, CFS_ERR_INVALID, "bad grid");
+    if (npoints < 3 || !xy) return fail(nullptr, CFS_ERR_INVALID, "a polygon needs at least 3 vertices");
+    cfs::IbList ib;
+    std::string err;
+    if (!cfs::build_polygon(nx, ny, lx, ly, std::vector<double>(xy, xy + 2 * static_cast<size_t>(npoints)), ib, err))
+        return fail(nullptr, CFS_ERR_INVALID, err);
+    return circle_setup_out(ib, types, max_n, n, cell, donor4, image_xy, normal_xy);
+}
+
 int cfs_circle_setup_device(int device, int nx, int ny, double lx, double ly, double radius, double cx, double cy,
                             int npoints, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4,
                             double* image_xy, double* normal_xy) {

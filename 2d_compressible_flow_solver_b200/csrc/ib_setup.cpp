@@ -88,6 +88,91 @@ bool select_donors(const uint8_t* t, int nx, int ny, double dx, double dy, const
     return true;
 }
 
+void mark_ghosts(std::vector<uint8_t>& t, int nx, int ny) {
+    // SetGhostcell(cells, 3) (Circle.cpp:53-103): from every fluid cell, walk
+    // each axis direction into solid/ghost cells and mark up to 3 as ghosts.
+    const int dirs[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+    auto at = [&](int i, int j) -> uint8_t& { return t[static_cast<size_t>(i) * ny + j]; };
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (at(i, j) != 0) continue;
+            for (const auto& d : dirs) {
+                const int ni = i + d[0], nj = j + d[1];
+                if (ni >= 0 && ni < nx && nj >= 0 && nj < ny && at(ni, nj) != 0) {
+                    for (int k = 1; k <= 3; ++k) {
+                        const int gi = i + k * d[0], gj = j + k * d[1];
+                        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny && at(gi, gj) != 0) at(gi, gj) = 2;
+                        else break;
+                    }
+                }
+            }
+        }
+}
+
+bool build_polygon(int nx, int ny, double lx, double ly, const std::vector<double>& xy, IbList& out,
+                   std::string& err) {
+    const int np = static_cast<int>(xy.size() / 2);
+    if (np < 3 || xy.size() != 2 * static_cast<size_t>(np)) {
+        err = "a polygon needs at least 3 vertices (x, y pairs)";
+        return false;
+    }
+    for (double v : xy)
+        if (!std::isfinite(v)) {
+            err = "polygon vertex not finite";
+            return false;
+        }
+    const double dx = lx / nx, dy = ly / ny;
+    auto centre = [&](int i, int j) { return P2{(i + 0.5) * dx, (j + 0.5) * dy}; };  // CartesianMesh.cpp:92
+    // solid iff the centre is inside (even-odd rule: crossings of a ray to +x)
+    std::vector<uint8_t>& t = out.types;
+    t.assign(static_cast<size_t>(nx) * ny, 0);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const P2 p = centre(i, j);
+            bool inside = false;
+            for (int k = 0, m = np - 1; k < np; m = k++) {
+                const double xk = xy[2 * k], yk = xy[2 * k + 1], xm = xy[2 * m], ym = xy[2 * m + 1];
+                if ((yk > p.y) != (ym > p.y) && p.x < (xm - xk) * (p.y - yk) / (ym - yk) + xk) inside = !inside;
+            }
+            if (inside) t[static_cast<size_t>(i) * ny + j] = 1;
+        }
+    mark_ghosts(t, nx, ny);
+    // image point: the mirror of the ghost centre in its nearest boundary
+    // point (projection onto each segment, clamped to it; the first segment
+    // wins ties)
+    out.cell.clear();
+    out.image.clear();
+    out.normal.clear();
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (t[static_cast<size_t>(i) * ny + j] != 2) continue;
+            const P2 pos = centre(i, j);
+            double best = std::numeric_limits<double>::max();
+            P2 q{pos.x, pos.y};
+            for (int k = 0; k < np; ++k) {
+                const int k1 = (k + 1) % np;
+                const P2 a{xy[2 * k], xy[2 * k + 1]}, b{xy[2 * k1], xy[2 * k1 + 1]};
+                const P2 ab{b.x - a.x, b.y - a.y};
+                const double len2 = ab.x * ab.x + ab.y * ab.y;
+                double u = len2 > 0.0 ? ((pos.x - a.x) * ab.x + (pos.y - a.y) * ab.y) / len2 : 0.0;
+                u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+                const P2 c{a.x + u * ab.x, a.y + u * ab.y};
+                const double dist = norm({c.x - pos.x, c.y - pos.y});
+                if (dist < best) {
+                    best = dist;
+                    q = c;
+                }
+            }
+            const P2 n = normalized({q.x - pos.x, q.y - pos.y});
+            out.cell.push_back(i * ny + j);
+            out.image.push_back(pos.x + 2 * (best * n.x));
+            out.image.push_back(pos.y + 2 * (best * n.y));
+            out.normal.push_back(n.x);
+            out.normal.push_back(n.y);
+        }
+    return select_donors(t.data(), nx, ny, dx, dy, out.cell, out.image, out.donor, err);
+}
+
 bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
                   IbList& out, std::string& err) {
     if (npoints < 3) {
@@ -108,24 +193,8 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
             if (norm({p.x - cx, p.y - cy}) <= radius) t[static_cast<size_t>(i) * ny + j] = 1;
         }
 
-    // SetGhostcell(cells, 3) (Circle.cpp:53-103): from every fluid cell, walk
-    // each axis direction into solid/ghost cells and mark up to 3 as ghosts.
-    const int dirs[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+    mark_ghosts(t, nx, ny);
     auto at = [&](int i, int j) -> uint8_t& { return t[static_cast<size_t>(i) * ny + j]; };
-    for (int i = 0; i < nx; ++i)
-        for (int j = 0; j < ny; ++j) {
-            if (at(i, j) != 0) continue;
-            for (const auto& d : dirs) {
-                const int ni = i + d[0], nj = j + d[1];
-                if (ni >= 0 && ni < nx && nj >= 0 && nj < ny && at(ni, nj) != 0) {
-                    for (int k = 1; k <= 3; ++k) {
-                        const int gi = i + k * d[0], gj = j + k * d[1];
-                        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny && at(gi, gj) != 0) at(gi, gj) = 2;
-                        else break;
-                    }
-                }
-            }
-        }
 
     out.cell.clear();
     out.image.clear();

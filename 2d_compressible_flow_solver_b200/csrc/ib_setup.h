@@ -29,6 +29,20 @@ bool build_circle(int nx, int ny, double lx, double ly, double radius, double cx
 bool build_circle_device(int nx, int ny, double lx, double ly, double radius, double cx, double cy, int npoints,
                          void* stream, IbList& out, std::string& err);
 
+// A closed polygon body (no counterpart in the reference, whose only
+// ImmersedBoundary shape is the circle): vertices xy[2*np] in order; a cell is
+// solid when its centre is inside (even-odd rule); ghosts are marked as for the
+// circle; a ghost's image point mirrors its centre in the nearest point of the
+// boundary (projection clamped to each segment, so non-convex shapes work);
+// donors as for the circle.
+bool build_polygon(int nx, int ny, double lx, double ly, const std::vector<double>& xy, IbList& out,
+                   std::string& err);
+
+// Ghost marking of SetGhostcell(cells, 3) (Circle.cpp:53-103) on types 0/1 in
+// place: from every fluid cell, up to 3 consecutive non-fluid cells along each
+// axis direction become ghosts (2).
+void mark_ghosts(std::vector<uint8_t>& types, int nx, int ny);
+
 // Pieces shared by both: the polygon of Circle::Initialize (Circle.cpp:12-41) as
 // vertex and unit-direction arrays [2*npoints]; and the 4 nearest fluid donors
 // of each image point (FindNearest4FluidCellsIndexed, Circle.cpp:160-215),

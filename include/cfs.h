@@ -203,6 +203,21 @@ int cfs_circle_setup_device(int device, int nx, int ny, double lx, double ly, do
                             int npoints, uint8_t* types, int max_n, int* n, int32_t* cell, int32_t* donor4,
                             double* image_xy, double* normal_xy);
 
+/* A closed polygon body (no counterpart in the reference, whose only
+ * ImmersedBoundary shape is the circle): npoints vertices xy[2*npoints] in
+ * order, either orientation, non-convex allowed.  A cell is solid when its
+ * centre is inside (even-odd rule); ghost cells are marked as SetGhostcell
+ * marks them (Circle.cpp:53-103); a ghost's image point mirrors its centre in
+ * the nearest point of the polygon's boundary; donors as for the circle
+ * (FindNearest4FluidCellsIndexed, Circle.cpp:160-215).  cfs_ib_build_polygon
+ * installs it in a context (types + cfs_set_ib with `mode`);
+ * cfs_polygon_setup returns the lists on the host as cfs_circle_setup does.
+ * CFS_ERR_INVALID for fewer than 3 vertices, non-finite vertices or a ghost
+ * with fewer than 4 fluid donors. */
+int cfs_ib_build_polygon(cfs_ctx* ctx, int npoints, const double* xy, int mode);
+int cfs_polygon_setup(int nx, int ny, double lx, double ly, int npoints, const double* xy, uint8_t* types, int max_n,
+                      int* n, int32_t* cell, int32_t* donor4, double* image_xy, double* normal_xy);
+
 /* Read-back of the immersed-boundary set-up: types[nx][ny], and for the first
  * min(n, max_n) immersed-ghost cells (i outer, j inner order) their cell
  * index, donors and image point.  *n receives the total count. */
