@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
             const long long off = L.offset(i, j);
             const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
             const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
-            const C rinv = C(1) / rho;
+            const C rinv = rcp_fast(rho);
             u = mx * rinv;
             v = my * rinv;
             const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);

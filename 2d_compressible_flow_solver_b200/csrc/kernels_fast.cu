@@ -175,18 +175,22 @@ int batch_blocks_per_sm(Prec p) {
 
 constexpr int kViscTI = 8;
 constexpr int kViscTJ = 32;
+// FP32 tiles twice as tall: the 3-cell halo of the primitive, gradient and
+// face phases is recomputed on fewer cells (37.5 KB of static shared memory;
+// the FP64 tile would not fit in 48 KB)
+constexpr int kViscTI32 = 16;
 
-inline dim3 visc_grid(const Layout& L) {
-    return dim3((L.ny + kViscTJ - 1) / kViscTJ, (L.nx + kViscTI - 1) / kViscTI);
+inline dim3 visc_grid(const Layout& L, int ti) {
+    return dim3((L.ny + kViscTJ - 1) / kViscTJ, (L.nx + ti - 1) / ti);
 }
 
 cudaError_t launch_viscous_f64(const ViscArgs& a, cudaStream_t s) {
-    viscous_kernel<PolF64, kViscTI, kViscTJ><<<visc_grid(a.L), kViscTI * kViscTJ, 0, s>>>(a);
+    viscous_kernel<PolF64, kViscTI, kViscTJ><<<visc_grid(a.L, kViscTI), kViscTI * kViscTJ, 0, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_viscous_f32(const ViscArgs& a, cudaStream_t s) {
-    viscous_kernel<PolF32, kViscTI, kViscTJ><<<visc_grid(a.L), kViscTI * kViscTJ, 0, s>>>(a);
+    viscous_kernel<PolF32, kViscTI32, kViscTJ><<<visc_grid(a.L, kViscTI32), kViscTI32 * kViscTJ, 0, s>>>(a);
     return cudaGetLastError();
 }
 
