@@ -56,10 +56,11 @@ constexpr int kDefaultVariantF64 = 8;
 // and a cylinder 5,672 against 5,476 Mcell-steps/s, the 2048 x 1024 Mach-3
 // cylinder 5,237 against 5,039.
 constexpr int kEdgeVariantF32 = 8;
-// FP64 ring blocks (4 warps, 70 KB dynamic + 4.6 KB static shared memory) per
-// SM, and the register-window variant the FP64 default falls back to when the
-// ring's last wave would run nearly empty (launch_stage_f64).
-constexpr int kRingBlocksPerSmF64 = 3;
+// FP64 ring blocks per SM (4 warps at 128 registers; 37 KB dynamic + 4.6 KB
+// static shared memory), and the register-window variant the FP64 default
+// falls back to when the ring's last wave would run nearly empty
+// (launch_stage_f64).
+constexpr int kRingBlocksPerSmF64 = 4;
 constexpr int kWindowVariantF64 = 4;
 
 // Batched forms (cfs_batch_*): one launch covers every case of a batch.

@@ -225,12 +225,18 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Ring of staged rows of the FP32 row march (load schedule 3), per warp: kRingRows
+// Ring of staged rows of the row march (load schedule 3), per warp: kRingRows
 // rows of its 36 columns (the segment and 2 halo columns each side), stored
-// values, and the same rows of U^0 for its 32 lanes.
+// values, and (FP32 storage) the same rows of U^0 for its 32 lanes.  The FP64
+// ring leaves U^0 out (each lane loads it early in the row's iteration): its
+// rows of doubles would otherwise cost a fourth block per SM.
 constexpr int kRingRows = 8, kRingDist = 2;
 constexpr int kRingRowWords = 36 * kVars, kRingU0Words = 32 * kVars;
 constexpr int kRingWords = kRingRows * (kRingRowWords + kRingU0Words);
+template <class T>
+__host__ __device__ constexpr int ring_words() {
+    return sizeof(T) == 4 ? kRingWords : kRingRows * kRingRowWords;
+}
 
 // One column's 4 variables to / from the shared row buffer in vector accesses.
 template <class C>
@@ -510,9 +516,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         }
     };
 
-    // Load schedule 3: this warp's ring (rows and U^0 rows, see kRingWords).
-    T* const rw = kRing ? ring + wid * kRingWords : nullptr;
-    T* const ru0 = kRing ? rw + kRingRows * kRingRowWords : nullptr;
+    // Load schedule 3: this warp's ring (rows, and U^0 rows in FP32; ring_words).
+    constexpr bool kU0Ring = kRing && sizeof(T) == 4;
+    T* const rw = kRing ? ring + wid * ring_words<T>() : nullptr;
+    T* const ru0 = kU0Ring ? rw + kRingRows * kRingRowWords : nullptr;
     auto ring_row = [&](int q) -> T* { return rw + (q & (kRingRows - 1)) * kRingRowWords; };
     auto ring_u0 = [&](int q) -> T* { return ru0 + (q & (kRingRows - 1)) * kRingU0Words; };
     // Issue the copies of row q (the lane's column; halo lanes also their
@@ -533,7 +540,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
                 }
-                if (a.stage >= 1 && q >= i0 && q < i1) {  // uniform: every lane fills its slot
+                if (kU0Ring && a.stage >= 1 && q >= i0 && q < i1) {  // uniform: every lane fills its slot
                     T* du = ring_u0(q);
                     const T* u0p = static_cast<const T*>(a.u0);
 #pragma unroll
@@ -572,6 +579,13 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     for (int r = i0 - 1; active_warp && r <= i1; ++r) {
         const unsigned int f_r = f_next;
         f_next = load_flags(r + 1);
+        if constexpr (kRing && !kU0Ring) {  // FP64 ring: U^0 of row r-1, ahead of the x reconstruction
+            if (a.stage >= 1 && owner && r - 1 >= i0) {
+                const long long off = L.offset(r - 1, j);
+#pragma unroll
+                for (int v = 0; v < kVars; ++v) pf_u0[v] = static_cast<const T*>(a.u0)[v * L.plane + off];
+            }
+        }
         if constexpr (kExtra) {  // viscous RHS of row r, a whole iteration ahead of its update
 #pragma unroll
             for (int q = 0; q < 3; ++q) rv_cur[q] = rv_pf[q];
@@ -628,11 +642,12 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             if (i >= i0 && owner) {
                 if constexpr (kRing) {
                     const T* cs = ring_row(i) + (lane + 2) * kVars;
-                    const T* us = ring_u0(i) + lane * kVars;
 #pragma unroll
-                    for (int v = 0; v < kVars; ++v) {
-                        pf_cur[v] = cs[v];
-                        pf_u0[v] = a.stage >= 1 ? us[v] : T(0);
+                    for (int v = 0; v < kVars; ++v) pf_cur[v] = cs[v];
+                    if constexpr (kU0Ring) {
+                        const T* us = ring_u0(i) + lane * kVars;
+#pragma unroll
+                        for (int v = 0; v < kVars; ++v) pf_u0[v] = a.stage >= 1 ? us[v] : T(0);
                     }
                 } else if constexpr (kL == 0) {
                     load_update(i);
@@ -801,8 +816,8 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const St
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring, threadIdx.x >> 5);
     } else if constexpr (kLoad == 3) {
-        // FP64 ring: kWarps * kRingWords doubles (69.6 KB for 4 warps), above the
-        // 48 KB of static shared memory: dynamic, sized at launch
+        // FP64 ring: kWarps * ring_words<double>() doubles (36.9 KB for 4
+        // warps); dynamic shared memory, sized at launch
         extern __shared__ __align__(16) unsigned char march_dyn_smem[];
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf,
                                               reinterpret_cast<typename Pol::T*>(march_dyn_smem), threadIdx.x >> 5);
@@ -839,7 +854,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
         const int c = unit_case[w], lu = unit_local[w];
         const int ns = case_nseg[c];
         const StageArgs a = args[c];
-        march_item<Pol, 1, kLoad, kFeat>(a, lu % ns, lu / ns, case_rows[c], wbuf, kRing ? ring + wid * kRingWords : nullptr, 0);
+        march_item<Pol, 1, kLoad, kFeat>(a, lu % ns, lu / ns, case_rows[c], wbuf, kRing ? ring + wid * ring_words<typename Pol::T>() : nullptr, 0);
     }
 }
 

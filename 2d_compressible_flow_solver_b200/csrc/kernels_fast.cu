@@ -32,11 +32,12 @@ int sm_count() {
     return count[dev];
 }
 
-// The FP64 default variant stages rows in a 74 KB shared ring, 3 blocks per
-// SM.  When its grid fills more than one but fewer than three such waves and
-// the last one is under half full, the register-window variant, 4 blocks per
-// SM, finishes first (Mach-3 cylinder 2048 x 1024: 2,105 against 1,832
-// Mcell-steps/s; at 1024^2, 2048^2 and 4096^2 the ring is 8-20 % faster).
+// The FP64 default variant stages rows in a shared ring, kRingBlocksPerSmF64
+// blocks per SM.  When its grid fills more than one but fewer than three such
+// waves and the last one is under half full, the register-window variant
+// finishes first (measured with the earlier 3-block ring on the Mach-3
+// cylinder, 2048 x 1024: 2,105 against 1,832 Mcell-steps/s; the 4-block ring
+// now fills that grid in one wave and runs it at 2,376).
 int default_variant_f64(const Layout& L) {
     const MarchVariant& d = kVariants[kDefaultVariantF64 - 1];
     const long long nseg = (L.ny + kSeg - 1) / kSeg;
@@ -85,7 +86,7 @@ cudaError_t launch_stage_f32(const StageArgs& a, cudaStream_t s) {
 // Dynamic shared memory of a batched march (the FP64 ring), 0 for the others.
 template <class Pol, int kLoad>
 constexpr size_t batch_dyn_bytes() {
-    return (kLoad == 3 && sizeof(typename Pol::T) == 8) ? static_cast<size_t>(kBatchWarps) * kRingWords * 8 : 0;
+    return (kLoad == 3 && sizeof(typename Pol::T) == 8) ? static_cast<size_t>(kBatchWarps) * ring_words<double>() * 8 : 0;
 }
 
 template <class Kernel>

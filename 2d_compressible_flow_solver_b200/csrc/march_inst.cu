@@ -22,7 +22,7 @@ cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
         // the FP64 ring lives in dynamic shared memory; allow it once per device
         constexpr int kMaxDev = 64;
         static bool allowed[kMaxDev] = {};
-        dyn = static_cast<size_t>(W) * kRingWords * sizeof(double);
+        dyn = static_cast<size_t>(W) * ring_words<double>() * sizeof(double);
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
