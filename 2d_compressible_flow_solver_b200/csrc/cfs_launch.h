@@ -70,10 +70,10 @@ constexpr int kBatchWarps = 4;
 constexpr int kBatchMinBlocksF32 = 4;
 constexpr int kBatchLoadF32 = 3;  // FP32 batches stage rows in the shared ring
 constexpr int kBatchMinBlocksF64 = 4;
-// FP64 batches march without the ring: its 70 KB of dynamic shared memory per
-// block leaves 3 blocks per SM, and the uneven 512-case batch ran 6 % slower
-// with it (2,775 against 2,938 Mcell-steps/s).
-constexpr int kBatchLoadF64 = 0;
+// FP64 batches stage rows in the ring too (dynamic shared memory, 4 blocks per
+// SM): the uneven 512-case batch 3,230 against 2,938 Mcell-steps/s without it
+// (the earlier ring that also held U^0 rows allowed 3 blocks and lost, 2,775).
+constexpr int kBatchLoadF64 = 3;
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s);  // feat: kFeatPos | kFeatEdge bits
