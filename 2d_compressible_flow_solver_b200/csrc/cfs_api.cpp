@@ -38,6 +38,10 @@ struct cfs_ctx {
     uint8_t* cflags_d = nullptr;  // [nx+2][ny+2] per-cell flags of the row march (with cell types)
     void* bflux = nullptr;        // boundary-face fluxes of the row march (physical sides)
     unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
+    // CFL maximum of the current state from the last stage of the last advance
+    // (FP64 bits), reused by the next advance while nothing changed the state
+    bool wmax_carry = false;
+    unsigned long long wmax_bits = 0;
     bool fixed_offsets = false;   // FP32 storage offsets set by cfs_set_storage_offsets
     float fixed_off[4] = {0, 0, 0, 0};
     bool has_types = false;
@@ -231,6 +235,7 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
 }
 
 int run_stage(cfs_ctx* c, int stage, double dt) {
+    if (c) c->wmax_carry = false;
     if (stage > 0 && stage != c->next_stage)
         return fail(c, CFS_ERR_STATE, "stage " + std::to_string(stage) + " requested but the RK sequence expects stage " +
                                           std::to_string(c->next_stage));
@@ -452,6 +457,7 @@ int cfs_destroy(cfs_ctx* c) {
 
 int cfs_set_state(cfs_ctx* c, const double* U) {
     if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
+    c->wmax_carry = false;
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
     CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
@@ -512,6 +518,7 @@ int cfs_get_rhs(cfs_ctx* c, double* R) {
 
 int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
     if (!c || !types) return fail(c, CFS_ERR_INVALID, "null argument");
+    c->wmax_carry = false;
     const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
     for (size_t k = 0; k < n; ++k)
         if (types[k] > 2) return fail(c, CFS_ERR_INVALID, "cell type out of range at " + std::to_string(k));
@@ -535,6 +542,7 @@ int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
 int cfs_set_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* donor4, const double* image_xy,
                const double* normal_xy) {
     if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    c->wmax_carry = false;
     if (mode != CFS_IB_REFERENCE && mode != CFS_IB_BILINEAR_SLIP) return fail(c, CFS_ERR_INVALID, "unknown IB mode");
     if (n < 0 || (n > 0 && (!cell || !donor4 || !image_xy))) return fail(c, CFS_ERR_INVALID, "bad IB list");
     if (n > 0 && mode == CFS_IB_BILINEAR_SLIP && !normal_xy) return fail(c, CFS_ERR_INVALID, "slip mode needs wall normals");
@@ -669,6 +677,7 @@ int cfs_get_ib(cfs_ctx* c, uint8_t* types, int max_n, int* n, int32_t* cell, int
 
 int cfs_ib_fill(cfs_ctx* c) {
     if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    c->wmax_carry = false;
     if (c->ib_n == 0) return CFS_OK;
     CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[c->cur]), c->stream));
     return CFS_OK;
@@ -721,8 +730,13 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     hp.cfl = cfl;
     hp.dt_fixed = dt;
     hp.seed[0] = hp.seed[1] = c->steps_done;
+    // first step's CFL maximum: carried from the previous advance's last stage
+    // while the state is unchanged (so that K calls of one step take the steps
+    // one call of K steps takes), else reduced now
+    const bool carry = hp.use_cfl && c->wmax_carry;
+    if (carry) hp.wmax[0] = c->wmax_bits;
     CFS_CUDA(c, cudaMemcpyAsync(c->P, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
-    if (hp.use_cfl) {
+    if (hp.use_cfl && !carry) {
         if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[0]), c->stream));
         CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[0], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
                                      c->dx, c->dy, reinterpret_cast<unsigned long long*>(c->P), c->stream));
@@ -769,8 +783,15 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     if (t_elapsed) *t_elapsed = out.t;
     if (dt_last) *dt_last = out.dt_last;
     c->steps_done += static_cast<unsigned int>(nsteps);
+    if (nsteps > 0) c->wmax_carry = false;
     if (nsteps > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
         return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
+    if (nsteps > 0 && hp.use_cfl) {
+        // the last step (parity 1 after an even count, 0 after an odd one)
+        // left the maximum of the final state in wmax[1 - parity]
+        c->wmax_bits = out.wmax[nsteps % 2 == 1 ? 1 : 0];
+        c->wmax_carry = c->wmax_bits != 0;
+    }
     return CFS_OK;
 }
 
@@ -805,6 +826,7 @@ int cfs_halo_pack(cfs_ctx* c, int side, void* dst) {
 
 int cfs_halo_unpack(cfs_ctx* c, int side, const void* src) {
     if (!c || !src || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo unpack arguments");
+    c->wmax_carry = false;
     const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
     const int first = side == 0 ? -cfs::kGhost : c->cfg.nx;
     for (int v = 0; v < kVars; ++v) {

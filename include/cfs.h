@@ -248,8 +248,11 @@ int cfs_step(cfs_ctx* ctx, double dt);
 /* nsteps full RK steps, the stage launches replayed from a CUDA graph.
  * cfl > 0: dt of every step comes from the CFL reduction of the step's
  * initial state, computed on the device inside the previous step's last stage
- * (no host round trip); cfl <= 0: fixed dt.  *t_elapsed (optional) receives
- * the simulated time advanced, *dt_last the last dt. */
+ * (no host round trip) -- also across calls, while nothing but cfs_advance has
+ * touched the state since (so K calls of one step take the steps one call of
+ * K steps takes); otherwise the first step's reduction runs at the call's
+ * start.  cfl <= 0: fixed dt.  *t_elapsed (optional) receives the simulated
+ * time advanced, *dt_last the last dt. */
 int cfs_advance(cfs_ctx* ctx, int nsteps, double cfl, double dt, double* t_elapsed, double* dt_last);
 
 /* Halo exchange of a slab decomposition along x (the reference's process
