@@ -571,9 +571,21 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
 // interpolated with zeta_r[1] (FourthOrderCS.h:38-42); stresses
 // sigma_11 = mu (4/3 u_x - 2/3 v_y), sigma_12 = mu (u_y + v_x), heat flux
 // kT T_x with kT = mu / ((gamma-1) Ma^2 Pr).
-__constant__ double kThetaR1[6] = {-3.0 / 640, 25.0 / 384, -75.0 / 64, 75.0 / 64, -25.0 / 384, 3.0 / 640};
-__constant__ double kThetaC[5] = {1.0 / 12, -8.0 / 12, 0.0, 8.0 / 12, -1.0 / 12};
-__constant__ double kZeta1[4] = {-1.0 / 16, 9.0 / 16, 9.0 / 16, -1.0 / 16};
+// (Functions of a constant table rather than __constant__ arrays: with the
+// loops unrolled every coefficient becomes an immediate, where an array read
+// costs a constant-bank load and, in FP32, a conversion per use.)
+__device__ __forceinline__ double theta_r1(int k) {
+    constexpr double t[6] = {-3.0 / 640, 25.0 / 384, -75.0 / 64, 75.0 / 64, -25.0 / 384, 3.0 / 640};
+    return t[k];
+}
+__device__ __forceinline__ double theta_c(int m) {
+    constexpr double t[5] = {1.0 / 12, -8.0 / 12, 0.0, 8.0 / 12, -1.0 / 12};
+    return t[m];
+}
+__device__ __forceinline__ double zeta1(int k) {
+    constexpr double t[4] = {-1.0 / 16, 9.0 / 16, 9.0 / 16, -1.0 / 16};
+    return t[k];
+}
 
 template <class Pol, int TI, int TJ>
 __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
@@ -617,7 +629,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         const int rr = rem / TJ, c = rem - rr * TJ;
         C s = C(0);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) s += C(kThetaC[m]) * sP[q][rr + 1][c + 1 + m];
+        for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][rr + 1][c + 1 + m];
         sGY[q][rr][c] = s * idy;
     }
     for (int e = t; e < 3 * TI * (TJ + 4); e += NT) {
@@ -625,7 +637,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         const int r = rem / (TJ + 4), cc = rem - r * (TJ + 4);
         C s = C(0);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) s += C(kThetaC[m]) * sP[q][r + 1 + m][cc + 1];
+        for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][r + 1 + m][cc + 1];
         sGX[q][r][cc] = s * idx;
     }
     __syncthreads();
@@ -637,17 +649,17 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         for (int q = 0; q < 3; ++q) {
             C s = C(0), x = C(0);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += C(kThetaR1[k]) * sP[q][fi + k][fj + kGhost];
+            for (int k = 0; k < 6; ++k) s += C(theta_r1(k)) * sP[q][fi + k][fj + kGhost];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) x += C(kZeta1[k]) * sGY[q][fi + k][fj];
+            for (int k = 0; k < 4; ++k) x += C(zeta1(k)) * sGY[q][fi + k][fj];
             dn[q] = s * idx;
             cr[q] = x;
         }
         C uf = C(0), vf = C(0);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            uf += C(kZeta1[k]) * sP[0][fi + 1 + k][fj + kGhost];
-            vf += C(kZeta1[k]) * sP[1][fi + 1 + k][fj + kGhost];
+            uf += C(zeta1(k)) * sP[0][fi + 1 + k][fj + kGhost];
+            vf += C(zeta1(k)) * sP[1][fi + 1 + k][fj + kGhost];
         }
         const C s11 = mu * (c43 * dn[0] - c23 * cr[1]);
         const C s12 = mu * (cr[0] + dn[1]);
@@ -662,17 +674,17 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         for (int q = 0; q < 3; ++q) {
             C s = C(0), x = C(0);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += C(kThetaR1[k]) * sP[q][fi + kGhost][fj + k];
+            for (int k = 0; k < 6; ++k) s += C(theta_r1(k)) * sP[q][fi + kGhost][fj + k];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) x += C(kZeta1[k]) * sGX[q][fi][fj + k];
+            for (int k = 0; k < 4; ++k) x += C(zeta1(k)) * sGX[q][fi][fj + k];
             dn[q] = s * idy;
             cr[q] = x;
         }
         C uf = C(0), vf = C(0);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            uf += C(kZeta1[k]) * sP[0][fi + kGhost][fj + 1 + k];
-            vf += C(kZeta1[k]) * sP[1][fi + kGhost][fj + 1 + k];
+            uf += C(zeta1(k)) * sP[0][fi + kGhost][fj + 1 + k];
+            vf += C(zeta1(k)) * sP[1][fi + kGhost][fj + 1 + k];
         }
         const C s22 = mu * (c43 * dn[1] - c23 * cr[0]);
         const C s21 = mu * (dn[0] + cr[1]);
