@@ -591,7 +591,6 @@ template <class Pol, int TI, int TJ>
 __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     using T = typename Pol::T;
     using C = typename Pol::C;
-    constexpr int NT = TI * TJ;
     constexpr int HI = TI + 2 * kGhost, HJ = TJ + 2 * kGhost;
     __shared__ C sP[3][HI][HJ];
     __shared__ C sGY[3][TI + 4][TJ];
@@ -602,48 +601,53 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const T* in = static_cast<const T*>(a.in);
     const int t = threadIdx.x;
-    const C g = C(a.gamma), gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
-    for (int e = t; e < HI * HJ; e += NT) {
-        const int r = e / HJ, c = e - r * HJ;
-        const int i = i0 - kGhost + r, j = j0 - kGhost + c;
-        C u = C(0), v = C(0), Tt = C(0);
-        if (i < L.nx + kGhost && j < L.ny + kGhost) {
-            const long long off = L.offset(i, j);
-            const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
-            const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
-            const C rinv = rcp_fast(rho);
-            u = mx * rinv;
-            v = my * rinv;
-            const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);
-            Tt = cT * p * rinv;
+    const C gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
+    // threads as a TI x TJ grid (TJ = 32: one warp per row): every phase walks
+    // rows by warp and columns by lane, with no index divisions
+    static_assert(TJ == 32, "one warp per tile row");
+    const int ty = t / TJ, tx = t - ty * TJ;
+    for (int r = ty; r < HI; r += TI)
+        for (int c = tx; c < HJ; c += TJ) {
+            const int i = i0 - kGhost + r, j = j0 - kGhost + c;
+            C u = C(0), v = C(0), Tt = C(0);
+            if (i < L.nx + kGhost && j < L.ny + kGhost) {
+                const long long off = L.offset(i, j);
+                const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
+                const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
+                const C rinv = rcp_fast(rho);
+                u = mx * rinv;
+                v = my * rinv;
+                const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);
+                Tt = cT * p * rinv;
+            }
+            sP[0][r][c] = u;
+            sP[1][r][c] = v;
+            sP[2][r][c] = Tt;
         }
-        sP[0][r][c] = u;
-        sP[1][r][c] = v;
-        sP[2][r][c] = Tt;
-    }
-    (void)g;
     __syncthreads();
     const C idx = C(1.0 / a.dx), idy = C(1.0 / a.dy);
-    for (int e = t; e < 3 * (TI + 4) * TJ; e += NT) {
-        const int q = e / ((TI + 4) * TJ), rem = e - q * (TI + 4) * TJ;
-        const int rr = rem / TJ, c = rem - rr * TJ;
-        C s = C(0);
+    for (int rr = ty; rr < TI + 4; rr += TI) {  // y-derivatives of rows i0-2 .. i0+TI+1
 #pragma unroll
-        for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][rr + 1][c + 1 + m];
-        sGY[q][rr][c] = s * idy;
+        for (int q = 0; q < 3; ++q) {
+            C s = C(0);
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][rr + 1][tx + 1 + m];
+            sGY[q][rr][tx] = s * idy;
+        }
     }
-    for (int e = t; e < 3 * TI * (TJ + 4); e += NT) {
-        const int q = e / (TI * (TJ + 4)), rem = e - q * TI * (TJ + 4);
-        const int r = rem / (TJ + 4), cc = rem - r * (TJ + 4);
-        C s = C(0);
+    for (int cc = tx; cc < TJ + 4; cc += TJ) {  // x-derivatives of columns j0-2 .. j0+TJ+1
 #pragma unroll
-        for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][r + 1 + m][cc + 1];
-        sGX[q][r][cc] = s * idx;
+        for (int q = 0; q < 3; ++q) {
+            C s = C(0);
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][ty + 1 + m][cc + 1];
+            sGX[q][ty][cc] = s * idx;
+        }
     }
     __syncthreads();
     const C mu = C(a.mu), kT = C(a.kT), c43 = C(4.0 / 3.0), c23 = C(2.0 / 3.0);
-    for (int f = t; f < (TI + 1) * TJ; f += NT) {  // x-normal faces between rows i0+fi-1 and i0+fi
-        const int fi = f / TJ, fj = f - fi * TJ;
+    for (int fi = ty; fi < TI + 1; fi += TI) {  // x-normal faces between rows i0+fi-1 and i0+fi
+        const int fj = tx;
         C dn[3], cr[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -667,8 +671,8 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         sFV[1][fi][fj] = s12;
         sFV[2][fi][fj] = uf * s11 + vf * s12 + kT * dn[2];
     }
-    for (int f = t; f < TI * (TJ + 1); f += NT) {  // y-normal faces between columns j0+fj-1 and j0+fj
-        const int fi = f / (TJ + 1), fj = f - fi * (TJ + 1);
+    for (int fj = tx; fj < TJ + 1; fj += TJ) {  // y-normal faces between columns j0+fj-1 and j0+fj
+        const int fi = ty;
         C dn[3], cr[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
