@@ -40,7 +40,7 @@ cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const doub
 struct MarchVariant {
     int rows, warps, min_blocks;
     int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead,
-               // 3 rows staged in shared memory by cp.async (FP32 form; FP64 runs 0)
+               // 3 rows staged in shared memory by cp.async
 };
 constexpr int kNumVariants = 10;
 constexpr MarchVariant kVariants[kNumVariants] = {

@@ -383,12 +383,13 @@ __global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArg
 //     the y work that precede their use;
 //   2 ahead: the next row two iterations ahead, the halo columns one row ahead,
 //     the RK operands before the x reconstruction;
-//   3 (FP32 form; the FP64 form uses 0) staged: every row of the segment (with
-//     its halo columns) and of U^0 is copied asynchronously (cp.async) into a
-//     per-warp shared ring `ring` kRingDist rows ahead of its use; the x and y
-//     stencils, the stored value and U^0 of the update are read from the ring,
-//     so no row window is held in registers and load latency overlaps rows of
-//     arithmetic.
+//   3 staged: every row of the segment (with its halo columns) and, in the
+//     FP32 form, of U^0 is copied asynchronously (cp.async) into a per-warp
+//     shared ring `ring` kRingDist rows ahead of its use; the x and y stencils,
+//     the stored value and (FP32) U^0 of the update are read from the ring, so
+//     no row window is held in registers and load latency overlaps rows of
+//     arithmetic (the FP64 form loads U^0 early in the row's iteration and
+//     keeps its ring in dynamic shared memory).
 //
 // The row loop holds no rarely taken code of any size: physical boundary faces
 // read the fluxes of boundary_flux_kernel and cell types and low-order faces

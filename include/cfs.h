@@ -129,8 +129,7 @@ typedef struct cfs_ctx cfs_ctx;
  * variant v (1-based): rows marched per warp, warps per block, minimum resident
  * blocks per SM requested from the compiler, and the row march's load schedule
  * (0: loads at their use; 1: issued early in each row's iteration; 2: two rows
- * ahead; 3: rows staged in shared memory by asynchronous copies, FP32-mixed
- * only -- the FP64 form runs schedule 0).
+ * ahead; 3: rows staged in shared memory by asynchronous copies).
  * Returns CFS_ERR_INVALID for an unknown v. */
 int cfs_variant_count(void);
 int cfs_variant_info(int v, int* rows, int* warps, int* min_blocks, int* prefetch);
