@@ -14,6 +14,12 @@ Arms:
   --impl reference   the reference's own CPU implementation (oracle/_ref, built
                      with the reference Makefile's optimisation flags) on all host
                      cores, on bounded samples of the same workload.
+  --workload batch   the uneven 512-case batch (persistent batched engine, FP32
+                     and FP64) against a loop of plain FP64 solvers.
+  --workload report  FP32-vs-FP64 accuracy, drift and rates on the quadrant,
+                     Mach-3 cylinder, Navier-Stokes shear-layer and batch
+                     configurations, and the circle set-up on host and device.
+  --workload modes   the row march's feature sets on one 2048^2 grid.
 
 Multi-GPU (torchrun, one rank per GPU, NCCL): one periodic grid of
 (4096 N) x 4096 cells on [0, N] x [0, 1] split into N slabs of 4096^2 along x
