@@ -67,6 +67,19 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// Device buffer of one call, freed on every return path (cudaFree waits for
+// the device, so a copy still queued on an error path ends first).
+struct DeviceScratch {
+    void* p = nullptr;
+    DeviceScratch() = default;
+    DeviceScratch(const DeviceScratch&) = delete;
+    DeviceScratch& operator=(const DeviceScratch&) = delete;
+    ~DeviceScratch() { cudaFree(p); }
+    cudaError_t alloc(size_t bytes) { return cudaMalloc(&p, bytes); }
+    template <class T>
+    T* get() const { return static_cast<T*>(p); }
+};
+
 int fail(cfs_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     else g_create_error = msg;
@@ -851,18 +864,17 @@ int cfs_conserved_totals(cfs_ctx* c, double totals[4]) {
 int cfs_weno5_faces(cfs_ctx* c, int n, const double* st, double* left, double* right) {
     if (!c || n < 0 || (n > 0 && (!st || !left || !right))) return fail(c, CFS_ERR_INVALID, "bad argument");
     if (n == 0) return CFS_OK;
-    double *d_st = nullptr, *d_l = nullptr, *d_r = nullptr;
-    CFS_CUDA(c, cudaMalloc(&d_st, sizeof(double) * 24 * n));
-    CFS_CUDA(c, cudaMalloc(&d_l, sizeof(double) * 5 * n));
-    CFS_CUDA(c, cudaMalloc(&d_r, sizeof(double) * 5 * n));
-    cudaMemcpyAsync(d_st, st, sizeof(double) * 24 * n, cudaMemcpyHostToDevice, c->stream);
-    cudaError_t e = cfs::launch_weno_faces(c->prec, n, d_st, d_l, d_r, c->cfg.gamma, c->cfg.weno_eps, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(left, d_l, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(right, d_r, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
+    DeviceScratch d_st, d_l, d_r;
+    cudaError_t e = d_st.alloc(sizeof(double) * 24 * n);
+    if (e == cudaSuccess) e = d_l.alloc(sizeof(double) * 5 * n);
+    if (e == cudaSuccess) e = d_r.alloc(sizeof(double) * 5 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_st.p, st, sizeof(double) * 24 * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cfs::launch_weno_faces(c->prec, n, d_st.get<double>(), d_l.get<double>(), d_r.get<double>(), c->cfg.gamma,
+                                   c->cfg.weno_eps, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(left, d_l.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(right, d_r.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(d_st);
-    cudaFree(d_l);
-    cudaFree(d_r);
     if (e != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("weno5 faces: ") + cudaGetErrorString(e));
     return CFS_OK;
 }
@@ -870,18 +882,17 @@ int cfs_weno5_faces(cfs_ctx* c, int n, const double* st, double* left, double* r
 int cfs_hll_faces(cfs_ctx* c, int n, int dir, const double* L, const double* R, double* F) {
     if (!c || n < 0 || (dir != 0 && dir != 1) || (n > 0 && (!L || !R || !F))) return fail(c, CFS_ERR_INVALID, "bad argument");
     if (n == 0) return CFS_OK;
-    double *d_l = nullptr, *d_r = nullptr, *d_f = nullptr;
-    CFS_CUDA(c, cudaMalloc(&d_l, sizeof(double) * 4 * n));
-    CFS_CUDA(c, cudaMalloc(&d_r, sizeof(double) * 4 * n));
-    CFS_CUDA(c, cudaMalloc(&d_f, sizeof(double) * 4 * n));
-    cudaMemcpyAsync(d_l, L, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
-    cudaMemcpyAsync(d_r, R, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
-    cudaError_t e = cfs::launch_hll_faces(c->prec, n, dir, d_l, d_r, d_f, c->cfg.gamma, c->cfg.hll, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(F, d_f, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    DeviceScratch d_l, d_r, d_f;
+    cudaError_t e = d_l.alloc(sizeof(double) * 4 * n);
+    if (e == cudaSuccess) e = d_r.alloc(sizeof(double) * 4 * n);
+    if (e == cudaSuccess) e = d_f.alloc(sizeof(double) * 4 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_l.p, L, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_r.p, R, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cfs::launch_hll_faces(c->prec, n, dir, d_l.get<double>(), d_r.get<double>(), d_f.get<double>(), c->cfg.gamma,
+                                  c->cfg.hll, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F, d_f.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(d_l);
-    cudaFree(d_r);
-    cudaFree(d_f);
     if (e != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("hll faces: ") + cudaGetErrorString(e));
     return CFS_OK;
 }
