@@ -602,28 +602,32 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     const T* in = static_cast<const T*>(a.in);
     const int t = threadIdx.x;
     const C gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
-    // threads as a TI x TJ grid (TJ = 32: one warp per row): every phase walks
-    // rows by warp and columns by lane, with no index divisions
+    // threads as a TI x TJ grid (TJ = 32: one warp per row).  Phases with TJ
+    // items per row walk rows by warp and columns by lane; the others (halo
+    // tile, x-derivatives, y-normal faces: TJ + 6, TJ + 4, TJ + 1 per row)
+    // number their items row by row over all threads (division by a constant),
+    // so that no warp makes a second pass for the few items past TJ
     static_assert(TJ == 32, "one warp per tile row");
+    constexpr int NT = TI * TJ;
     const int ty = t / TJ, tx = t - ty * TJ;
-    for (int r = ty; r < HI; r += TI)
-        for (int c = tx; c < HJ; c += TJ) {
-            const int i = i0 - kGhost + r, j = j0 - kGhost + c;
-            C u = C(0), v = C(0), Tt = C(0);
-            if (i < L.nx + kGhost && j < L.ny + kGhost) {
-                const long long off = L.offset(i, j);
-                const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
-                const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
-                const C rinv = rcp_fast(rho);
-                u = mx * rinv;
-                v = my * rinv;
-                const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);
-                Tt = cT * p * rinv;
-            }
-            sP[0][r][c] = u;
-            sP[1][r][c] = v;
-            sP[2][r][c] = Tt;
+    for (int e = t; e < HI * HJ; e += NT) {
+        const int r = e / HJ, c = e - r * HJ;
+        const int i = i0 - kGhost + r, j = j0 - kGhost + c;
+        C u = C(0), v = C(0), Tt = C(0);
+        if (i < L.nx + kGhost && j < L.ny + kGhost) {
+            const long long off = L.offset(i, j);
+            const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
+            const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
+            const C rinv = rcp_fast(rho);
+            u = mx * rinv;
+            v = my * rinv;
+            const C p = gm1 * (E - C(0.5) * (mx * mx + my * my) * rinv);
+            Tt = cT * p * rinv;
         }
+        sP[0][r][c] = u;
+        sP[1][r][c] = v;
+        sP[2][r][c] = Tt;
+    }
     __syncthreads();
     const C idx = C(1.0 / a.dx), idy = C(1.0 / a.dy);
     for (int rr = ty; rr < TI + 4; rr += TI) {  // y-derivatives of rows i0-2 .. i0+TI+1
@@ -635,13 +639,14 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
             sGY[q][rr][tx] = s * idy;
         }
     }
-    for (int cc = tx; cc < TJ + 4; cc += TJ) {  // x-derivatives of columns j0-2 .. j0+TJ+1
+    for (int e = t; e < TI * (TJ + 4); e += NT) {  // x-derivatives of columns j0-2 .. j0+TJ+1
+        const int rr = e / (TJ + 4), cc = e - rr * (TJ + 4);
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             C s = C(0);
 #pragma unroll
-            for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][ty + 1 + m][cc + 1];
-            sGX[q][ty][cc] = s * idx;
+            for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][rr + 1 + m][cc + 1];
+            sGX[q][rr][cc] = s * idx;
         }
     }
     __syncthreads();
@@ -671,8 +676,8 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         sFV[1][fi][fj] = s12;
         sFV[2][fi][fj] = uf * s11 + vf * s12 + kT * dn[2];
     }
-    for (int fj = tx; fj < TJ + 1; fj += TJ) {  // y-normal faces between columns j0+fj-1 and j0+fj
-        const int fi = ty;
+    for (int e = t; e < TI * (TJ + 1); e += NT) {  // y-normal faces between columns j0+fj-1 and j0+fj
+        const int fi = e / (TJ + 1), fj = e - fi * (TJ + 1);
         C dn[3], cr[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
