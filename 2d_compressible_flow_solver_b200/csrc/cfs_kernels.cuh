@@ -602,11 +602,12 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     const T* in = static_cast<const T*>(a.in);
     const int t = threadIdx.x;
     const C gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
-    // threads as a TI x TJ grid (TJ = 32: one warp per row).  Phases with TJ
-    // items per row walk rows by warp and columns by lane; the others (halo
-    // tile, x-derivatives, y-normal faces: TJ + 6, TJ + 4, TJ + 1 per row)
-    // number their items row by row over all threads (division by a constant),
-    // so that no warp makes a second pass for the few items past TJ
+    // threads as a TI x TJ grid (TJ = 32: one warp per row).  Phases walk rows
+    // by warp and columns by lane; the x-derivatives and y-normal faces (TJ + 4
+    // and TJ + 1 per row) give their items past TJ to one short extra pass
+    // whose lanes lie a whole tile row apart (distinct shared-memory banks), and
+    // the halo tile (TJ + 6 per row, stored only) numbers its cells row by row
+    // over all threads, so that no warp makes a second pass for a few items
     static_assert(TJ == 32, "one warp per tile row");
     constexpr int NT = TI * TJ;
     const int ty = t / TJ, tx = t - ty * TJ;
@@ -639,8 +640,9 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
             sGY[q][rr][tx] = s * idy;
         }
     }
-    for (int e = t; e < TI * (TJ + 4); e += NT) {  // x-derivatives of columns j0-2 .. j0+TJ+1
-        const int rr = e / (TJ + 4), cc = e - rr * (TJ + 4);
+    for (int pass = 0; pass < 2; ++pass) {  // x-derivatives of columns j0-2 .. j0+TJ+1
+        if (pass == 1 && t >= 4 * TI) break;
+        const int rr = pass == 0 ? ty : t % TI, cc = pass == 0 ? tx : TJ + t / TI;
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             C s = C(0);
@@ -676,8 +678,9 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         sFV[1][fi][fj] = s12;
         sFV[2][fi][fj] = uf * s11 + vf * s12 + kT * dn[2];
     }
-    for (int e = t; e < TI * (TJ + 1); e += NT) {  // y-normal faces between columns j0+fj-1 and j0+fj
-        const int fi = e / (TJ + 1), fj = e - fi * (TJ + 1);
+    for (int pass = 0; pass < 2; ++pass) {  // y-normal faces between columns j0+fj-1 and j0+fj
+        if (pass == 1 && t >= TI) break;
+        const int fi = pass == 0 ? ty : t, fj = pass == 0 ? tx : TJ;
         C dn[3], cr[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
