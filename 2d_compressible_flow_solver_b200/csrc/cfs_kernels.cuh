@@ -640,43 +640,92 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
             sGY[q][rr][tx] = s * idy;
         }
     }
-    for (int pass = 0; pass < 2; ++pass) {  // x-derivatives of columns j0-2 .. j0+TJ+1
-        if (pass == 1 && t >= 4 * TI) break;
-        const int rr = pass == 0 ? ty : t % TI, cc = pass == 0 ? tx : TJ + t / TI;
+    // x-derivatives of columns j0-2 .. j0+TJ+1, rows rr and rr+1 per thread
+    // (four of their five stencil values shared): columns 0..TJ-1 by lane,
+    // the 4 past them in a tail whose lanes lie two tile rows apart; on the
+    // top warps, as the y-derivatives' second pass runs on the bottom ones
+    static_assert(TI % 2 == 0, "row pairs");
+    {
+        constexpr int kMain = (TI / 2) * TJ, kCount = kMain + 4 * (TI / 2);
+        constexpr int kFirst = NT - (kCount + 31) / 32 * 32;
+        static_assert(kFirst >= 0, "x-derivative pairs fit in one pass");
+        const int u = t - kFirst;
+        if (u >= 0 && u < kCount) {
+            const int pr = u < kMain ? u / TJ : (u - kMain) % (TI / 2);
+            const int cc = u < kMain ? u % TJ : TJ + (u - kMain) / (TI / 2);
+            const int rr = 2 * pr;
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            C s = C(0);
+            for (int q = 0; q < 3; ++q) {
+                C col[6];
 #pragma unroll
-            for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * sP[q][rr + 1 + m][cc + 1];
-            sGX[q][rr][cc] = s * idx;
+                for (int m = 0; m < 6; ++m) col[m] = sP[q][rr + 1 + m][cc + 1];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    C s = C(0);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) s += C(theta_c(m)) * col[h + m];
+                    sGX[q][rr + h][cc] = s * idx;
+                }
+            }
         }
     }
     __syncthreads();
     const C mu = C(a.mu), kT = C(a.kT), c43 = C(4.0 / 3.0), c23 = C(2.0 / 3.0);
-    for (int fi = ty; fi < TI + 1; fi += TI) {  // x-normal faces between rows i0+fi-1 and i0+fi
-        const int fj = tx;
-        C dn[3], cr[3];
+    // x-normal faces between rows i0+fi-1 and i0+fi, faces fi0 and fi0+1 of a
+    // column per thread (five of their six stencil values shared; TI + 1
+    // faces per column, so the last pair has one face); on the top warps, as
+    // the y-normal faces' tail runs on the bottom one
+    {
+        constexpr int kCount = (TI + 2) / 2 * TJ;
+        constexpr int kFirst = NT - kCount;
+        static_assert(kFirst >= 0, "x-face pairs fit in one pass");
+        const int u = t - kFirst;
+        if (u >= 0) {
+            const int fi0 = 2 * (u / TJ), fj = u % TJ;
+            const bool two = fi0 + 1 <= TI;
+            C dn[2][3], cr[2][3], uf[2] = {C(0), C(0)}, vf[2] = {C(0), C(0)};
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            C s = C(0), x = C(0);
+            for (int q = 0; q < 3; ++q) {
+                C col[7], gy[5];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += C(theta_r1(k)) * sP[q][fi + k][fj + kGhost];
+                for (int k = 0; k < 6; ++k) col[k] = sP[q][fi0 + k][fj + kGhost];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) x += C(zeta1(k)) * sGY[q][fi + k][fj];
-            dn[q] = s * idx;
-            cr[q] = x;
+                for (int k = 0; k < 4; ++k) gy[k] = sGY[q][fi0 + k][fj];
+                col[6] = C(0);
+                gy[4] = C(0);
+                if (two) {
+                    col[6] = sP[q][fi0 + 6][fj + kGhost];
+                    gy[4] = sGY[q][fi0 + 4][fj];
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    C s = C(0), x = C(0);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) s += C(theta_r1(k)) * col[h + k];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) x += C(zeta1(k)) * gy[h + k];
+                    dn[h][q] = s * idx;
+                    cr[h][q] = x;
+                    if (q < 2) {
+                        C w = C(0);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) w += C(zeta1(k)) * col[h + 1 + k];
+                        if (q == 0) uf[h] = w;
+                        else vf[h] = w;
+                    }
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h == 1 && !two) break;
+                const int fi = fi0 + h;
+                const C s11 = mu * (c43 * dn[h][0] - c23 * cr[h][1]);
+                const C s12 = mu * (cr[h][0] + dn[h][1]);
+                sFV[0][fi][fj] = s11;
+                sFV[1][fi][fj] = s12;
+                sFV[2][fi][fj] = uf[h] * s11 + vf[h] * s12 + kT * dn[h][2];
+            }
         }
-        C uf = C(0), vf = C(0);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            uf += C(zeta1(k)) * sP[0][fi + 1 + k][fj + kGhost];
-            vf += C(zeta1(k)) * sP[1][fi + 1 + k][fj + kGhost];
-        }
-        const C s11 = mu * (c43 * dn[0] - c23 * cr[1]);
-        const C s12 = mu * (cr[0] + dn[1]);
-        sFV[0][fi][fj] = s11;
-        sFV[1][fi][fj] = s12;
-        sFV[2][fi][fj] = uf * s11 + vf * s12 + kT * dn[2];
     }
     for (int pass = 0; pass < 2; ++pass) {  // y-normal faces between columns j0+fj-1 and j0+fj
         if (pass == 1 && t >= TI) break;
