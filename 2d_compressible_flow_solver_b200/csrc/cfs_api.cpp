@@ -223,6 +223,8 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
         va.gamma = c->cfg.gamma;
         va.dx = c->dx;
         va.dy = c->dy;
+        va.inv_dx = 1.0 / c->dx;
+        va.inv_dy = 1.0 / c->dy;
         va.mu = c->cfg.mu;
         va.mach2 = c->cfg.mach * c->cfg.mach;
         va.kT = c->cfg.mu / ((c->cfg.gamma - 1) * va.mach2 * c->cfg.prandtl);

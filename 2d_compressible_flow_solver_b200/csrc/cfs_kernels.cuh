@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         sP[2][r][c] = Tt;
     }
     __syncthreads();
-    const C idx = C(1.0 / a.dx), idy = C(1.0 / a.dy);
+    const C idx = C(a.inv_dx), idy = C(a.inv_dy);
     for (int rr = ty; rr < TI + 4; rr += TI) {  // y-derivatives of rows i0-2 .. i0+TI+1
 #pragma unroll
         for (int q = 0; q < 3; ++q) {

@@ -138,6 +138,7 @@ struct ViscArgs {
     void* rv;
     Layout L;
     double gamma, dx, dy, mu, kT, mach2;
+    double inv_dx, inv_dy;  // 1/dx, 1/dy (formed once on the host: a thread here covers about one cell)
 };
 
 struct IbArgs {
