@@ -17,8 +17,9 @@ def _rel_linf(a, b):
 
 @pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 2e-5)])
 @pytest.mark.parametrize("bc", [(2, 2, 2, 2), (0, 0, 1, 0)])
-def test_navier_stokes_step_matches_oracle(cfsb, workloads, prec, tol, bc):
-    nx, ny = 72, 64
+@pytest.mark.parametrize("shape", [(72, 64), (53, 45)])  # 53 x 45: partial tiles in both directions
+def test_navier_stokes_step_matches_oracle(cfsb, workloads, prec, tol, bc, shape):
+    nx, ny = shape
     mu = 2e-3
     if bc == (2, 2, 2, 2):
         U = workloads.shear_layer(max(nx, ny), seed=2).U0[:, :nx, :ny].copy()
