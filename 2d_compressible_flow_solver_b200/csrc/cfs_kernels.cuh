@@ -603,11 +603,12 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     const int t = threadIdx.x;
     const C gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
     // threads as a TI x TJ grid (TJ = 32: one warp per row).  Phases walk rows
-    // by warp and columns by lane; the x-derivatives and y-normal faces (TJ + 4
-    // and TJ + 1 per row) give their items past TJ to one short extra pass
-    // whose lanes lie a whole tile row apart (distinct shared-memory banks), and
-    // the halo tile (TJ + 6 per row, stored only) numbers its cells row by row
-    // over all threads, so that no warp makes a second pass for a few items
+    // by warp and columns by lane.  Items past column TJ (TJ + 4 x-derivatives
+    // and TJ + 1 y-normal faces per row) go to one short extra pass whose lanes
+    // lie whole tile rows apart (distinct shared-memory banks); x-derivatives
+    // and x-normal faces take two rows per thread; the halo tile (TJ + 6 per
+    // row, stored only) numbers its cells row by row over all threads.  So no
+    // warp makes a second pass for a few items.
     static_assert(TJ == 32, "one warp per tile row");
     constexpr int NT = TI * TJ;
     const int ty = t / TJ, tx = t - ty * TJ;
