@@ -228,6 +228,12 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
         va.mu = c->cfg.mu;
         va.mach2 = c->cfg.mach * c->cfg.mach;
         va.kT = c->cfg.mu / ((c->cfg.gamma - 1) * va.mach2 * c->cfg.prandtl);
+        va.gm1_f = static_cast<float>(va.gamma - 1);
+        va.cT_f = static_cast<float>(va.gamma * va.mach2);
+        va.mu_f = static_cast<float>(va.mu);
+        va.kT_f = static_cast<float>(va.kT);
+        va.inv_dx_f = static_cast<float>(va.inv_dx);
+        va.inv_dy_f = static_cast<float>(va.inv_dy);
         CFS_CUDA(c, cfs::launch_viscous(c->prec, va, c->stream));
     }
     cfs::StageArgs a = base_args(c);

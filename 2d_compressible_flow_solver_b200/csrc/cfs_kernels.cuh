@@ -601,7 +601,8 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
     const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const T* in = static_cast<const T*>(a.in);
     const int t = threadIdx.x;
-    const C gm1 = C(a.gamma - 1), cT = C(a.gamma * a.mach2);
+    constexpr bool kF = sizeof(C) == 4;  // FP32 form: constants rounded on the host
+    const C gm1 = kF ? C(a.gm1_f) : C(a.gamma - 1), cT = kF ? C(a.cT_f) : C(a.gamma * a.mach2);
     // threads as a TI x TJ grid (TJ = 32: one warp per row).  Phases walk rows
     // by warp and columns by lane.  Items past column TJ (TJ + 4 x-derivatives
     // and TJ + 1 y-normal faces per row) go to one short extra pass whose lanes
@@ -631,7 +632,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         sP[2][r][c] = Tt;
     }
     __syncthreads();
-    const C idx = C(a.inv_dx), idy = C(a.inv_dy);
+    const C idx = kF ? C(a.inv_dx_f) : C(a.inv_dx), idy = kF ? C(a.inv_dy_f) : C(a.inv_dy);
     for (int rr = ty; rr < TI + 4; rr += TI) {  // y-derivatives of rows i0-2 .. i0+TI+1
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -671,7 +672,7 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         }
     }
     __syncthreads();
-    const C mu = C(a.mu), kT = C(a.kT), c43 = C(4.0 / 3.0), c23 = C(2.0 / 3.0);
+    const C mu = kF ? C(a.mu_f) : C(a.mu), kT = kF ? C(a.kT_f) : C(a.kT), c43 = C(4.0 / 3.0), c23 = C(2.0 / 3.0);
     // x-normal faces between rows i0+fi-1 and i0+fi, faces fi0 and fi0+1 of a
     // column per thread (five of their six stencil values shared; TI + 1
     // faces per column, so the last pair has one face); on the top warps, as

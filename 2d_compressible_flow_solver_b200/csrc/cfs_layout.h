@@ -139,6 +139,9 @@ struct ViscArgs {
     Layout L;
     double gamma, dx, dy, mu, kT, mach2;
     double inv_dx, inv_dy;  // 1/dx, 1/dy (formed once on the host: a thread here covers about one cell)
+    // the FP32 form's constants, rounded once on the host: gamma - 1,
+    // gamma Ma^2, mu, kT, 1/dx, 1/dy
+    float gm1_f, cT_f, mu_f, kT_f, inv_dx_f, inv_dy_f;
 };
 
 struct IbArgs {
