@@ -80,9 +80,14 @@ struct DeviceScratch {
     T* get() const { return static_cast<T*>(p); }
 };
 
+// Every error reaches the caller through here.  A failed runtime call (an
+// allocation, a launch) also leaves its error as this thread's last CUDA
+// error; it is consumed here, so that the launch checks of later calls do
+// not report it again as their own.
 int fail(cfs_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     else g_create_error = msg;
+    (void)cudaGetLastError();
     return code;
 }
 
@@ -317,8 +322,12 @@ int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* d
 }  // namespace
 
 namespace cfs {
-// Error message of a context-free entry point, read by cfs_last_error(NULL).
-void record_global_error(const std::string& msg) { g_create_error = msg; }
+// Error message of a context-free entry point, read by cfs_last_error(NULL)
+// (the thread's last CUDA error consumed as in fail()).
+void record_global_error(const std::string& msg) {
+    g_create_error = msg;
+    (void)cudaGetLastError();
+}
 
 cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s) {
     if (p == kF64Exact) return launch_stage_exact(a, s);

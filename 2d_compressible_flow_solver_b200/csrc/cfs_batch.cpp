@@ -93,9 +93,11 @@ int bfail(cfs_batch* b, int code, const std::string& m);
 
 thread_local std::string g_batch_create_error;
 
+// As fail() of the single-grid API: consumes the thread's last CUDA error.
 int bfail(cfs_batch* b, int code, const std::string& m) {
     if (b) b->err = m;
     else g_batch_create_error = m;
+    (void)cudaGetLastError();
     return code;
 }
 
