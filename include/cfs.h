@@ -16,8 +16,9 @@
  * a failed cfs_create).  A failed call leaves no CUDA error pending on the
  * calling thread (a refused allocation does not fail the next call's launch
  * checks, on this context or another).  Calls on one context come from one
- * host thread; all work of a context is ordered on the context's CUDA stream.  There is no CPU
- * fallback: without a usable CUDA device cfs_create fails with CFS_ERR_CUDA.
+ * host thread; all work of a context is ordered on the context's CUDA stream.
+ * There is no CPU fallback: without a usable CUDA device cfs_create fails with
+ * CFS_ERR_CUDA.
  */
 #ifndef CFS_H
 #define CFS_H
