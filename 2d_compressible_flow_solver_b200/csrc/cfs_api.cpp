@@ -454,7 +454,10 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
     }
     cudaMemsetAsync(c->P, 0, sizeof(cfs::DevParams), c->stream);
     for (int b = 0; b < 3; ++b) cfs::launch_ghost_fill(c->L.elem_bytes, c->S[b], c->L, c->sides, c->stream);
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { c->err = std::string("initialisation failed: ") + cudaGetErrorString(cudaGetLastError()); return bail(CFS_ERR_CUDA); }
+    // the clears and ghost fills above are checked here, at enqueue and at completion
+    cudaError_t ie = cudaStreamSynchronize(c->stream);
+    if (ie == cudaSuccess) ie = cudaGetLastError();
+    if (ie != cudaSuccess) { c->err = std::string("initialisation failed: ") + cudaGetErrorString(ie); return bail(CFS_ERR_CUDA); }
     *out = c;
     return CFS_OK;
 }

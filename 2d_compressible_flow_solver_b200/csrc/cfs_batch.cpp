@@ -426,10 +426,12 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     bool flags = false;
     for (const BatchCase& c : b->cases) flags = flags || c.cflags_off >= 0;
     b->feat = (common->positivity ? cfs::kFeatPos : 0) | (b->any_bflux || flags ? cfs::kFeatEdge : 0);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, common->device);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, common->device) != cudaSuccess || sms <= 0)
+        return bail(CFS_ERR_CUDA, "SM count query failed");
     b->grid = sms * cfs::batch_blocks_per_sm(b->prec);
-    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(CFS_ERR_CUDA, "batch initialisation failed");
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+        return bail(CFS_ERR_CUDA, "batch initialisation failed");
     *out = b;
     return CFS_OK;
 }
