@@ -131,6 +131,8 @@ _SIGNATURES = {
     "cfs_halo_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_halo_unpack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_set_storage_offsets": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "cfs_get_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint), _c_double_p, _c_double_p]),
+    "cfs_set_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double]),
     "cfs_conserved_totals": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_compute_dt_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -144,6 +146,7 @@ _SIGNATURES = {
     "cfs_batch_get_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
     "cfs_batch_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          _c_double_p]),
+    "cfs_batch_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "cfs_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                       ctypes.POINTER(ctypes.c_int)]),
     "cfs_weno5_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
@@ -409,6 +412,24 @@ class Solver:
                 raise ValueError("need 4 offsets")
             self._check(self._lib.cfs_set_storage_offsets(self._ctx, _dp(a)))
 
+    def run_counters(self) -> dict:
+        """Counters a bit-exact resume needs (cfs_get_step): completed steps,
+        the carried CFL maximum (0 if none) and the FP32 storage offsets."""
+        step = ctypes.c_uint(0)
+        m = ctypes.c_double(0.0)
+        off = np.zeros(4)
+        self._check(self._lib.cfs_get_step(self._ctx, ctypes.byref(step), ctypes.byref(m), _dp(off)))
+        return {"step": int(step.value), "cfl_max": float(m.value), "offsets": [float(x) for x in off]}
+
+    def resume(self, U, counters: dict) -> None:
+        """Installs a state and the counters of run_counters(), so that the
+        following steps are those of the run the counters were taken from:
+        storage offsets (FP32-mixed), state, then step and CFL maximum."""
+        if self.config.precision == FP32_MIXED:
+            self.set_storage_offsets(counters["offsets"])
+        self.set_state(U)
+        self._check(self._lib.cfs_set_step(self._ctx, int(counters["step"]), float(counters["cfl_max"])))
+
     def halo_bytes(self) -> int:
         n = ctypes.c_longlong(0)
         self._check(self._lib.cfs_halo_bytes(self._ctx, ctypes.byref(n)))
@@ -500,6 +521,11 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+    @property
+    def stream(self) -> int:
+        """The batch's cudaStream_t as an integer handle."""
+        return int(self._lib.cfs_batch_get_stream(self._b) or 0)
 
     def info(self):
         cells = ctypes.c_longlong(0)

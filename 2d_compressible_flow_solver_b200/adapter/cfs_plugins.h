@@ -23,7 +23,7 @@
 // Errors: the reference has no error convention; a failing cfs_* call throws
 // std::runtime_error carrying cfs_last_error.
 //
-// Integration in Run.cpp (see INTEGRATION.md):
+// Integration in Run.cpp:
 //     auto gpu = std::make_shared<cfs_plugins::Session>(cfg, m_cellsLv1);
 //     gpu->set_circle(0.1, 0.5, 1.0, 400);          // the Circle of Run.cpp:48
 //     m_model = std::make_shared<cfs_plugins::GpuModel>();

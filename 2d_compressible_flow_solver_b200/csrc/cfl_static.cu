@@ -12,7 +12,11 @@
 // the process exits.
 //
 // Built with -fmad=false, like the context's reduction, so the per-cell wave
-// speed sum and hence dt are the same bits as cfs_compute_dt's.
+// speed sum and hence dt are the same bits as cfs_compute_dt's for a state
+// held by an FP64 or FP64_EXACT context (an FP32-mixed context reduces its
+// FP32-rounded, offset storage instead).  Every call copies dt to pageable
+// host memory and waits for the stream, so no call may be made on a stream
+// that is being captured into a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -23,7 +27,7 @@
 #include "cfs.h"
 
 namespace cfs {
-void record_global_error(const std::string& msg);  // cfs_api.cpp
+void record_global_error(int code, const std::string& msg);  // cfs_api.cpp
 }
 
 namespace {
@@ -74,7 +78,10 @@ __global__ void __launch_bounds__(kThreads) cfl_partial_kernel(const double* U, 
         const long long k = base + static_cast<long long>(c) * kThreads;
         if (k >= n) break;
         if (types && types[k] != 0) continue;
-        const double w = wave_sum_static(U[k], U[n + k], U[2 * n + k], U[3 * n + k], g, dx, dy);
+        // a non-finite sum (a blown-up cell) counts as +infinity: dt becomes 0
+        // and the call reports CFS_ERR_NUMERIC, as cfs_compute_dt does
+        double w = wave_sum_static(U[k], U[n + k], U[2 * n + k], U[3 * n + k], g, dx, dy);
+        if (!(w == w)) w = __longlong_as_double(0x7ff0000000000000LL);
         if (w > m) m = w;
     }
     m = block_max_static(m, red);
@@ -113,7 +120,7 @@ cudaError_t scratch_on_current_device(unsigned long long** out) {
 }
 
 int fail_static(int code, const std::string& msg) {
-    cfs::record_global_error(msg);
+    cfs::record_global_error(code, msg);
     return code;
 }
 
@@ -145,7 +152,7 @@ extern "C" int cfs_compute_dt_static(const double* U, const uint8_t* types, int 
     double m;
     std::memcpy(&m, &bits, sizeof(m));
     if (!(m > 0) || !std::isfinite(m))
-        return fail_static(CFS_ERR_NUMERIC, "cfs_compute_dt_static: no finite positive wave speed");
+        return fail_static(CFS_ERR_NUMERIC, "cfs_compute_dt_static: a fluid cell is non-finite or every wave speed is 0");
     *dt = cfl / m;
     return CFS_OK;
 }

@@ -82,12 +82,14 @@ struct DeviceScratch {
 
 // Every error reaches the caller through here.  A failed runtime call (an
 // allocation, a launch) also leaves its error as this thread's last CUDA
-// error; it is consumed here, so that the launch checks of later calls do
-// not report it again as their own.
+// error; on those paths (CFS_ERR_CUDA, CFS_ERR_NOMEM) it is consumed here, so
+// that the launch checks of later calls do not report it again as their own.
+// Argument and state errors made no CUDA call and leave any error pending
+// from other code on the thread untouched.
 int fail(cfs_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     else g_create_error = msg;
-    (void)cudaGetLastError();
+    if (code == CFS_ERR_CUDA || code == CFS_ERR_NOMEM) (void)cudaGetLastError();
     return code;
 }
 
@@ -261,7 +263,8 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
 }
 
 int run_stage(cfs_ctx* c, int stage, double dt) {
-    if (c) c->wmax_carry = false;
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    c->wmax_carry = false;
     if (stage > 0 && stage != c->next_stage)
         return fail(c, CFS_ERR_STATE, "stage " + std::to_string(stage) + " requested but the RK sequence expects stage " +
                                           std::to_string(c->next_stage));
@@ -281,6 +284,7 @@ int run_stage(cfs_ctx* c, int stage, double dt) {
 // cfs::slip_donors (the given donors serve as its fallback).
 int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* donor4, const double* image,
               const double* normal) {
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     release_graph(c);
     cudaFree(c->ib_cell);
     cudaFree(c->ib_donor);
@@ -323,10 +327,11 @@ int upload_ib(cfs_ctx* c, int mode, int n, const int32_t* cell, const int32_t* d
 
 namespace cfs {
 // Error message of a context-free entry point, read by cfs_last_error(NULL)
-// (the thread's last CUDA error consumed as in fail()).
-void record_global_error(const std::string& msg) {
+// (the thread's last CUDA error consumed as in fail(): on CUDA and allocation
+// failures only).
+void record_global_error(int code, const std::string& msg) {
     g_create_error = msg;
-    (void)cudaGetLastError();
+    if (code == CFS_ERR_CUDA || code == CFS_ERR_NOMEM) (void)cudaGetLastError();
 }
 
 cudaError_t launch_stage(Prec p, const StageArgs& a, cudaStream_t s) {
@@ -464,6 +469,7 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
 
 int cfs_destroy(cfs_ctx* c) {
     if (!c) return CFS_OK;
+    cudaSetDevice(c->cfg.device);  // best effort: the frees below belong to that device
     if (c->stream) cudaStreamSynchronize(c->stream);
     release_graph(c);
     for (void* p : c->S) cudaFree(p);
@@ -530,6 +536,30 @@ int cfs_set_storage_offsets(cfs_ctx* c, const double* off4) {
     return CFS_OK;
 }
 
+int cfs_get_step(cfs_ctx* c, unsigned int* step, double* cfl_max, double* off4) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (step) *step = c->steps_done;
+    if (cfl_max) {
+        double m = 0.0;
+        if (c->wmax_carry) std::memcpy(&m, &c->wmax_bits, sizeof(m));
+        *cfl_max = m;
+    }
+    if (off4)
+        for (int v = 0; v < kVars; ++v) off4[v] = static_cast<double>(c->L.off[v]);
+    return CFS_OK;
+}
+
+int cfs_set_step(cfs_ctx* c, unsigned int step, double cfl_max) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (!(cfl_max >= 0) || !std::isfinite(cfl_max)) return fail(c, CFS_ERR_INVALID, "cfl_max must be finite and >= 0");
+    if (c->next_stage != 0) return fail(c, CFS_ERR_STATE, "a step is in progress (stage sequence not at stage 0)");
+    c->steps_done = step;
+    c->wmax_carry = cfl_max > 0;
+    c->wmax_bits = 0;
+    if (c->wmax_carry) std::memcpy(&c->wmax_bits, &cfl_max, sizeof(cfl_max));
+    return CFS_OK;
+}
+
 int cfs_get_state(cfs_ctx* c, double* U) {
     if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
@@ -543,6 +573,7 @@ int cfs_get_state(cfs_ctx* c, double* U) {
 int cfs_get_rhs(cfs_ctx* c, double* R) {
     if (!c || !R) return fail(c, CFS_ERR_INVALID, "null argument");
     if (!c->cfg.keep_rhs) return fail(c, CFS_ERR_STATE, "context created without keep_rhs");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
     CFS_CUDA(c, cudaMemcpyAsync(R, c->rhs, hb, cudaMemcpyDeviceToHost, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -555,6 +586,7 @@ int cfs_set_cell_types(cfs_ctx* c, const uint8_t* types) {
     const size_t n = static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
     for (size_t k = 0; k < n; ++k)
         if (types[k] > 2) return fail(c, CFS_ERR_INVALID, "cell type out of range at " + std::to_string(k));
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     release_graph(c);
     if (!c->types_d) CFS_CUDA(c, cudaMalloc(&c->types_d, n));
     CFS_CUDA(c, cudaMemcpy(c->types_d, types, n, cudaMemcpyHostToDevice));
@@ -712,6 +744,7 @@ int cfs_ib_fill(cfs_ctx* c) {
     if (!c) return fail(c, CFS_ERR_INVALID, "null context");
     c->wmax_carry = false;
     if (c->ib_n == 0) return CFS_OK;
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[c->cur]), c->stream));
     return CFS_OK;
 }
@@ -719,6 +752,7 @@ int cfs_ib_fill(cfs_ctx* c) {
 int cfs_compute_dt(cfs_ctx* c, double cfl, double* dt) {
     if (!c || !dt) return fail(c, CFS_ERR_INVALID, "null argument");
     if (!(cfl > 0)) return fail(c, CFS_ERR_INVALID, "cfl must be positive");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     CFS_CUDA(c, cudaMemsetAsync(c->wmax, 0, sizeof(unsigned long long), c->stream));
     CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
                                  c->dx, c->dy, c->wmax, c->stream));
@@ -727,7 +761,8 @@ int cfs_compute_dt(cfs_ctx* c, double cfl, double* dt) {
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     double m;
     std::memcpy(&m, &bits, sizeof(m));
-    if (!(m > 0) || !std::isfinite(m)) return fail(c, CFS_ERR_NUMERIC, "CFL reduction found no finite positive wave speed");
+    if (!(m > 0) || !std::isfinite(m))
+        return fail(c, CFS_ERR_NUMERIC, "CFL reduction: a fluid cell is non-finite or every wave speed is 0");
     *dt = cfl / m;
     return CFS_OK;
 }
@@ -821,15 +856,18 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
         return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
     if (nsteps > 0 && hp.use_cfl) {
         // the last step (parity 1 after an even count, 0 after an odd one)
-        // left the maximum of the final state in wmax[1 - parity]
+        // left the maximum of the final state in wmax[1 - parity]; it is
+        // +infinity when a fluid cell of that state is non-finite
         c->wmax_bits = out.wmax[nsteps % 2 == 1 ? 1 : 0];
         c->wmax_carry = c->wmax_bits != 0;
+        if (c->wmax_bits == 0x7ff0000000000000ull) return fail(c, CFS_ERR_NUMERIC, "a fluid cell became non-finite");
     }
     return CFS_OK;
 }
 
 int cfs_synchronize(cfs_ctx* c) {
     if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     return CFS_OK;
 }
@@ -846,6 +884,7 @@ int cfs_halo_bytes(cfs_ctx* c, long long* bytes) {
 // 3 * pitch consecutive elements, so a message is 4 plain copies.
 int cfs_halo_pack(cfs_ctx* c, int side, void* dst) {
     if (!c || !dst || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo pack arguments");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
     const int first = side == 0 ? 0 : c->cfg.nx - cfs::kGhost;
     for (int v = 0; v < kVars; ++v) {
@@ -859,6 +898,7 @@ int cfs_halo_pack(cfs_ctx* c, int side, void* dst) {
 
 int cfs_halo_unpack(cfs_ctx* c, int side, const void* src) {
     if (!c || !src || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo unpack arguments");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     c->wmax_carry = false;
     const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
     const int first = side == 0 ? -cfs::kGhost : c->cfg.nx;
@@ -873,8 +913,9 @@ int cfs_halo_unpack(cfs_ctx* c, int side, const void* src) {
 
 int cfs_conserved_totals(cfs_ctx* c, double totals[4]) {
     if (!c || !totals) return fail(c, CFS_ERR_INVALID, "null argument");
-    CFS_CUDA(c, cudaMemsetAsync(c->totals, 0, 4 * sizeof(double), c->stream));
-    CFS_CUDA(c, cfs::launch_totals(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->totals, c->stream));
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    CFS_CUDA(c, cfs::launch_totals(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->sums,
+                                   c->totals, c->stream));
     CFS_CUDA(c, cudaMemcpyAsync(totals, c->totals, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int v = 0; v < 4; ++v) totals[v] *= c->dx * c->dy;
@@ -884,6 +925,7 @@ int cfs_conserved_totals(cfs_ctx* c, double totals[4]) {
 int cfs_weno5_faces(cfs_ctx* c, int n, const double* st, double* left, double* right) {
     if (!c || n < 0 || (n > 0 && (!st || !left || !right))) return fail(c, CFS_ERR_INVALID, "bad argument");
     if (n == 0) return CFS_OK;
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     DeviceScratch d_st, d_l, d_r;
     cudaError_t e = d_st.alloc(sizeof(double) * 24 * n);
     if (e == cudaSuccess) e = d_l.alloc(sizeof(double) * 5 * n);
@@ -902,6 +944,7 @@ int cfs_weno5_faces(cfs_ctx* c, int n, const double* st, double* left, double* r
 int cfs_hll_faces(cfs_ctx* c, int n, int dir, const double* L, const double* R, double* F) {
     if (!c || n < 0 || (dir != 0 && dir != 1) || (n > 0 && (!L || !R || !F))) return fail(c, CFS_ERR_INVALID, "bad argument");
     if (n == 0) return CFS_OK;
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     DeviceScratch d_l, d_r, d_f;
     cudaError_t e = d_l.alloc(sizeof(double) * 4 * n);
     if (e == cudaSuccess) e = d_r.alloc(sizeof(double) * 4 * n);

@@ -93,15 +93,19 @@ int bfail(cfs_batch* b, int code, const std::string& m);
 
 thread_local std::string g_batch_create_error;
 
-// As fail() of the single-grid API: consumes the thread's last CUDA error.
+// As fail() of the single-grid API: consumes the thread's last CUDA error on
+// CUDA and allocation failures (argument errors leave it alone).
 int bfail(cfs_batch* b, int code, const std::string& m) {
     if (b) b->err = m;
     else g_batch_create_error = m;
-    (void)cudaGetLastError();
+    if (code == CFS_ERR_CUDA || code == CFS_ERR_NOMEM) (void)cudaGetLastError();
     return code;
 }
 
 int stages_of(int rk) { return rk == CFS_RK_TVD2 ? 2 : 3; }
+
+// FP64 bit pattern of +infinity: the CFL maximum of a state with a non-finite fluid cell
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
 
 void* state_buf(const cfs_batch* b, const BatchCase& c, int k) {
     return b->arena + c.state_off + static_cast<size_t>(k) * static_cast<size_t>(c.L.plane) * kVars * b->elem;
@@ -205,6 +209,7 @@ const char* cfs_batch_last_error(const cfs_batch* b) { return b ? b->err.c_str()
 
 int cfs_batch_destroy(cfs_batch* b) {
     if (!b) return CFS_OK;
+    cudaSetDevice(b->common.device);  // best effort: the frees below belong to that device
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph2) cudaGraphExecDestroy(b->graph2);
     cudaFree(b->arena);
@@ -436,6 +441,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     return CFS_OK;
 }
 
+void* cfs_batch_get_stream(cfs_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
 int cfs_batch_info(const cfs_batch* b, long long* cells, int* items) {
     if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
     if (cells) *cells = b->total_cells;
@@ -445,6 +452,7 @@ int cfs_batch_info(const cfs_batch* b, long long* cells, int* items) {
 
 int cfs_batch_set_state(cfs_batch* b, int ci, const double* U) {
     if (!b || !U || ci < 0 || ci >= b->n) return bfail(b, CFS_ERR_INVALID, "bad case or state");
+    CFSB_CUDA(b, cudaSetDevice(b->common.device));
     BatchCase& c = b->cases[ci];
     const size_t n = static_cast<size_t>(c.desc.nx) * c.desc.ny;
     CFSB_CUDA(b, cudaMemcpyAsync(b->staging, U, sizeof(double) * kVars * n, cudaMemcpyHostToDevice, b->stream));
@@ -471,6 +479,7 @@ int cfs_batch_set_state(cfs_batch* b, int ci, const double* U) {
 
 int cfs_batch_get_state(cfs_batch* b, int ci, double* U) {
     if (!b || !U || ci < 0 || ci >= b->n) return bfail(b, CFS_ERR_INVALID, "bad case or state");
+    CFSB_CUDA(b, cudaSetDevice(b->common.device));
     const BatchCase& c = b->cases[ci];
     const size_t n = static_cast<size_t>(c.desc.nx) * c.desc.ny;
     CFSB_CUDA(b, cfs::launch_unpack(b->elem, state_buf(b, c, 0), b->staging, c.L, b->stream));
@@ -529,6 +538,10 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
         if (t) t[ci] = hp[ci].t;
         if (nsteps > 0 && (!(hp[ci].dt_last > 0) || !std::isfinite(hp[ci].dt_last)))
             return bfail(b, CFS_ERR_NUMERIC, "case " + std::to_string(ci) + ": time step became non-finite or non-positive");
+        // the final state's CFL maximum (left by the last stage) is +infinity
+        // when a fluid cell of it is non-finite
+        if (nsteps > 0 && cfl > 0 && hp[ci].wmax[nsteps % 2 == 1 ? 1 : 0] == kInfBits)
+            return bfail(b, CFS_ERR_NUMERIC, "case " + std::to_string(ci) + ": a fluid cell became non-finite");
     }
     return CFS_OK;
 }

@@ -359,6 +359,15 @@ __device__ __forceinline__ double wave_sum(double rho, double mx, double my, dou
     return (fabs(u) + a) / dx + (fabs(v) + a) / dy;
 }
 
+// A CFL maximum takes a non-finite wave-speed sum (a NaN from a negative
+// pressure or density, an infinity) as +infinity, so that one blown-up fluid
+// cell makes the maximum infinite and dt = cfl / max zero, which every caller
+// reports as CFS_ERR_NUMERIC (a plain `w > m` would skip NaN cells and keep
+// stepping on a finite dt).
+__device__ __forceinline__ double cfl_term(double w) {
+    return w == w ? w : __longlong_as_double(0x7ff0000000000000LL);
+}
+
 // The same wave-speed sum for the CFL maximum fused into the last stage of the
 // throughput forms: one reciprocal and one square root, in the form's
 // arithmetic type (inv_dx = 1/dx, inv_dy = 1/dy).
@@ -551,7 +560,7 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
         }
         store_cell4<T>(out, L, a.bc, i, j, sv);
         if (a.P && a.last_stage && a.P->use_cfl && fluid) {
-            const double w = wave_sum(nv[0], nv[1], nv[2], nv[3], a.gamma, a.dx, a.dy);
+            const double w = cfl_term(wave_sum(nv[0], nv[1], nv[2], nv[3], a.gamma, a.dx, a.dy));
             if (w > wloc) wloc = w;
         }
     }
@@ -864,8 +873,8 @@ __global__ void __launch_bounds__(NT) wmax_kernel(const T* U, const Layout L, co
         if (types && types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
         const long long off = L.offset(i, j);
-        const double w = wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1), dec<T>(U[2 * L.plane + off], L, 2),
-                                  dec<T>(U[3 * L.plane + off], L, 3), g, dx, dy);
+        const double w = cfl_term(wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1),
+                                           dec<T>(U[2 * L.plane + off], L, 2), dec<T>(U[3 * L.plane + off], L, 3), g, dx, dy));
         if (w > m) m = w;
     }
     m = block_max<NT>(m, red);
@@ -886,33 +895,39 @@ __global__ void __launch_bounds__(NT) batch_wmax_kernel(const StageArgs* __restr
         if (a.types && a.types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
         const long long off = L.offset(i, j);
-        const double w = wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1), dec<T>(U[2 * L.plane + off], L, 2),
-                                  dec<T>(U[3 * L.plane + off], L, 3), a.gamma, a.dx, a.dy);
+        const double w = cfl_term(wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1),
+                                           dec<T>(U[2 * L.plane + off], L, 2), dec<T>(U[3 * L.plane + off], L, 3), a.gamma,
+                                           a.dx, a.dy));
         if (w > m) m = w;
     }
     m = block_max<NT>(m, red);
     if (threadIdx.x == 0 && m > 0.0) atomicMax(&a.P->wmax[0], static_cast<unsigned long long>(__double_as_longlong(m)));
 }
 
-// Sums of rho, m_x, m_y, E over fluid cells (FP64 accumulation).
-template <class T, int NT>
-__global__ void __launch_bounds__(NT) totals_kernel(const T* U, const Layout L, const uint8_t* types, double* out) {
-    double s[kVars] = {0, 0, 0, 0};
+// Sums of rho, m_x, m_y, E over fluid cells (FP64 accumulation), in a fixed
+// order so that the totals are the same bits on every run: block b of plane
+// blockIdx.y sums the cells b, b + NB*NT, ... of each of its threads, reduces
+// them as a tree, and writes partial[v * NB + b]; plane_final_sums_kernel adds
+// the partials in index order.
+template <class T, int NT, int NB>
+__global__ void __launch_bounds__(NT) totals_partial_kernel(const T* U, const Layout L, const uint8_t* types,
+                                                            double* partial) {
+    __shared__ double red[NT];
+    const int v = blockIdx.y;
     const long long n = static_cast<long long>(L.nx) * L.ny;
-    for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
+    double s = 0.0;
+    for (long long k = static_cast<long long>(blockIdx.x) * NT + threadIdx.x; k < n; k += static_cast<long long>(NB) * NT) {
         if (types && types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
-        const long long off = L.offset(i, j);
-#pragma unroll
-        for (int v = 0; v < kVars; ++v) s[v] += dec<T>(U[v * L.plane + off], L, v);
+        s += dec<T>(U[v * L.plane + L.offset(i, j)], L, v);
     }
-#pragma unroll
-    for (int v = 0; v < kVars; ++v) {
-        double x = s[v];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&out[v], x);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = NT / 2; w > 0; w >>= 1) {
+        if (static_cast<int>(threadIdx.x) < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
     }
+    if (threadIdx.x == 0) partial[v * NB + blockIdx.x] = red[0];
 }
 
 // --------------------------------------------- layout conversion / ghosts

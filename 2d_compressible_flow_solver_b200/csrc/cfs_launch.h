@@ -25,8 +25,10 @@ cudaError_t launch_batch_wmax(int elem_bytes, const StageArgs* args, int ncases,
 // sums land at scratch[plane_sums_scratch_doubles() - 4 ..].
 int plane_sums_scratch_doubles();
 cudaError_t launch_plane_sums(const double* U, long long n, double* scratch, cudaStream_t s);
-cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
-                          cudaStream_t s);
+// Sums of the four planes over fluid cells, deterministic (fixed order);
+// scratch holds plane_sums_scratch_doubles() doubles, the 4 sums go to out.
+cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* scratch,
+                          double* out, cudaStream_t s);
 cudaError_t launch_pack(int elem_bytes, const double* src, void* dst, const Layout& L, cudaStream_t s);
 cudaError_t launch_unpack(int elem_bytes, const void* src, double* dst, const Layout& L, cudaStream_t s);
 cudaError_t launch_ghost_fill(int elem_bytes, void* U, const Layout& L, const BcSides& sides, cudaStream_t s);

@@ -720,8 +720,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                 }
                 store_cell4<T>(out, L, a.bc, i, j, sv);
                 if (do_cfl) {
-                    const C w = wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy));
-                    if (fluid && double(w) > wloc) wloc = double(w);
+                    const double w = cfl_term(double(wave_sum_fast<C>(nv[0], nv[1], nv[2], nv[3], C(g), C(inv_dx), C(inv_dy))));
+                    if (fluid && w > wloc) wloc = w;
                 }
             }
         }

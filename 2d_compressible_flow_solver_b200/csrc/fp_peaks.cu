@@ -14,7 +14,7 @@
 #include "cfs.h"
 
 namespace cfs {
-void record_global_error(const std::string& msg);  // cfs_api.cpp
+void record_global_error(int code, const std::string& msg);  // cfs_api.cpp
 }
 
 namespace {
@@ -87,11 +87,11 @@ float best_ms(F launch, cudaStream_t st) {
 
 extern "C" int cfs_fp_peaks(int device, double* fp32_tflops, double* fp32x2_tflops, double* fp64_tflops) {
     if (!fp32_tflops || !fp32x2_tflops || !fp64_tflops) {
-        cfs::record_global_error("cfs_fp_peaks: null output");
+        cfs::record_global_error(CFS_ERR_INVALID, "cfs_fp_peaks: null output");
         return CFS_ERR_INVALID;
     }
     if (cudaSetDevice(device) != cudaSuccess) {
-        cfs::record_global_error("cfs_fp_peaks: cudaSetDevice failed");
+        cfs::record_global_error(CFS_ERR_CUDA, "cfs_fp_peaks: cudaSetDevice failed");
         return CFS_ERR_CUDA;
     }
     int sms = 0;
@@ -99,13 +99,13 @@ extern "C" int cfs_fp_peaks(int device, double* fp32_tflops, double* fp32x2_tflo
     const int blocks = (sms > 0 ? sms : 148) * 8;
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
-        cfs::record_global_error("cfs_fp_peaks: stream creation failed");
+        cfs::record_global_error(CFS_ERR_CUDA, "cfs_fp_peaks: stream creation failed");
         return CFS_ERR_CUDA;
     }
     void* sink = nullptr;
     if (cudaMalloc(&sink, sizeof(double) * blocks * kThreads) != cudaSuccess) {
         cudaStreamDestroy(st);
-        cfs::record_global_error("cfs_fp_peaks: device allocation failed");
+        cfs::record_global_error(CFS_ERR_NOMEM, "cfs_fp_peaks: device allocation failed");
         return CFS_ERR_NOMEM;
     }
     const int it32 = 4096, it64 = 1024;
@@ -116,7 +116,7 @@ extern "C" int cfs_fp_peaks(int device, double* fp32_tflops, double* fp32x2_tflo
     cudaFree(sink);
     cudaStreamDestroy(st);
     if (m32 <= 0.0f || m2 <= 0.0f || m64 <= 0.0f) {
-        cfs::record_global_error("cfs_fp_peaks: a timing launch failed");
+        cfs::record_global_error(CFS_ERR_CUDA, "cfs_fp_peaks: a timing launch failed");
         return CFS_ERR_CUDA;
     }
     // 2 flops per FMA; FFMA2 carries two FMAs

@@ -99,12 +99,14 @@ cudaError_t launch_plane_sums(const double* U, long long n, double* scratch, cud
     return cudaGetLastError();
 }
 
-cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* out,
-                          cudaStream_t s) {
-    constexpr int nt = 256;
-    const int nb = flat_blocks(static_cast<long long>(L.nx) * L.ny, nt);
-    if (elem_bytes == 8) totals_kernel<double, nt><<<nb, nt, 0, s>>>(static_cast<const double*>(U), L, types, out);
-    else totals_kernel<float, nt><<<nb, nt, 0, s>>>(static_cast<const float*>(U), L, types, out);
+cudaError_t launch_totals(int elem_bytes, const void* U, const Layout& L, const uint8_t* types, double* scratch,
+                          double* out, cudaStream_t s) {
+    const dim3 grid(kSumBlocks, kVars);
+    if (elem_bytes == 8)
+        totals_partial_kernel<double, kSumThreads, kSumBlocks><<<grid, kSumThreads, 0, s>>>(static_cast<const double*>(U), L, types, scratch);
+    else
+        totals_partial_kernel<float, kSumThreads, kSumBlocks><<<grid, kSumThreads, 0, s>>>(static_cast<const float*>(U), L, types, scratch);
+    plane_final_sums_kernel<<<1, 32, 0, s>>>(scratch, out);
     return cudaGetLastError();
 }
 

@@ -1,5 +1,7 @@
 // Kernels of the throughput forms: FP64 with FMA contraction and the
 // FP32-mixed form.  Built with FMA contraction on (nvcc default).
+#include <atomic>
+
 #include "cfs_kernels.cuh"
 #include "cfs_launch.h"
 #include "cfs_march.cuh"
@@ -21,15 +23,17 @@ cudaError_t launch_boundary_flux(const StageArgs& a, cudaStream_t s) {
 // SM count of the current device (cached per device).
 int sm_count() {
     constexpr int kMaxDev = 64;
-    static int count[kMaxDev] = {};
+    static std::atomic<int> count[kMaxDev] = {};  // every writer stores the same value
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 148;
-    if (count[dev] == 0) {
+    int c = count[dev].load(std::memory_order_relaxed);
+    if (c == 0) {
         int n = 0;
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        count[dev] = n > 0 ? n : 148;
+        c = n > 0 ? n : 148;
+        count[dev].store(c, std::memory_order_relaxed);
     }
-    return count[dev];
+    return c;
 }
 
 // The FP64 default variant stages rows in a shared ring, kRingBlocksPerSmF64

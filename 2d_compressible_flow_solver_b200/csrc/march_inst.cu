@@ -2,6 +2,8 @@
 //   -DCFS_MARCH_POL=PolF32|PolF64  -DCFS_MARCH_FEAT=0..7  -DCFS_MARCH_FN=<launcher name>
 // (the build gives each pair its own object, so the 160 kernels compile in
 // parallel).  The launcher runs the variant `v` of kVariants (1-based).
+#include <mutex>
+
 #include "cfs_kernels.cuh"
 #include "cfs_launch.h"
 #include "cfs_march.cuh"
@@ -19,19 +21,27 @@ cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
     size_t dyn = 0;
     if constexpr (Ld == 3 && sizeof(typename Pol::T) == 8) {
-        // the FP64 ring lives in dynamic shared memory; allow it once per device
+        // the FP64 ring lives in dynamic shared memory; allow it once per
+        // device (std::call_once: host threads may make their first launches
+        // on one device at the same time)
         constexpr int kMaxDev = 64;
-        static bool allowed[kMaxDev] = {};
+        static std::once_flag once[kMaxDev];
+        static cudaError_t allow_err[kMaxDev];
         dyn = static_cast<size_t>(W) * ring_words<double>() * sizeof(double);
+        auto allow = [dyn] {
+            return cudaFuncSetAttribute(march_kernel<Pol, R, W, B, Ld, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(dyn));
+        };
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
-        if (dev < 0 || dev >= kMaxDev || !allowed[dev]) {
-            e = cudaFuncSetAttribute(march_kernel<Pol, R, W, B, Ld, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(dyn));
-            if (e != cudaSuccess) return e;
-            if (dev >= 0 && dev < kMaxDev) allowed[dev] = true;
+        if (dev < 0 || dev >= kMaxDev) {
+            e = allow();
+        } else {
+            std::call_once(once[dev], [&] { allow_err[dev] = allow(); });
+            e = allow_err[dev];
         }
+        if (e != cudaSuccess) return e;
     }
     march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(a);
     return cudaGetLastError();

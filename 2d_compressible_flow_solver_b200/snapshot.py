@@ -12,6 +12,13 @@ hold zeros there, and so do these.
 HDF5 is written when h5py is importable (same dataset names); otherwise the
 same datasets are written raw: ``<dir>/<Name>.f64`` (little-endian float64,
 Nx * Ny values in the order above) plus ``<dir>/index.json`` describing them.
+
+A snapshot may also carry the run's counters (no reference counterpart: the
+reference writes snapshots and never reads them back, Output.cpp:20): time,
+last dt, completed steps, the CFL maximum the next step would use and the
+FP32-mixed storage offsets -- what a new engine context needs to continue the
+run bit for bit (``resume_solver``).  Raw: the ``run`` entry of index.json;
+HDF5: attributes of the file.
 """
 from __future__ import annotations
 
@@ -44,9 +51,10 @@ def snapshot_arrays(U: np.ndarray, rhs: np.ndarray | None = None, gamma: float =
 
 
 def write_snapshot(path, U: np.ndarray, rhs: np.ndarray | None = None, *, gamma: float = 1.4, time: float | None = None,
-                   fmt: str = "auto") -> Path:
+                   fmt: str = "auto", run: dict | None = None) -> Path:
     """Writes one snapshot.  fmt: "hdf5" (needs h5py), "raw", or "auto"
-    (HDF5 when h5py is importable, else raw).  Returns the written path."""
+    (HDF5 when h5py is importable, else raw).  run: optional counters
+    (step, cfl_max, offsets, dt; JSON-serialisable).  Returns the written path."""
     data = snapshot_arrays(U, rhs, gamma)
     path = Path(path)
     if fmt == "auto":
@@ -60,6 +68,10 @@ def write_snapshot(path, U: np.ndarray, rhs: np.ndarray | None = None, *, gamma:
         with h5py.File(path, "w") as f:
             for name in DATASETS:
                 f.create_dataset(name, data=np.ascontiguousarray(data[name]))
+            if time is not None:
+                f.attrs["time"] = float(time)
+            if run is not None:
+                f.attrs["run"] = json.dumps(run)
         return path
     if fmt != "raw":
         raise ValueError(f"unknown snapshot format {fmt!r}")
@@ -71,6 +83,8 @@ def write_snapshot(path, U: np.ndarray, rhs: np.ndarray | None = None, *, gamma:
              "order": "x-major: value (i, j) at i * ny + j", "source": "Output::WriteToHDF5 layout"}
     if time is not None:
         index["time"] = float(time)
+    if run is not None:
+        index["run"] = run
     (path / "index.json").write_text(json.dumps(index, indent=1) + "\n")
     return path
 
@@ -87,9 +101,45 @@ def read_snapshot(path) -> dict[str, np.ndarray]:
         return {name: f[name][...] for name in DATASETS}
 
 
-def write_solver_snapshot(solver, path, *, time: float | None = None, fmt: str = "auto") -> Path:
-    """Snapshot of an engine Solver: its state, and its last RHS when it was
-    created with keep_rhs=True (else the flux datasets are zero)."""
+def read_run(path) -> dict:
+    """The run counters (and time) stored with a snapshot, {} when it has none."""
+    path = Path(path)
+    if path.is_dir():
+        index = json.loads((path / "index.json").read_text())
+        run = dict(index.get("run", {}))
+        if "time" in index:
+            run["time"] = index["time"]
+        return run
+    import h5py
+    with h5py.File(path, "r") as f:
+        run = json.loads(f.attrs["run"]) if "run" in f.attrs else {}
+        if "time" in f.attrs:
+            run["time"] = float(f.attrs["time"])
+    return run
+
+
+def write_solver_snapshot(solver, path, *, time: float | None = None, dt: float | None = None,
+                          fmt: str = "auto") -> Path:
+    """Snapshot of an engine Solver: its state, its last RHS when it was
+    created with keep_rhs=True (else the flux datasets are zero), and its run
+    counters (Solver.run_counters) with the caller's time and last dt."""
     U = solver.get_state()
     rhs = solver.get_rhs() if solver.config.keep_rhs else None
-    return write_snapshot(path, U, rhs, gamma=solver.config.gamma, time=time, fmt=fmt)
+    run = solver.run_counters()
+    if dt is not None:
+        run["dt"] = float(dt)
+    return write_snapshot(path, U, rhs, gamma=solver.config.gamma, time=time, fmt=fmt, run=run)
+
+
+def resume_solver(solver, path) -> dict:
+    """Loads a snapshot written by write_solver_snapshot into a Solver of the
+    same configuration so that its next steps are the bits the original run
+    would have taken (storage offsets, state, step counter, carried CFL
+    maximum).  Returns the stored run counters (with time and dt)."""
+    d = read_snapshot(path)
+    U = np.stack([d["Rho"], d["Mu"], d["Mv"], d["Energy"]])
+    run = read_run(path)
+    if not run:
+        raise ValueError(f"{path} holds no run counters (written without them)")
+    solver.resume(U, run)
+    return run

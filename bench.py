@@ -56,15 +56,19 @@ FALLBACK_HBM_GBS = 6650.0
 # stages 2 and 3 read U_s and U^n and write U -> 32 state words.
 WORDS_PER_CELL_STEP = 32
 # DRAM traffic of one stage launch per cell (dram__bytes_read.sum +
-# dram__bytes_write.sum, averaged over the 3 stage launches of a step) from the
-# ncu capture of the tuned FP32 march kernel at 4096^2 summarised in
-# profiles/march_kernel_f32_smooth4096_traffic.md.
+# dram__bytes_write.sum, averaged over the 3 stage launches of a step) from an
+# ncu capture of the tuned FP32 march kernel on this 4096^2 workload (one pass
+# per launch, the three stage launches of one warm step).
 MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
 # Floating-point operations the FP32-mixed march executes per cell-step (its
 # three stage launches; packed FFMA2 = 4, FADD2/FMUL2 = 2, FFMA/DFMA = 2, others
-# 1), from ncu's per-opcode thread-instruction counts of the periodic 2048^2 run
-# in profiles/march_kernel_f32_flops2048.md.  Data-independent on smooth states.
+# 1), from ncu's per-opcode thread-instruction counts (sm__sass_thread_inst_
+# executed_op_*) of a periodic 2048^2 run.  Data-independent on smooth states.
 MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2927.9, "fp64": 27.9}}
+# The reference's scheme as its own driver runs it (Run.cpp:41-48 with
+# TVD3rdRK, RiemmanSolverHLL, transmissive sides, fixed dt): what the
+# reference arm times, and the engine's like-for-like companion rate.
+REF_SCHEME_DT = 1e-4
 
 
 def env_rank():
@@ -229,21 +233,25 @@ def engine_arm(args):
         s.close()
         return ms, t_sim, None, totals
 
-    def timed_advance(prec, steps, warm):
+    def timed_advance(prec, steps, warm, scheme=None):
         if world > 1:
             return timed_advance_slab(prec, steps, warm)
-        s = cfsb.Solver(n, n, precision=prec, variant=variants[prec], **kw)
+        skw, adv = dict(kw), dict(cfl=w.cfl)
+        if scheme == "reference":
+            skw.update(rk=cfsb.RK_TVD3_REFERENCE, hll=cfsb.HLL_REFERENCE, bc=(cfsb.BC_NEUMANN,) * 4)
+            adv = dict(dt=REF_SCHEME_DT)
+        s = cfsb.Solver(n, n, precision=prec, variant=variants[prec], **skw)
         s.set_state(w.U0)
         stream = torch.cuda.ExternalStream(s.stream, device=local)
         if warm:
-            s.advance(warm, cfl=w.cfl)
+            s.advance(warm, **adv)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)
-        t_sim, dt_last = s.advance(steps, cfl=w.cfl)
+        t_sim, dt_last = s.advance(steps, **adv)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -293,8 +301,8 @@ def engine_arm(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                          "traffic": None if trf is None else round(trf * cells),
-                         "traffic_is": "DRAM bytes per stage launch (ncu dram__bytes_read+write, 4096^2, "
-                                       "profiles/march_kernel_f32_smooth4096_traffic.md)",
+                         "traffic_is": "DRAM bytes per stage launch (ncu dram__bytes_read.sum + "
+                                       "dram__bytes_write.sum of the FP32 march kernel on this 4096^2 workload)",
                          "algorithmic_bytes_per_cell_step": WORDS_PER_CELL_STEP * 4,
                          "avg_stage_launch_ms": round(per_launch_ms, 4),
                          "fp_pipe": {"achieved": round(fp_achieved, 2), "unit": "TFLOP/s",
@@ -304,13 +312,25 @@ def engine_arm(args):
                                                     f"packed FFMA2 {fp_peak['fp32_ffma2']:.1f}, "
                                                     f"FP64 DFMA {fp_peak['fp64_dfma']:.1f} TFLOP/s)",
                                      "flops_per_cell_step": round(fl["fp32"] + fl["fp64"], 1),
-                                     "flops_source": "ncu per-opcode counts, profiles/march_kernel_f32_flops2048.md"}},
+                                     "flops_source": "ncu per-opcode thread-instruction counts of the FP32 march "
+                                                     "kernel (periodic 2048^2)"}},
             "fp64": {"value": round(v64, 1), "ms_per_step": round(ms64 / K, 4),
                      "roofline_frac": round(WORDS_PER_CELL_STEP * 8 * cells * K / (ms64 / 1e3) / 1e9 / peak, 4),
                      "fp32_over_fp64": round(v32 / v64, 3)},
             "clocks": clocks,
             "gpu_launches": launches,
         }
+    # like-for-like companion of the reference arm: the reference's own scheme
+    # (TVD3rdRK as written, its HLL, transmissive sides, fixed dt) on the same
+    # 4096^2 state, FP64 and FP32-mixed
+    if world == 1 and rank == 0:
+        msr64, _, _, _ = timed_advance(cfsb.FP64, K, W, scheme="reference")
+        msr32, _, _, _ = timed_advance(cfsb.FP32_MIXED, K, W, scheme="reference")
+        result["same_scheme_as_reference_arm"] = {
+            "scheme": f"TVD3rdRK as written + reference HLL + WENO5 eps 1e-2, transmissive sides, fixed dt "
+                      f"{REF_SCHEME_DT}, {n}x{n}, smooth advection state",
+            "fp64": round(cells * K / (msr64 / 1e3) / 1e6, 1), "fp32_mixed": round(cells * K / (msr32 / 1e3) / 1e6, 1),
+            "timing": "CUDA events on the engine's stream, K steps after W warm-up steps"}
     # accuracy of FP32-mixed against FP64 at t_end (fixed dt so both forms sit
     # on the same time levels), and conservation drift
     if rank == 0 and args.accuracy_n > 0:
@@ -358,11 +378,16 @@ def engine_arm(args):
             s.get_state(out.numpy())
             wall = time.perf_counter() - t0
         state_bytes = 4 * cells * 8
-        result["e2e"] = {"value": round(cells * K / wall / 1e6, 1), "unit": UNIT,
+        result["e2e"] = {"value": round(cells * K / wall / 1e6, 1), "unit": UNIT, "steps": K,
                          "h2d_bytes_per_step": int(state_bytes / K + 40),
                          "d2h_bytes_per_step": int(state_bytes / K + 48),
                          "how": "cfs_set_state from pinned host, K x cfs_advance(1) with dt/t read back, "
-                                "cfs_get_state to pinned host; host wall clock"}
+                                "cfs_get_state to pinned host; host wall clock.  One FP64 state (537 MB) goes "
+                                "up and one comes down per run, so the rate depends on K (the steps field)"}
+    # the uneven 512-case batch (persistent batched engine), bounded: K steps
+    # per form, device-timed with CUDA events on the batch's stream
+    if rank == 0 and world == 1 and args.batch_cases > 0:
+        result["batch"] = batch_subresult(cfsb, wl, torch, args.batch_cases, K, W, local)
     # CPU baseline: the reference's own classes on the host cores (rank 0, N=1)
     if rank == 0:
         if world == 1 and args.cpu_sample > 0:
@@ -385,6 +410,41 @@ def engine_arm(args):
 
 
 # ------------------------------------------------------------ batch arm
+def batch_subresult(cfsb, wl, torch, ncases: int, K: int, W: int, device: int) -> dict:
+    """The uneven batch in the default line: every case of `ncases` (seeded,
+    nx, ny in 64..768) advanced K steps after W warm-up steps by the persistent
+    batched engine, FP32-mixed and FP64, timed with CUDA events on the batch's
+    stream (the per-case CFL reductions, graph replays and the final read-back
+    of the per-case times included)."""
+    cases, states = wl.batch_cases(ncases, seed=1)
+    out = {"workload": f"{ncases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
+                       "cylinder (slip wall), SSP-RK3, Davis HLL, positivity fallbacks with floors, per-case CFL 0.5",
+           "steps": K, "warmup": W}
+    for prec, key in ((cfsb.FP32_MIXED, "fp32"), (cfsb.FP64, "fp64")):
+        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR, device=device) as b:
+            cells, items = b.info()
+            for k, U in enumerate(states):
+                b.set_state(k, U)
+            b.advance(W, cfl=0.5)
+            stream = torch.cuda.ExternalStream(b.stream, device=device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            b.advance(K, cfl=0.5)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            out[key] = round(cells * K / (e0.elapsed_time(e1) / 1e3) / 1e6, 1)
+        out["cells"] = cells
+        out["work_items_per_stage"] = items
+    peak, kind = hbm_peak()
+    out["value"] = out["fp32"]
+    out["unit"] = UNIT
+    out["fp32_over_fp64"] = round(out["fp32"] / out["fp64"], 3)
+    out["hbm_frac_fp32"] = round(out["fp32"] * 1e6 * WORDS_PER_CELL_STEP * 4 / 1e9 / peak, 4)
+    out["hbm_peak"] = f"{peak} GB/s ({kind})"
+    return out
+
+
 def batch_arm(args):
     """Uneven batch of independent cases (512 by default): aggregate
     Mcell-steps/s of the persistent batched engine (FP32-mixed and FP64) and of
@@ -581,7 +641,90 @@ def report_arm(args):
 
 
 # ----------------------------------------------------------- reference arm
+# Bytes the reference's object graph holds per cell (Cell, faces, phases,
+# fluxes, stencil lists), measured on its own build: about 2.2 KB; the arm sizes
+# its tiles against the host's available memory with this figure.
+REF_BYTES_PER_CELL = 2500
+
+
+def _ref_tile_worker(conn, n: int, root: str) -> None:
+    """One host core's share of the reference arm: builds an n x n grid of the
+    smooth workload with the reference's own classes (perf build) once, then
+    on each request runs one RK step (3 Run::solver iterations of TVD3rdRK) and
+    returns the stage loop's wall-clock seconds."""
+    sys.path.insert(0, root)
+    sys.path.insert(0, str(Path(root) / "tests"))
+    import oracle_bind as ob
+    wl = importlib.import_module(f"{PKG}.workloads")
+    lib = ob.ref_lib(perf=True)
+    lib.ref_session_create.restype = ctypes.c_void_p
+    lib.ref_session_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.ref_session_stages.restype = ctypes.c_double
+    lib.ref_session_stages.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.ref_session_destroy.restype = None
+    lib.ref_session_destroy.argtypes = [ctypes.c_void_p]
+    U = np.ascontiguousarray(wl.smooth_advection(n).U0)
+    c = ob.make_ref_config(n, n, integrator=3, dt=REF_SCHEME_DT)
+    t0 = time.perf_counter()
+    h = lib.ref_session_create(ctypes.byref(c), ob.P(U))
+    del U
+    conn.send(("ready", time.perf_counter() - t0))
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        conn.send(lib.ref_session_stages(h, 3))
+    lib.ref_session_destroy(h)
+    conn.close()
+
+
+def ref_tiles_rate(cores: int, n: int, steps: int, warm: int) -> dict:
+    """`cores` concurrent reference processes, one n x n tile each: every step
+    all of them run one RK step; the step's time is the host wall clock from the
+    request to the last answer.  Returns the rate over the timed steps."""
+    ctx = mp.get_context("spawn")
+    procs, pipes = [], []
+    for _ in range(cores):
+        a, b = ctx.Pipe()
+        pr = ctx.Process(target=_ref_tile_worker, args=(b, n, str(ROOT)), daemon=True)
+        pr.start()
+        procs.append(pr)
+        pipes.append(a)
+    try:
+        build = max(pp.recv()[1] for pp in pipes)
+        walls = []
+        for k in range(warm + steps):
+            t0 = time.perf_counter()
+            for pp in pipes:
+                pp.send(1)
+            for pp in pipes:
+                pp.recv()
+            if k >= warm:
+                walls.append(time.perf_counter() - t0)
+    finally:
+        for pp in pipes:
+            try:
+                pp.send(None)
+            except (BrokenPipeError, OSError):
+                pass
+        for pr in procs:
+            pr.join(timeout=60)
+    total = sum(walls)
+    cells = cores * n * n
+    return {"value": cells * steps / total / 1e6, "ms_per_step": total / steps * 1e3, "cells_per_step": cells,
+            "build_s": build, "step_walls_s": [round(x, 3) for x in walls]}
+
+
 def reference_arm(args):
+    """The reference's own CPU implementation of the path (its classes built
+    with its Makefile's optimisation flags, oracle/_ref/libref_perf.so) on all
+    host cores: one single-rank process per core, each holding its own tile of
+    the smooth workload, all stepping together (the MPI build's per-rank work
+    without its halo exchange, CartesianParallel.cpp:3-47).  The tiles add up
+    to the engine's n x n cells when the host's memory allows (about 2.2 KB per
+    cell in the reference's object graph), else to the largest share it allows;
+    the line reports the cells actually stepped and the measured time per step,
+    nothing extrapolated."""
     rank, world, _ = env_rank()
     if rank != 0:
         return
@@ -591,21 +734,34 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_perf.so not built "
                           "(needs the reference tree; run __graft_entry__.build())"}), flush=True)
         return
-    n = args.cpu_sample
-    rates, walls = cpu_reference_rate(cores, n, args.steps, warm=args.warmup)
-    v = statistics.median(rates)
-    ms_per_step = 4096 * 4096 / (v * 1e6) * 1e3
+    n = args.ref_tile
+    if n <= 0:
+        n = int(args.n / math.sqrt(cores)) // 16 * 16
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+            while n > 64 and cores * n * n * REF_BYTES_PER_CELL > 0.6 * avail:
+                n -= 64
+        except ImportError:
+            pass
+    r = ref_tiles_rate(cores, n, args.steps, args.warmup)
+    v = r["value"]
+    workload = (f"smooth advection state (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1) as {cores} independent {n}x{n} tiles "
+                f"= {r['cells_per_step']} cells per step (engine line: {args.n}x{args.n} = {args.n * args.n}), "
+                f"one single-rank reference process per host core; TVD3rdRK as written, reference HLL "
+                f"(RiemmanSolverHLL), WENO5 eps 1e-2, transmissive sides, fixed dt {REF_SCHEME_DT}")
     out = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"smooth periodic advection {args.n}x{args.n} (rho=1+0.2 sin 2pi(x+y), u=v=1, p=1), "
-                               "SSP-RK3, WENO5 eps 1e-2, Davis HLL, CFL 0.4 on-device dt",
-                   "precision": "reference FP64 (-O3 -ffast-math)", "grid": [args.n, args.n]},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_per_step"], 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload, "tiles": cores, "tile": [n, n], "cells_per_step": r["cells_per_step"],
+                   "precision": "reference FP64 (its Makefile's -O3 -ffast-math flags, -march=x86-64-v3)",
+                   "timing": "host wall clock per step from the request to the last process's answer; grid "
+                             f"set-up outside (slowest {r['build_s']:.1f} s)",
+                   "same_scheme_engine_rate": "the engine line's same_scheme_as_reference_arm"},
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"each step: {cores} concurrent single-rank processes of the reference's classes, "
-                                   f"one RK3 step (TVD3rdRK) on a {n}^2 grid of the workload with transmissive sides "
-                                   "(no periodic sides in the reference); ms_per_step extrapolated to the full grid"},
+                                   f"one RK step (3 solver iterations) each on its own {n}x{n} tile"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -680,6 +836,10 @@ def main():
                          "FP32-vs-FP64 accuracy and drift on the other configurations; modes: the row march's "
                          "feature sets on one grid (one JSON line each)")
     ap.add_argument("--cases", type=int, default=512, help="cases of the batch workload")
+    ap.add_argument("--batch-cases", type=int, default=512,
+                    help="cases of the batch sub-result in the default line (0 = skip)")
+    ap.add_argument("--ref-tile", type=int, default=0,
+                    help="reference arm: tile edge per host core (0 = tiles summing to n^2 cells)")
     ap.add_argument("--modes-n", type=int, default=2048, help="grid edge of the modes workload")
     ap.add_argument("--mode", choices=list(MODES), default=None, help="modes workload: run this mode only (FP32)")
     args = ap.parse_args()

@@ -36,7 +36,8 @@ enum cfs_status {
     CFS_ERR_CUDA = 2,       /* a CUDA call failed (message has the CUDA error) */
     CFS_ERR_NOMEM = 3,      /* device or host allocation failed */
     CFS_ERR_STATE = 4,      /* call not valid in the context's current state */
-    CFS_ERR_NUMERIC = 5     /* non-finite or non-positive dt from the CFL reduction */
+    CFS_ERR_NUMERIC = 5     /* the CFL reduction met a non-finite fluid cell (a blow-up), or
+                               gave a non-positive dt */
 };
 
 enum cfs_precision {
@@ -232,7 +233,9 @@ int cfs_ib_fill(cfs_ctx* ctx);
 /* CFL step on the current state: dt = cfl / max over fluid cells of
  * (|u|+a)/dx + (|v|+a)/dy.  No reference counterpart (the reference fixes dt,
  * param.h:20, set by Explicit::setTimeStep at Run.cpp:95).  Warp-shuffle max
- * reduction; the max is exact, so dt is the same on every launch. */
+ * reduction; the max is exact, so dt is the same on every launch.  A fluid
+ * cell whose wave-speed sum is not finite (NaN from a negative pressure or
+ * density) makes the maximum +infinity: CFS_ERR_NUMERIC. */
 int cfs_compute_dt(cfs_ctx* ctx, double cfl, double* dt);
 
 /* One iteration of Run::solver's loop (Run.cpp:153-203) with loop counter
@@ -254,7 +257,10 @@ int cfs_step(cfs_ctx* ctx, double dt);
  * touched the state since (so K calls of one step take the steps one call of
  * K steps takes); otherwise the first step's reduction runs at the call's
  * start.  cfl <= 0: fixed dt.  *t_elapsed (optional) receives the simulated
- * time advanced, *dt_last the last dt. */
+ * time advanced, *dt_last the last dt.  With cfl > 0, a fluid cell that turns
+ * non-finite in any step makes every later dt 0, and the call returns
+ * CFS_ERR_NUMERIC (also when it happens in the last step: the final stage's
+ * CFL maximum is then +infinity). */
 int cfs_advance(cfs_ctx* ctx, int nsteps, double cfl, double dt, double* t_elapsed, double* dt_last);
 
 /* Halo exchange of a slab decomposition along x (the reference's process
@@ -275,6 +281,21 @@ int cfs_halo_unpack(cfs_ctx* ctx, int side, const void* dev_src);
  * cfs_set_state calls; off = NULL returns to the default.  No effect on the
  * FP64 forms.  (No reference counterpart.) */
 int cfs_set_storage_offsets(cfs_ctx* ctx, const double* off4);
+
+/* Run counters, for resuming a run bit for bit from a snapshot in a new
+ * context (no reference counterpart: the reference writes snapshots but never
+ * reads them back, Output.cpp:20).
+ * get: *step = completed RK steps (the counter the FP32-mixed stochastic
+ *   rounding hashes with each cell); *cfl_max = the CFL maximum of the current
+ *   state that the next cfs_advance will use (left by the last advance's final
+ *   stage), 0 when none is carried; off4[4] = the FP32-mixed storage offsets
+ *   (cfs_set_storage_offsets; 0 in the FP64 forms).  Any pointer may be NULL.
+ * set: after cfs_set_state, installs step and cfl_max (0: the next
+ *   cfs_advance reduces the maximum afresh).  CFS_ERR_STATE inside a step.
+ * Resume = cfs_set_storage_offsets(off4), cfs_set_state(U), cfs_set_step(step,
+ * cfl_max): the following steps are then the bits the uninterrupted run takes. */
+int cfs_get_step(cfs_ctx* ctx, unsigned int* step, double* cfl_max, double* off4);
+int cfs_set_step(cfs_ctx* ctx, unsigned int step, double cfl_max);
 
 /* Waits for the context's stream. */
 int cfs_synchronize(cfs_ctx* ctx);
@@ -317,22 +338,30 @@ int cfs_batch_get_state(cfs_batch* b, int c, double* U);
 /* nsteps RK steps of every case with per-case CFL dt (cfl > 0) or a common
  * fixed dt; t (optional, [ncases]) receives each case's simulated time. */
 int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t);
+/* The batch's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against it. */
+void* cfs_batch_get_stream(cfs_batch* b);
 /* Total cells of the batch and the number of work items of one stage launch. */
 int cfs_batch_info(const cfs_batch* b, long long* cells, int* items);
 
 /* CFL step of a caller-owned device state, for callers that cannot allocate
- * device memory (no counterpart in the reference).  Same dt, bit for bit, as
- * cfs_compute_dt on the same state; needs no context and calls no cudaMalloc,
- * cudaFree or allocating library routine.  U: device array U[4][nx][ny]
- * (reference order, FP64); types: device uint8 [nx][ny] (0 = fluid) or NULL
- * for all fluid; stream: a cudaStream_t or NULL; *dt: host output.  Runs on the
- * current device and waits for its stream before returning.
+ * device memory (no counterpart in the reference).  For a state held by a
+ * CFS_FP64 or CFS_FP64_EXACT context, the same dt, bit for bit, as
+ * cfs_compute_dt on that context (a CFS_FP32_MIXED context reduces its
+ * FP32-rounded, offset storage, so its dt can differ in the last bits); needs
+ * no context and calls no cudaMalloc, cudaFree or allocating library routine.
+ * U: device array U[4][nx][ny] (reference order, FP64); types: device uint8
+ * [nx][ny] (0 = fluid) or NULL for all fluid; stream: a cudaStream_t or NULL;
+ * *dt: host output.  Runs on the current device.
  * Scratch is a fixed static device array, so nx*ny is limited to 16,777,216
  * cells (4096 x 4096); larger grids are refused with CFS_ERR_INVALID.  The first
- * call on a device looks up that array's device address (cudaGetSymbolAddress),
- * so make the first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (other streams, other host threads)
- * race and must be serialised by the caller.  Errors: cfs_last_error(NULL). */
+ * call on a device looks up that array's device address (cudaGetSymbolAddress).
+ * Every call copies dt to the host (pageable memory) and waits for `stream`,
+ * so no call may be made on a stream that is being captured into a CUDA graph.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  A fluid cell
+ * whose wave-speed sum is not finite gives CFS_ERR_NUMERIC, as in
+ * cfs_compute_dt.  Errors: cfs_last_error(NULL). */
 int cfs_compute_dt_static(const double* U, const uint8_t* types, int nx, int ny, double lx, double ly,
                           double gamma, double cfl, void* stream, double* dt);
 

@@ -358,7 +358,8 @@ double orc_cfl_dt(const orc_config* c, const uint8_t* types, const double* U, do
         const double p = (g - 1) * (E - 0.5 * (mx * mx + my * my) / rho);
         const double a = sqrt(g * p / rho);
         const double u = mx / rho, v = my / rho;
-        const double w = (fabs(u) + a) / dx + (fabs(v) + a) / dy;
+        double w = (fabs(u) + a) / dx + (fabs(v) + a) / dy;
+        if (!(w == w)) w = INFINITY; /* a blown-up cell: dt = 0, as the engine reports it */
         if (w > m) m = w;
     }
     return cfl / m;

@@ -20,6 +20,7 @@
 #include "initialcondition/Initialcondition.h"
 
 #include <chrono>
+#include <cmath>
 #include <cstring>
 
 #ifdef CFS_WITH_GPU_PLUGINS
@@ -199,7 +200,8 @@ double cfl_dt(Sim& s, const ref_config& c) {
             const double p = (Gamma - 1) * (E - 0.5 * (mx * mx + my * my) / rho);
             const double a = std::sqrt(Gamma * p / rho);
             const double u = mx / rho, v = my / rho;
-            const double w = (std::fabs(u) + a) / dx + (std::fabs(v) + a) / dy;
+            double w = (std::fabs(u) + a) / dx + (std::fabs(v) + a) / dy;
+            if (!(w == w)) w = HUGE_VAL;  // a blown-up cell: dt = 0, as the engine and the oracle take it
             if (w > m) m = w;
         }
     return c.cfl / m;
@@ -282,6 +284,35 @@ int ref_run(const ref_config* c, const double* U_in, int nstages, double* U_out,
     }
     reset_globals();
     return 0;
+}
+
+// A grid kept between timing calls (one per process: the reference's plugins
+// are process globals): create builds it as Run::initialize does, each
+// ref_session_stages call runs the next `nstages` solver iterations and
+// returns their wall-clock seconds, destroy frees it.
+struct RefSession {
+    Sim s;
+    int next = 1;  // loop counter of the next iteration
+};
+
+void* ref_session_create(const ref_config* c, const double* U_in) {
+    auto* r = new RefSession();
+    initialize(r->s, *c, U_in);
+    preloop(r->s, c->dt);
+    return r;
+}
+
+double ref_session_stages(void* h, int nstages) {
+    auto* r = static_cast<RefSession*>(h);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < nstages; ++k) stage(r->s, r->next++);
+    const auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void ref_session_destroy(void* h) {
+    delete static_cast<RefSession*>(h);
+    reset_globals();
 }
 
 // Wall-clock seconds of `nstages` solver iterations (setup excluded).

@@ -20,7 +20,20 @@ REF_STRICT = ORACLE / "_ref" / "libref_strict.so"
 REF_PERF = ORACLE / "_ref" / "libref_perf.so"
 REF_GPU = ORACLE / "_ref" / "libref_gpu.so"
 ORACLE_LIB = ORACLE / "libcfs_oracle.so"
-REFERENCE_TREE = Path("/root/reference")
+
+
+def _reference_tree() -> Path | None:
+    """The reference source tree, as oracle/Makefile resolves it
+    (CFS_REFERENCE_TREE or the recipe's own default), or None when absent."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", str(ORACLE), "ref-tree"], capture_output=True, text=True, timeout=60)
+    except (OSError, subprocess.TimeoutExpired):
+        return None
+    out = r.stdout.strip()
+    return Path(out) if r.returncode == 0 and out else None
+
+
+REFERENCE_TREE = _reference_tree()
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -57,7 +70,7 @@ def ensure_built() -> None:
     targets = []
     if not ORACLE_LIB.exists():
         targets.append("oracle")
-    if (not REF_STRICT.exists() or not REF_PERF.exists()) and REFERENCE_TREE.exists():
+    if (not REF_STRICT.exists() or not REF_PERF.exists()) and REFERENCE_TREE is not None:
         targets.append("ref")
     if targets:
         subprocess.run(["make", "-C", str(ORACLE), "-j8", *targets], check=True, capture_output=True)

@@ -9,7 +9,7 @@ import pytest
 import oracle_bind as ob
 
 GOLD = Path(__file__).resolve().parent / "golden"
-has_ref = ob.REF_STRICT.exists() or ob.REFERENCE_TREE.exists()
+has_ref = ob.REF_STRICT.exists() or ob.REFERENCE_TREE is not None
 
 
 def test_cylinder_full_size_matches_reference_fixture(cfsb):

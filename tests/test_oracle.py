@@ -13,7 +13,7 @@ import oracle_bind as ob
 
 GOLD = Path(__file__).resolve().parent / "golden"
 MACH3 = (1.4, 3.0, 0.0, 1.0)
-has_ref = ob.REF_STRICT.exists() or ob.REFERENCE_TREE.exists()
+has_ref = ob.REF_STRICT.exists() or ob.REFERENCE_TREE is not None
 
 
 def _load(name):

@@ -65,3 +65,41 @@ def test_static_dt_refuses_grids_beyond_its_scratch(cfsb):
         # the size check comes before any device work, so no state is needed
         _static_dt(cfsb, 1 << 20, 0, 4097, 4096, 1.0, 1.0, 0.5)
     assert e.value.code == 1 and "static scratch limit" in str(e.value)
+
+
+@pytest.mark.parametrize("nx,ny", [(4096, 1024), (4096, 4096)])
+def test_static_dt_on_many_blocks_matches_context_dt(cfsb, workloads, nx, ny):
+    """512 and 2048 partial blocks: the final kernel's strided loop over more
+    than its 256 threads, and the largest grid the static scratch admits."""
+    import torch
+
+    w = workloads.riemann_quadrants(nx, ny, seed=13)
+    with cfsb.Solver(nx, ny) as s:
+        s.set_state(w.U0)
+        ref = s.compute_dt(0.5)
+    U_dev = torch.tensor(w.U0, dtype=torch.float64, device="cuda:0").contiguous()
+    del w
+    torch.cuda.synchronize()
+    for _ in range(2):
+        assert _static_dt(cfsb, U_dev.data_ptr(), 0, nx, ny, 1.0, 1.0, 0.5) == ref
+    del U_dev
+    torch.cuda.empty_cache()
+
+
+def test_static_dt_reports_a_non_finite_cell(cfsb, workloads):
+    import torch
+
+    w = workloads.riemann_quadrants(300, 217, seed=12)
+    U = w.U0.copy()
+    U[3, 150, 100] = np.nan
+    U_dev = torch.tensor(U, dtype=torch.float64, device="cuda:0").contiguous()
+    torch.cuda.synchronize()
+    with pytest.raises(cfsb.CfsError) as e:
+        _static_dt(cfsb, U_dev.data_ptr(), 0, 300, 217, 1.0, 1.0, 0.5)
+    assert e.value.code == 5
+    # the shared scratch holds nothing over from the failed call
+    U_dev[3, 150, 100] = float(w.U0[3, 150, 100])
+    torch.cuda.synchronize()
+    with cfsb.Solver(300, 217) as s:
+        s.set_state(w.U0)
+        assert _static_dt(cfsb, U_dev.data_ptr(), 0, 300, 217, 1.0, 1.0, 0.5) == s.compute_dt(0.5)
