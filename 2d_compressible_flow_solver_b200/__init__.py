@@ -147,6 +147,9 @@ _SIGNATURES = {
     "cfs_batch_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          _c_double_p]),
     "cfs_batch_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "cfs_batch_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "cfs_batch_advance_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p]),
+    "cfs_batch_dt_last": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                       ctypes.POINTER(ctypes.c_int)]),
     "cfs_weno5_faces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
@@ -546,9 +549,28 @@ class Batch:
         self._check(self._lib.cfs_batch_get_state(self._b, int(case), _dp(out)))
         return out
 
-    def advance(self, nsteps: int, cfl: float = 0.0, dt: float = 0.0) -> np.ndarray:
-        """Runs nsteps RK steps of every case; returns each case's simulated time."""
+    def advance(self, nsteps: int, cfl: float = 0.0, dt=0.0) -> np.ndarray:
+        """Runs nsteps RK steps of every case (per-case CFL dt when cfl > 0;
+        else dt, a common value or one per case); returns each case's
+        simulated time."""
         t = np.zeros(len(self.shapes))
-        self._check(self._lib.cfs_batch_advance(self._b, int(nsteps), float(cfl), float(dt), _dp(t)))
+        if np.ndim(dt) == 0:
+            self._check(self._lib.cfs_batch_advance(self._b, int(nsteps), float(cfl), float(dt), _dp(t)))
+        else:
+            d = np.ascontiguousarray(dt, dtype=np.float64)
+            if d.shape != (len(self.shapes),):
+                raise ValueError("need one dt per case")
+            self._check(self._lib.cfs_batch_advance_dt(self._b, int(nsteps), _dp(d), _dp(t)))
         return t
+
+    def dt_last(self) -> np.ndarray:
+        """Per case, the dt of the last step taken."""
+        d = np.zeros(len(self.shapes))
+        self._check(self._lib.cfs_batch_dt_last(self._b, _dp(d)))
+        return d
+
+    @property
+    def stream(self) -> int:
+        """The batch's cudaStream_t as an integer handle."""
+        return int(self._lib.cfs_batch_get_stream(self._b) or 0)
 

@@ -77,6 +77,7 @@ struct cfs_batch {
     long long total_cells = 0;
     bool args_dirty = true;
     unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
+    std::vector<double> dt_last;  // per case: dt of the last step taken (0 before any)
     cudaGraphExec_t graph2 = nullptr;
     std::string err;
 };
@@ -265,6 +266,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     b->elem = b->prec == cfs::kF32Mixed ? 4 : 8;
     b->n = ncases;
     b->cases.resize(ncases);
+    b->dt_last.assign(ncases, 0.0);
     if (cudaSetDevice(common->device) != cudaSuccess) return bail(CFS_ERR_CUDA, "cudaSetDevice failed");
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(CFS_ERR_CUDA, "stream creation failed");
@@ -443,6 +445,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
 
 void* cfs_batch_get_stream(cfs_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
 
+void* cfs_batch_get_stream(cfs_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
 int cfs_batch_info(const cfs_batch* b, long long* cells, int* items) {
     if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
     if (cells) *cells = b->total_cells;
@@ -488,21 +492,24 @@ int cfs_batch_get_state(cfs_batch* b, int ci, double* U) {
     return CFS_OK;
 }
 
-int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t) {
-    if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
-    if (nsteps < 0 || (!(cfl > 0) && !(dt > 0))) return bfail(b, CFS_ERR_INVALID, "give nsteps >= 0 and cfl > 0 or dt > 0");
+namespace {
+
+// nsteps steps of every case: per-case CFL dt (cfl > 0), else a fixed dt per
+// case (dt_case[c], or the common dt when dt_case is null).
+int batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, const double* dt_case, double* t) {
     CFSB_CUDA(b, cudaSetDevice(b->common.device));
     if (b->args_dirty) {
         const int rc = upload_args(b);
         if (rc != CFS_OK) return rc;
     }
     std::vector<cfs::DevParams> hp(b->n);
-    for (auto& p : hp) {
+    for (int ci = 0; ci < b->n; ++ci) {
+        cfs::DevParams& p = hp[ci];
         p = cfs::DevParams{};
         p.use_cfl = cfl > 0 ? 1 : 0;
         p.seed[0] = p.seed[1] = b->steps_done;
         p.cfl = cfl;
-        p.dt_fixed = dt;
+        p.dt_fixed = dt_case ? dt_case[ci] : dt;
     }
     CFSB_CUDA(b, cudaMemcpyAsync(b->P, hp.data(), sizeof(cfs::DevParams) * b->n, cudaMemcpyHostToDevice, b->stream));
     // first step's CFL maxima: the stage-0 arguments of parity 0 read S0 and
@@ -536,6 +543,7 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
     b->steps_done += static_cast<unsigned int>(nsteps);
     for (int ci = 0; ci < b->n; ++ci) {
         if (t) t[ci] = hp[ci].t;
+        if (nsteps > 0) b->dt_last[ci] = hp[ci].dt_last;
         if (nsteps > 0 && (!(hp[ci].dt_last > 0) || !std::isfinite(hp[ci].dt_last)))
             return bfail(b, CFS_ERR_NUMERIC, "case " + std::to_string(ci) + ": time step became non-finite or non-positive");
         // the final state's CFL maximum (left by the last stage) is +infinity
@@ -543,6 +551,29 @@ int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t
         if (nsteps > 0 && cfl > 0 && hp[ci].wmax[nsteps % 2 == 1 ? 1 : 0] == kInfBits)
             return bfail(b, CFS_ERR_NUMERIC, "case " + std::to_string(ci) + ": a fluid cell became non-finite");
     }
+    return CFS_OK;
+}
+
+}  // namespace
+
+int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t) {
+    if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
+    if (nsteps < 0 || (!(cfl > 0) && !(dt > 0))) return bfail(b, CFS_ERR_INVALID, "give nsteps >= 0 and cfl > 0 or dt > 0");
+    return batch_advance(b, nsteps, cfl, dt, nullptr, t);
+}
+
+int cfs_batch_advance_dt(cfs_batch* b, int nsteps, const double* dt_case, double* t) {
+    if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
+    if (nsteps < 0 || !dt_case) return bfail(b, CFS_ERR_INVALID, "give nsteps >= 0 and a dt per case");
+    for (int ci = 0; ci < b->n; ++ci)
+        if (!(dt_case[ci] > 0) || !std::isfinite(dt_case[ci]))
+            return bfail(b, CFS_ERR_INVALID, "case " + std::to_string(ci) + ": dt must be finite and positive");
+    return batch_advance(b, nsteps, 0.0, 0.0, dt_case, t);
+}
+
+int cfs_batch_dt_last(const cfs_batch* b, double* dt) {
+    if (!b || !dt) return bfail(nullptr, CFS_ERR_INVALID, "null argument");
+    for (int ci = 0; ci < b->n; ++ci) dt[ci] = b->dt_last[ci];
     return CFS_OK;
 }
 

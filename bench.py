@@ -544,100 +544,217 @@ def _errors(a, b):
             "E_L1": float(np.abs(a[3] - b[3]).mean()), "E_Linf": float(np.abs(a[3] - b[3]).max())}
 
 
+def _perturbed(U, kind: str, seed: int = 7):
+    """U with every value moved by a random-sign relative amount: one FP64 ulp
+    ("ulp64") or the FP32 unit roundoff 2^-24 ("u32")."""
+    rng = np.random.default_rng(seed)
+    sign = rng.choice([-1.0, 1.0], size=U.shape)
+    if kind == "ulp64":
+        return np.where(sign > 0, np.nextafter(U, np.inf), np.nextafter(U, -np.inf))
+    return U * (1.0 + sign * 2.0 ** -24)
+
+
 def report_arm(args):
-    """Accuracy and conservation of the FP32-mixed form against FP64 on the
-    configurations beside the headline: four-quadrant Riemann problems (256^2,
-    200 steps, the reference's scheme: TVD3 as written + its HLL, where the FP64
-    form is also compared with the exact form, the reference's arithmetic), the
-    Mach-3 cylinder (2048 x 1024, 3000 steps, slip wall, positivity fallbacks with floors), the
+    """Accuracy and conservation of the FP32-mixed form against FP64, every
+    comparison on ONE time-step sequence: the FP64 run takes its CFL steps one
+    advance call at a time and records each dt; the other runs replay that
+    sequence with fixed steps, so both forms end at the same t_end.
+    Configurations: four-quadrant Riemann problems (256^2, 200 steps, the
+    reference's scheme: TVD3 as written + its HLL; the FP64 form also against
+    the exact form, the reference's arithmetic), the Mach-3 cylinder (2048 x
+    1024, 3000 steps, slip wall, positivity fallbacks with floors), the
     Navier-Stokes shear layer (1024^2, 5000 steps) and the uneven batch (512
-    cases, 100 steps).  Open boundaries (quadrants, cylinder): drift is the
-    FP32-vs-FP64 difference of the totals; periodic shear layer: the change of
-    each form's totals.  One JSON line."""
+    cases, 500 steps).  Beside each FP32 error, the sensitivity of the FP64
+    run itself: the difference at t_end made by perturbing its initial state
+    by one FP64 ulp, and by the FP32 unit roundoff, per value (random signs).
+    Then the smooth-advection convergence table (FP64 and FP32 against the
+    exact solution at t = 0.5, N = 128 .. --conv-max).  Open boundaries:
+    drift is the FP32-vs-FP64 difference of the totals; periodic: the change
+    of each form's totals.  One JSON line."""
     import torch
 
     torch.cuda.set_device(0)
     cfsb = importlib.import_module(PKG)
     wl = importlib.import_module(f"{PKG}.workloads")
-    out = {"report": "FP32-mixed vs FP64 at t_end per configuration"}
+    out = {"report": "FP32-mixed vs FP64 at t_end on one time-step sequence per configuration"}
 
-    def run(w, prec, steps, cfl, extra, circle=None, ib_mode=None):
-        with cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, bc=w.bc, bc_prim=w.bc_prim, **extra) as s:
-            if circle is not None:
-                s.build_circle(*circle, 400, ib_mode)
+    def solver(w, prec, extra, circle=None, ib_mode=None):
+        s = cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, bc=w.bc, bc_prim=w.bc_prim, **extra)
+        if circle is not None:
+            s.build_circle(*circle, 400, ib_mode)
+        return s
+
+    def run_cfl(w, prec, steps, cfl, extra, circle, ib_mode):
+        with solver(w, prec, extra, circle, ib_mode) as s:
             s.set_state(w.U0)
             m0 = s.totals()
+            dts = []
             t0 = time.perf_counter()
-            t, _ = s.advance(steps, cfl=cfl)
+            for _ in range(steps):
+                dts.append(s.advance(1, cfl=cfl)[1])
             wall = time.perf_counter() - t0
-            return s.get_state(), m0, s.totals(), t, wall
+            return s.get_state(), m0, s.totals(), np.array(dts), wall
+
+    def run_dts(w, prec, dts, extra, circle, ib_mode, U0=None):
+        with solver(w, prec, extra, circle, ib_mode) as s:
+            s.set_state(w.U0 if U0 is None else U0)
+            m0 = s.totals()
+            t0 = time.perf_counter()
+            for dt in dts:
+                s.advance(1, dt=float(dt))
+            wall = time.perf_counter() - t0
+            return s.get_state(), m0, s.totals(), wall
 
     def compare(name, w, steps, cfl, extra, circle=None, ib_mode=None, exact=False, periodic=False):
-        r64 = run(w, cfsb.FP64, steps, cfl, extra, circle, ib_mode)
-        r32 = run(w, cfsb.FP32_MIXED, steps, cfl, extra, circle, ib_mode)
-        row = {"grid": [w.nx, w.ny], "steps": steps, "t_end_fp64": r64[3], "t_end_fp32": r32[3],
-               "fp32_vs_fp64": _errors(r32[0], r64[0]),
-               "finite": bool(np.all(np.isfinite(r64[0])) and np.all(np.isfinite(r32[0]))),
-               "mcell_steps_per_s": {"fp64": round(w.nx * w.ny * steps / r64[4] / 1e6, 1),
-                                     "fp32": round(w.nx * w.ny * steps / r32[4] / 1e6, 1)}}
+        U64, m0_64, m1_64, dts, wall64 = run_cfl(w, cfsb.FP64, steps, cfl, extra, circle, ib_mode)
+        U32, m0_32, m1_32, wall32 = run_dts(w, cfsb.FP32_MIXED, dts, extra, circle, ib_mode)
+        row = {"grid": [w.nx, w.ny], "steps": steps, "t_end": float(dts.sum()),
+               "dt_sequence": "FP64 CFL steps, replayed as fixed steps by the other runs",
+               "fp32_vs_fp64": _errors(U32, U64),
+               "finite": bool(np.all(np.isfinite(U64)) and np.all(np.isfinite(U32))),
+               "mcell_steps_per_s_one_step_per_call": {"fp64": round(w.nx * w.ny * steps / wall64 / 1e6, 1),
+                                                       "fp32": round(w.nx * w.ny * steps / wall32 / 1e6, 1)}}
+        sens = {}
+        for kind in ("ulp64", "u32"):
+            Up = _perturbed(w.U0, kind)
+            Ux, _, _, _ = run_dts(w, cfsb.FP64, dts, extra, circle, ib_mode, U0=Up)
+            d0 = float(np.abs(Up[0] - w.U0[0]).mean())
+            e = _errors(Ux, U64)
+            sens[kind] = {"rho_L1_initial": d0, "rho_L1_at_t_end": e["rho_L1"], "rho_Linf_at_t_end": e["rho_Linf"],
+                          "amplification_L1": e["rho_L1"] / d0 if d0 > 0 else None}
+        row["fp64_sensitivity"] = sens
         if periodic:
-            row["drift_fp32"] = {"mass": float(abs(r32[2][0] - r32[1][0]) / abs(r32[1][0])),
-                                 "energy": float(abs(r32[2][3] - r32[1][3]) / abs(r32[1][3]))}
-            row["drift_fp64"] = {"mass": float(abs(r64[2][0] - r64[1][0]) / abs(r64[1][0])),
-                                 "energy": float(abs(r64[2][3] - r64[1][3]) / abs(r64[1][3]))}
+            row["drift_fp32"] = {"mass": float(abs(m1_32[0] - m0_32[0]) / abs(m0_32[0])),
+                                 "energy": float(abs(m1_32[3] - m0_32[3]) / abs(m0_32[3]))}
+            row["drift_fp64"] = {"mass": float(abs(m1_64[0] - m0_64[0]) / abs(m0_64[0])),
+                                 "energy": float(abs(m1_64[3] - m0_64[3]) / abs(m0_64[3]))}
         else:
-            row["totals_fp32_vs_fp64"] = {"mass": float(abs(r32[2][0] - r64[2][0]) / abs(r64[2][0])),
-                                          "energy": float(abs(r32[2][3] - r64[2][3]) / abs(r64[2][3]))}
+            row["totals_fp32_vs_fp64"] = {"mass": float(abs(m1_32[0] - m1_64[0]) / abs(m1_64[0])),
+                                          "energy": float(abs(m1_32[3] - m1_64[3]) / abs(m1_64[3]))}
         if exact:
-            rx = run(w, cfsb.FP64_EXACT, steps, cfl, extra, circle, ib_mode)
-            row["fp64_vs_exact"] = _errors(r64[0], rx[0])
-            row["exact_finite"] = bool(np.all(np.isfinite(rx[0])))
+            Ue, _, _, _ = run_dts(w, cfsb.FP64_EXACT, dts, extra, circle, ib_mode)
+            row["fp64_vs_exact_form"] = _errors(U64, Ue)
+            row["exact_form_finite"] = bool(np.all(np.isfinite(Ue)))
         out[name] = row
+        print(json.dumps({name: row}), file=sys.stderr, flush=True)
 
-    w1 = wl.riemann_quadrants(256, 256, seed=1)
-    compare("quadrants_256_reference_scheme", w1, 200, 0.5,
-            dict(rk=cfsb.RK_TVD3_REFERENCE, hll=cfsb.HLL_REFERENCE), exact=True)
-    w3 = wl.mach3_cylinder(2048, 1024)
-    compare("mach3_cylinder_2048x1024", w3, 3000, 0.5,
-            dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, positivity=cfsb.POSITIVITY_FLOOR),
-            circle=w3.circle, ib_mode=cfsb.IB_BILINEAR_SLIP)
-    w4 = wl.shear_layer(1024)
-    compare("shear_layer_1024_ns", w4, 5000, 0.5,
-            dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, viscous=cfsb.VISCOUS_NS, mu=w4.meta["mu"], prandtl=0.72,
-                 mach=1.0), periodic=True)
-    # immersed-boundary set-up of the cylinder grid on the host and on the device
-    def best_s(fn, reps=3):
-        best = None
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            r = fn()
-            dt = time.perf_counter() - t0
-            best = dt if best is None or dt < best else best
-        return best, r
-    geo = (w3.nx, w3.ny, w3.lx, w3.ly, *w3.circle, 400)
-    th, rh = best_s(lambda: cfsb.circle_setup(*geo))
-    td, rd = best_s(lambda: cfsb.circle_setup(*geo, device=0))
-    out["ib_setup_2048x1024"] = {"host_ms": round(th * 1e3, 2), "device_ms": round(td * 1e3, 2),
-                                 "ghost_cells": int(rh[1].size),
-                                 "identical": all(np.array_equal(a, b) for a, b in zip(rh, rd)),
-                                 "timing": "host wall clock, best of 3, both through the C ABI with host outputs"}
-    cases, states = wl.batch_cases(args.cases, seed=1)
-    res = {}
-    for prec in (cfsb.FP64, cfsb.FP32_MIXED):
-        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR) as b:
-            for k, U in enumerate(states):
-                b.set_state(k, U)
-            b.advance(100, cfl=0.5)
-            res[prec] = [b.get_state(k) for k in range(len(cases))]
+    parts = args.report_parts.split(",")
+    if "quadrants" in parts:
+        compare("quadrants_256_reference_scheme", wl.riemann_quadrants(256, 256, seed=1), 200, 0.5,
+                dict(rk=cfsb.RK_TVD3_REFERENCE, hll=cfsb.HLL_REFERENCE), exact=True)
+    if "cylinder" in parts:
+        w3 = wl.mach3_cylinder(2048, 1024)
+        compare("mach3_cylinder_2048x1024", w3, 3000, 0.5,
+                dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, positivity=cfsb.POSITIVITY_FLOOR),
+                circle=w3.circle, ib_mode=cfsb.IB_BILINEAR_SLIP)
+
+        def best_s(fn, reps=3):
+            best = None
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                r = fn()
+                dt = time.perf_counter() - t0
+                best = dt if best is None or dt < best else best
+            return best, r
+        geo = (w3.nx, w3.ny, w3.lx, w3.ly, *w3.circle, 400)
+        th, rh = best_s(lambda: cfsb.circle_setup(*geo))
+        td, rd = best_s(lambda: cfsb.circle_setup(*geo, device=0))
+        out["ib_setup_2048x1024"] = {"host_ms": round(th * 1e3, 2), "device_ms": round(td * 1e3, 2),
+                                     "ghost_cells": int(rh[1].size),
+                                     "identical": all(np.array_equal(a, b) for a, b in zip(rh, rd)),
+                                     "timing": "host wall clock, best of 3, both through the C ABI with host outputs"}
+    if "shear" in parts:
+        w4 = wl.shear_layer(1024)
+        compare("shear_layer_1024_ns", w4, 5000, 0.5,
+                dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, viscous=cfsb.VISCOUS_NS, mu=w4.meta["mu"], prandtl=0.72,
+                     mach=1.0), periodic=True)
+    if "batch" in parts:
+        out[f"batch_{args.cases}_cases_{args.batch_steps}_steps"] = _report_batch(cfsb, wl, args.cases, args.batch_steps)
+    if "convergence" in parts:
+        out["convergence_smooth_advection"] = _report_convergence(cfsb, wl, args.conv_max)
+    print(json.dumps(out), flush=True)
+
+
+def _report_batch(cfsb, wl, ncases: int, steps: int) -> dict:
+    """The uneven batch: FP64 with per-case CFL steps (one advance call per
+    step, each case's dt recorded), FP32-mixed replaying every case's dt
+    sequence; worst case over the cases at t_end."""
+    cases, states = wl.batch_cases(ncases, seed=1)
+    kw = dict(positivity=cfsb.POSITIVITY_FLOOR)
+    with cfsb.Batch(cases, precision=cfsb.FP64, **kw) as b:
+        for k, U in enumerate(states):
+            b.set_state(k, U)
+        seq = []
+        for _ in range(steps):
+            b.advance(1, cfl=0.5)
+            seq.append(b.dt_last())
+        t64 = np.sum(seq, axis=0)
+        U64 = [b.get_state(k) for k in range(len(cases))]
+    with cfsb.Batch(cases, precision=cfsb.FP32_MIXED, **kw) as b:
+        for k, U in enumerate(states):
+            b.set_state(k, U)
+        t32 = np.zeros(len(cases))
+        for d in seq:
+            t32 += b.advance(1, dt=d)
+        U32 = [b.get_state(k) for k in range(len(cases))]
     worst = {"rho_L1": 0.0, "rho_Linf": 0.0, "E_L1": 0.0, "E_Linf": 0.0}
+    l1 = []
     finite = True
-    for a, b in zip(res[cfsb.FP32_MIXED], res[cfsb.FP64]):
-        e = _errors(a, b)
-        finite = finite and bool(np.all(np.isfinite(a)) and np.all(np.isfinite(b)))
+    for a, c in zip(U32, U64):
+        e = _errors(a, c)
+        l1.append(e["rho_L1"])
+        finite = finite and bool(np.all(np.isfinite(a)) and np.all(np.isfinite(c)))
         for k in worst:
             worst[k] = max(worst[k], e[k])
-    out["batch_512_cases_100_steps"] = {"worst_case_fp32_vs_fp64": worst, "finite": finite}
-    print(json.dumps(out), flush=True)
+    l1 = np.array(l1)
+    half = len(cases) // 2
+    return {"worst_case_fp32_vs_fp64": worst, "finite": finite, "steps": steps,
+            "rho_L1_median": float(np.median(l1)),
+            "rho_L1_worst_quadrant_case": float(l1[:half].max()), "rho_L1_worst_cylinder_case": float(l1[half:].max()),
+            "cases_over_1e-5": int((l1 > 1e-5).sum()),
+            "same_t_end": bool(np.allclose(t32, t64, rtol=1e-12, atol=0.0)),
+            "dt_sequence": "per case: FP64 CFL steps, replayed by the FP32 batch (cfs_batch_advance_dt)"}
+
+
+def _report_convergence(cfsb, wl, nmax: int) -> dict:
+    """Smooth periodic advection to t = 0.5 at CFL <= 0.4 (fixed dt = 0.5 /
+    ceil(0.5 / dt_CFL), so t_end is exact), SSP-RK3, Davis HLL, WENO5 eps 1e-2:
+    density L1 error against the exact cell averages per N, FP64 and FP32, the
+    observed order log2(e(N/2) / e(N)), and FP32 vs FP64."""
+    rows = []
+    kw = dict(rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS, bc=(cfsb.BC_PERIODIC,) * 4)
+    n = 128
+    prev = None
+    while n <= nmax:
+        w = wl.smooth_advection(n)
+        with cfsb.Solver(n, n, precision=cfsb.FP64, **kw) as s:
+            s.set_state(w.U0)
+            dt0 = s.compute_dt(w.cfl)
+        nsteps = int(math.ceil(w.t_end / dt0))
+        dt = w.t_end / nsteps
+        exact = wl.smooth_advection_exact(n, w.t_end)
+        res = {}
+        for prec, key in ((cfsb.FP64, "fp64"), (cfsb.FP32_MIXED, "fp32")):
+            with cfsb.Solver(n, n, precision=prec, **kw) as s:
+                s.set_state(w.U0)
+                m0 = s.totals()
+                s.advance(nsteps, dt=dt)
+                U = s.get_state()
+                m1 = s.totals()
+            res[key] = (U, float(np.abs(U[0] - exact).mean()), float(abs(m1[0] - m0[0]) / abs(m0[0])))
+        row = {"n": n, "steps": nsteps, "dt": dt,
+               "rho_L1_fp64_vs_exact": res["fp64"][1], "rho_L1_fp32_vs_exact": res["fp32"][1],
+               "rho_L1_fp32_vs_fp64": float(np.abs(res["fp32"][0][0] - res["fp64"][0][0]).mean()),
+               "rho_Linf_fp32_vs_fp64": float(np.abs(res["fp32"][0][0] - res["fp64"][0][0]).max()),
+               "mass_drift_fp64": res["fp64"][2], "mass_drift_fp32": res["fp32"][2]}
+        if prev is not None:
+            row["order_fp64"] = math.log2(prev["rho_L1_fp64_vs_exact"] / row["rho_L1_fp64_vs_exact"])
+            row["order_fp32"] = math.log2(prev["rho_L1_fp32_vs_exact"] / row["rho_L1_fp32_vs_exact"])
+        rows.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+        prev = row
+        n *= 2
+    return {"rows": rows, "scheme": "SSP-RK3, Davis HLL, WENO5 eps 1e-2 (Weno5th.cpp:5), CFL <= 0.4, t = 0.5"}
 
 
 # ----------------------------------------------------------- reference arm
@@ -798,7 +915,8 @@ def modes_arm(args):
         w = wl.shear_layer(n) if ns else quads
         extra = dict(viscous=cfsb.VISCOUS_NS, mu=w.meta["mu"], prandtl=0.72, mach=1.0) if ns else {}
         with cfsb.Solver(n, n, 1.0, 1.0, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
-                         bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos), **extra) as s:
+                         bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos), variant=args.variant,
+                         **extra) as s:
             if cyl:
                 s.build_circle(0.1, 0.5, 0.5, 400, cfsb.IB_BILINEAR_SLIP)
             s.set_state(w.U0)
@@ -842,6 +960,11 @@ def main():
                     help="reference arm: tile edge per host core (0 = tiles summing to n^2 cells)")
     ap.add_argument("--modes-n", type=int, default=2048, help="grid edge of the modes workload")
     ap.add_argument("--mode", choices=list(MODES), default=None, help="modes workload: run this mode only (FP32)")
+    ap.add_argument("--variant", type=int, default=0, help="modes workload: stage-kernel variant (0 = default)")
+    ap.add_argument("--report-parts", default="quadrants,cylinder,shear,batch,convergence",
+                    help="report workload: comma-separated parts to run")
+    ap.add_argument("--batch-steps", type=int, default=500, help="report workload: steps of the batch comparison")
+    ap.add_argument("--conv-max", type=int, default=4096, help="report workload: largest N of the convergence table")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -336,8 +336,19 @@ const char* cfs_batch_last_error(const cfs_batch* b);
 int cfs_batch_set_state(cfs_batch* b, int c, const double* U);
 int cfs_batch_get_state(cfs_batch* b, int c, double* U);
 /* nsteps RK steps of every case with per-case CFL dt (cfl > 0) or a common
- * fixed dt; t (optional, [ncases]) receives each case's simulated time. */
+ * fixed dt; t (optional, [ncases]) receives each case's simulated time.
+ * With cfl > 0, a fluid cell of some case that turns non-finite gives
+ * CFS_ERR_NUMERIC (its CFL maximum becomes +infinity). */
 int cfs_batch_advance(cfs_batch* b, int nsteps, double cfl, double dt, double* t);
+/* nsteps RK steps with a fixed dt per case (dt_case[ncases], finite and
+ * positive): replays another run's time steps, e.g. an FP64 batch's CFL steps
+ * on an FP32-mixed batch of the same cases.  t as cfs_batch_advance. */
+int cfs_batch_advance_dt(cfs_batch* b, int nsteps, const double* dt_case, double* t);
+/* Per case, the dt of the last step taken (dt[ncases]; 0 before any step). */
+int cfs_batch_dt_last(const cfs_batch* b, double* dt);
+/* The batch's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against it. */
+void* cfs_batch_get_stream(cfs_batch* b);
 /* The batch's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against it. */
 void* cfs_batch_get_stream(cfs_batch* b);

@@ -37,3 +37,30 @@ def test_batch_rejects_exact_form(cfsb, workloads):
     cases, _ = workloads.batch_cases(2, seed=1, sizes=[32])
     with pytest.raises(cfsb.CfsError):
         cfsb.Batch(cases, precision=cfsb.FP64_EXACT)
+
+
+def test_batch_replays_a_dt_sequence_per_case(cfsb, workloads):
+    """cfs_batch_dt_last records each case's CFL step; cfs_batch_advance_dt
+    replays those steps on a second batch of the same cases and form: the
+    states are equal bit for bit and every case reaches the same time."""
+    cases, states = workloads.batch_cases(12, seed=3, sizes=[64, 96, 128])
+    kw = dict(precision=cfsb.FP64, positivity=cfsb.POSITIVITY_FLOOR)
+    with cfsb.Batch(cases, **kw) as b:
+        for k, U in enumerate(states):
+            b.set_state(k, U)
+        seq, t_ref = [], np.zeros(len(cases))
+        for _ in range(5):
+            t_ref += b.advance(1, cfl=0.5)
+            seq.append(b.dt_last())
+        ref = [b.get_state(k) for k in range(len(cases))]
+    assert np.all(np.array(seq) > 0)
+    assert np.any(np.array(seq)[0] != np.array(seq)[0][0])  # the cases keep their own dt
+    with cfsb.Batch(cases, **kw) as b:
+        for k, U in enumerate(states):
+            b.set_state(k, U)
+        t = np.zeros(len(cases))
+        for d in seq:
+            t += b.advance(1, dt=d)
+        for k in range(len(cases)):
+            assert np.array_equal(b.get_state(k), ref[k])
+    assert np.array_equal(t, t_ref)

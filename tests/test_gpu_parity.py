@@ -169,6 +169,49 @@ def test_fp64_per_step_relative_linf(cfsb, workloads, rk, hll, bc):
     assert worst <= 1e-12, worst
 
 
+@pytest.fixture(scope="module")
+def c1_oracle_run(workloads):
+    """The four-quadrant configuration at its own size (256^2, seed 1, TVD3 as
+    written, reference HLL, transmissive sides, CFL 0.5): the oracle's 200
+    steps (600 stages) with their dt."""
+    w = workloads.riemann_quadrants(256, 256, seed=1)
+    U, dts = ob.orc_run(ob.make_orc_config(256, 256), w.U0, 1, 600, cfl=0.5)
+    return w, U, dts
+
+
+def test_exact_form_is_bitwise_the_oracle_over_the_quadrant_configuration(cfsb, c1_oracle_run):
+    """CFS_FP64_EXACT through the stage API, 600 loop iterations with the CFL
+    dt at each step start: every dt and the final state equal the oracle's bit
+    for bit (the oracle equals the reference's own classes, test_oracle.py)."""
+    w, ref, ref_dt = c1_oracle_run
+    with cfsb.Solver(256, 256, precision=cfsb.FP64_EXACT) as s:
+        s.set_state(w.U0)
+        dts = run_counters(s, 1, 600, cfl=0.5)
+        got = s.get_state()
+    assert np.array_equal(dts, ref_dt)
+    assert np.array_equal(got, ref, equal_nan=True)
+
+
+def test_fp64_per_step_on_the_quadrant_configuration(cfsb, c1_oracle_run):
+    """CFS_FP64 at 256^2, all 200 steps: each step started from the oracle's
+    state with the oracle's dt, relative L-infinity <= 1e-12 per step."""
+    w, _, _ = c1_oracle_run
+    cfg = ob.make_orc_config(256, 256)
+    U = w.U0.copy()
+    worst = 0.0
+    with cfsb.Solver(256, 256, precision=cfsb.FP64) as s:
+        for _ in range(200):
+            dt = ob.orc_cfl_dt(cfg, U, 0.5)
+            s.set_state(U)
+            s.step(dt)
+            got = s.get_state()
+            ref, _ = ob.orc_run(cfg, U, 1, 3, dt=dt)
+            assert np.all(np.isfinite(ref))
+            worst = max(worst, _rel_linf(got, ref))
+            U = ref
+    assert worst <= 1e-12, worst
+
+
 def test_fp64_full_quadrant_run_tracks_oracle(cfsb, workloads):
     """256^2 quadrant configuration, 200 steps at CFL 0.5: the FP64 form stays
     within 1e-9 relative of the oracle over the whole run (per-step error 1e-15
