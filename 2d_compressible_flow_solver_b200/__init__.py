@@ -147,7 +147,6 @@ _SIGNATURES = {
     "cfs_batch_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          _c_double_p]),
     "cfs_batch_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
-    "cfs_batch_get_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "cfs_batch_advance_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p]),
     "cfs_batch_dt_last": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "cfs_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
@@ -569,8 +568,4 @@ class Batch:
         self._check(self._lib.cfs_batch_dt_last(self._b, _dp(d)))
         return d
 
-    @property
-    def stream(self) -> int:
-        """The batch's cudaStream_t as an integer handle."""
-        return int(self._lib.cfs_batch_get_stream(self._b) or 0)
 

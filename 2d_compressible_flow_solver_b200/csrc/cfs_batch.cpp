@@ -445,8 +445,6 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
 
 void* cfs_batch_get_stream(cfs_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
 
-void* cfs_batch_get_stream(cfs_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
-
 int cfs_batch_info(const cfs_batch* b, long long* cells, int* items) {
     if (!b) return bfail(nullptr, CFS_ERR_INVALID, "null batch");
     if (cells) *cells = b->total_cells;

@@ -349,9 +349,6 @@ int cfs_batch_dt_last(const cfs_batch* b, double* dt);
 /* The batch's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against it. */
 void* cfs_batch_get_stream(cfs_batch* b);
-/* The batch's CUDA stream (a cudaStream_t), for callers that time or order
- * their own work against it. */
-void* cfs_batch_get_stream(cfs_batch* b);
 /* Total cells of the batch and the number of work items of one stage launch. */
 int cfs_batch_info(const cfs_batch* b, long long* cells, int* items);
 
