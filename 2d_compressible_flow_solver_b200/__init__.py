@@ -26,7 +26,7 @@ __all__ = [
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
     "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "POSITIVITY_FLOOR", "ROUND_STOCHASTIC",
-    "ROUND_NEAREST", "variants", "fp_peaks",
+    "ROUND_NEAREST", "PART_ALL", "PART_INTERIOR", "PART_EDGES", "variants", "fp_peaks",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -42,6 +42,7 @@ IB_REFERENCE, IB_BILINEAR_SLIP = 0, 1
 VISCOUS_OFF, VISCOUS_NS = 0, 1
 POSITIVITY_OFF, POSITIVITY_FACE, POSITIVITY_BODY, POSITIVITY_FLOOR = 0, 1, 2, 3
 ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
+PART_ALL, PART_INTERIOR, PART_EDGES = 0, 1, 2
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _c_int32_p = ctypes.POINTER(ctypes.c_int32)
@@ -131,6 +132,11 @@ _SIGNATURES = {
     "cfs_halo_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_halo_unpack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "cfs_set_storage_offsets": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "cfs_steps_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
+    "cfs_steps_stage": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cfs_cfl_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cfs_cfl_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cfs_steps_end": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p]),
     "cfs_get_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint), _c_double_p, _c_double_p]),
     "cfs_set_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double]),
     "cfs_conserved_totals": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
@@ -431,6 +437,26 @@ class Solver:
             self.set_storage_offsets(counters["offsets"])
         self.set_state(U)
         self._check(self._lib.cfs_set_step(self._ctx, int(counters["step"]), float(counters["cfl_max"])))
+
+    # -- device-ordered stepping (decomposed grids): see cfs_steps_* in cfs.h
+    def steps_begin(self, cfl: float = 0.0, dt: float = 0.0) -> None:
+        self._check(self._lib.cfs_steps_begin(self._ctx, float(cfl), float(dt)))
+
+    def steps_stage(self, part: int = PART_ALL) -> None:
+        self._check(self._lib.cfs_steps_stage(self._ctx, int(part)))
+
+    def cfl_export(self, dev_ptr: int) -> None:
+        self._check(self._lib.cfs_cfl_export(self._ctx, ctypes.c_void_p(dev_ptr)))
+
+    def cfl_import(self, dev_ptr: int) -> None:
+        self._check(self._lib.cfs_cfl_import(self._ctx, ctypes.c_void_p(dev_ptr)))
+
+    def steps_end(self):
+        """Waits for the run of steps; returns (simulated time, last dt)."""
+        t = ctypes.c_double(0.0)
+        dl = ctypes.c_double(0.0)
+        self._check(self._lib.cfs_steps_end(self._ctx, ctypes.byref(t), ctypes.byref(dl)))
+        return t.value, dl.value
 
     def halo_bytes(self) -> int:
         n = ctypes.c_longlong(0)

@@ -60,6 +60,11 @@ struct cfs_ctx {
     unsigned long long* wmax = nullptr;
     double* totals = nullptr;
     cudaGraphExec_t graph2 = nullptr;  // two full steps (parity 0 then 1)
+    // device-ordered stepping (cfs_steps_*): between begin and end
+    bool in_steps = false;
+    bool steps_cfl = false;
+    int steps_parity = 0;         // DevParams slot parity of the running step
+    int steps_part = 0;           // part of the current stage already enqueued (CFS_PART_*)
     std::string err;
 };
 
@@ -220,9 +225,9 @@ Roles roles_for(const cfs_ctx* c, int stage, int cur, int u0_idx, int u1_idx) {
 // Enqueues one stage (immersed-ghost fill + stage kernel).  P/parity/flags
 // select graph mode.
 int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_mode, int parity, bool first,
-                  bool last) {
-    if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[r.in]), c->stream));
-    if (c->rv) {
+                  bool last, int row_lo = 0, int row_hi = 0, bool with_fill = true) {
+    if (with_fill && c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[r.in]), c->stream));
+    if (c->rv && with_fill) {
         cfs::ViscArgs va{};
         va.in = c->S[r.in];
         va.rv = c->rv;
@@ -252,6 +257,8 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
     a.rhs = c->cfg.keep_rhs ? c->rhs : nullptr;
     a.stage = stage;
     a.dt = dt;
+    a.row_lo = row_lo;
+    a.row_hi = row_hi;
     if (graph_mode) {
         a.P = c->P;
         a.parity = parity;
@@ -859,6 +866,123 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
         // left the maximum of the final state in wmax[1 - parity]; it is
         // +infinity when a fluid cell of that state is non-finite
         c->wmax_bits = out.wmax[nsteps % 2 == 1 ? 1 : 0];
+        c->wmax_carry = c->wmax_bits != 0;
+        if (c->wmax_bits == 0x7ff0000000000000ull) return fail(c, CFS_ERR_NUMERIC, "a fluid cell became non-finite");
+    }
+    return CFS_OK;
+}
+
+// ---- device-ordered stepping of decomposed grids
+int cfs_steps_begin(cfs_ctx* c, double cfl, double dt) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (c->in_steps) return fail(c, CFS_ERR_STATE, "cfs_steps_begin inside a run of steps");
+    if (c->next_stage != 0) return fail(c, CFS_ERR_STATE, "a step is in progress (stage sequence not at stage 0)");
+    if (!(cfl > 0) && !(dt > 0)) return fail(c, CFS_ERR_INVALID, "give cfl > 0 or dt > 0");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    cfs::DevParams hp{};
+    hp.use_cfl = cfl > 0 ? 1 : 0;
+    hp.cfl = cfl;
+    hp.dt_fixed = dt;
+    hp.seed[0] = hp.seed[1] = c->steps_done;
+    const bool carry = hp.use_cfl && c->wmax_carry;
+    if (carry) hp.wmax[0] = c->wmax_bits;
+    CFS_CUDA(c, cudaMemcpyAsync(c->P, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+    if (hp.use_cfl && !carry) {
+        if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[c->cur]), c->stream));
+        CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[c->cur], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
+                                     c->dx, c->dy, reinterpret_cast<unsigned long long*>(c->P), c->stream));
+    }
+    c->wmax_carry = false;
+    c->in_steps = true;
+    c->steps_cfl = hp.use_cfl != 0;
+    c->steps_parity = 0;
+    c->steps_part = CFS_PART_ALL;
+    return CFS_OK;
+}
+
+int cfs_steps_stage(cfs_ctx* c, int part) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (!c->in_steps) return fail(c, CFS_ERR_STATE, "cfs_steps_stage outside cfs_steps_begin / cfs_steps_end");
+    if (part != CFS_PART_ALL && part != CFS_PART_INTERIOR && part != CFS_PART_EDGES)
+        return fail(c, CFS_ERR_INVALID, "unknown stage part");
+    const bool split = part != CFS_PART_ALL;
+    if (split && (c->prec == cfs::kF64Exact || c->rv || c->ib_n > 0 || c->cfg.nx < 2 * cfs::kGhost))
+        return fail(c, CFS_ERR_INVALID, "interior/edge parts need a throughput form, no viscous terms, no immersed "
+                                        "boundary and nx >= 6");
+    if (part == CFS_PART_EDGES && c->steps_part != CFS_PART_INTERIOR)
+        return fail(c, CFS_ERR_STATE, "the edge part follows the interior part of the same stage");
+    if (part != CFS_PART_EDGES && c->steps_part == CFS_PART_INTERIOR)
+        return fail(c, CFS_ERR_STATE, "the interior part of this stage awaits its edge part");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    const int S = stages_per_step(c->cfg.rk);
+    const int stage = c->next_stage;
+    const Roles r = roles_for(c, stage, c->cur, c->u0_idx, c->u1_idx);
+    // the step's first-stage bookkeeping (t, dt, CFL slot reset) runs in
+    // exactly one launch: the full stage or its interior part; the
+    // immersed-ghost fill and viscous RHS run with the full stage only (the
+    // split parts refuse both above)
+    const bool first = stage == 0 && part != CFS_PART_EDGES;
+    const bool last = stage == S - 1;
+    if (part == CFS_PART_ALL) {
+        const int rc = enqueue_stage(c, stage, r, 0.0, true, c->steps_parity, first, last, 0, 0, true);
+        if (rc != CFS_OK) return rc;
+    } else if (part == CFS_PART_INTERIOR) {
+        const int rc = enqueue_stage(c, stage, r, 0.0, true, c->steps_parity, first, last, cfs::kGhost,
+                                     c->cfg.nx - cfs::kGhost, false);
+        if (rc != CFS_OK) return rc;
+    } else {
+        int rc = enqueue_stage(c, stage, r, 0.0, true, c->steps_parity, first, last, 0, cfs::kGhost, false);
+        if (rc == CFS_OK)
+            rc = enqueue_stage(c, stage, r, 0.0, true, c->steps_parity, first, last, c->cfg.nx - cfs::kGhost,
+                               c->cfg.nx, false);
+        if (rc != CFS_OK) return rc;
+    }
+    c->steps_part = part;
+    if (part == CFS_PART_INTERIOR) return CFS_OK;
+    if (stage == 0) c->u0_idx = r.u0;
+    if (stage == 1) c->u1_idx = r.u1;
+    c->cur = r.out;
+    c->next_stage = (stage + 1) % S;
+    if (c->next_stage == 0) {
+        ++c->steps_done;
+        c->steps_parity ^= 1;
+    }
+    return CFS_OK;
+}
+
+int cfs_cfl_export(cfs_ctx* c, void* dev_dst) {
+    if (!c || !dev_dst) return fail(c, CFS_ERR_INVALID, "null argument");
+    if (!c->in_steps || c->next_stage != 0) return fail(c, CFS_ERR_STATE, "the CFL slot is exchanged between steps");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    CFS_CUDA(c, cudaMemcpyAsync(dev_dst, &c->P->wmax[c->steps_parity], sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    return CFS_OK;
+}
+
+int cfs_cfl_import(cfs_ctx* c, const void* dev_src) {
+    if (!c || !dev_src) return fail(c, CFS_ERR_INVALID, "null argument");
+    if (!c->in_steps || c->next_stage != 0) return fail(c, CFS_ERR_STATE, "the CFL slot is exchanged between steps");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    CFS_CUDA(c, cudaMemcpyAsync(&c->P->wmax[c->steps_parity], dev_src, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    return CFS_OK;
+}
+
+int cfs_steps_end(cfs_ctx* c, double* t_elapsed, double* dt_last) {
+    if (!c) return fail(c, CFS_ERR_INVALID, "null context");
+    if (!c->in_steps) return fail(c, CFS_ERR_STATE, "cfs_steps_end without cfs_steps_begin");
+    if (c->next_stage != 0) return fail(c, CFS_ERR_STATE, "a step is in progress (stage sequence not at stage 0)");
+    CFS_CUDA(c, cudaSetDevice(c->cfg.device));
+    cfs::DevParams out{};
+    CFS_CUDA(c, cudaMemcpyAsync(&out, c->P, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->in_steps = false;
+    if (t_elapsed) *t_elapsed = out.t;
+    if (dt_last) *dt_last = out.dt_last;
+    if (out.t > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
+        return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
+    if (c->steps_cfl && out.t > 0) {
+        c->wmax_bits = out.wmax[c->steps_parity];
         c->wmax_carry = c->wmax_bits != 0;
         if (c->wmax_bits == 0x7ff0000000000000ull) return fail(c, CFS_ERR_NUMERIC, "a fluid cell became non-finite");
     }

@@ -100,7 +100,14 @@ struct StageArgs {
                            // i = -1..nx, j = -1..ny, [nx+2][ny+2]; null = all fluid, no low-order faces
     void* bflux;           // throughput forms: fluxes through the physical boundary faces
                            // (bflux_side_offset), arithmetic type of the form
+    int row_lo, row_hi;    // throughput forms: the launch updates cells of rows [row_lo, row_hi)
+                           // (row_hi 0: up to nx); a decomposed grid updates its interior
+                           // rows while the halo exchange is in flight, then its edge rows
 };
+
+// Rows [lo, hi) a stage launch updates.
+CFS_HD int stage_row_lo(const StageArgs& a) { return a.row_lo; }
+CFS_HD int stage_row_hi(const StageArgs& a) { return a.row_hi > 0 ? a.row_hi : a.L.nx; }
 
 // Bits of StageArgs::cflags.  The x-faces of cell (i, j) are (i-1/2, j) (lo)
 // and (i+1/2, j) (hi), its y-faces (i, j-1/2) and (i, j+1/2); a low-order face

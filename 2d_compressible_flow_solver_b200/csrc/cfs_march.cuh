@@ -413,8 +413,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     const int lane = threadIdx.x & 31;
     const int seg = bx * kWarps + wid;
     const int j0 = seg * kSeg;
-    const int i0 = by * rows;
-    const int i1 = min(i0 + rows, L.nx);
+    const int i0 = stage_row_lo(a) + by * rows;
+    const int i1 = min(i0 + rows, stage_row_hi(a));
     const int j = j0 - 1 + lane;                 // this lane's column
     const bool col_ok = j <= L.ny + kGhost - 1;  // inside the padded row
     const bool owner = lane >= 1 && lane <= kSeg && j < L.ny;  // updates cells of this column

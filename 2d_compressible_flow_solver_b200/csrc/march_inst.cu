@@ -18,7 +18,9 @@ namespace {
 template <class Pol, int R, int W, int B, int Ld, int F>
 cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     const int nseg = (a.L.ny + kSeg - 1) / kSeg;
-    const dim3 grid((nseg + W - 1) / W, (a.L.nx + R - 1) / R);
+    const int nrows = stage_row_hi(a) - stage_row_lo(a);
+    if (nrows <= 0) return cudaSuccess;
+    const dim3 grid((nseg + W - 1) / W, (nrows + R - 1) / R);
     size_t dyn = 0;
     if constexpr (Ld == 3 && sizeof(typename Pol::T) == 8) {
         // the FP64 ring lives in dynamic shared memory; allow it once per

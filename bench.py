@@ -278,7 +278,9 @@ def engine_arm(args):
         peak, peak_kind = hbm_peak()
         bytes32 = WORDS_PER_CELL_STEP * 4 * cells * K
         achieved = bytes32 / (ms32 / 1e3) / 1e9
-        launches = 3 * K + 1 if world == 1 else 4 * K  # slabs: 3 stages + 1 CFL launch per step
+        # single grid: 3 stage launches per step + the first step's CFL
+        # reduction; slabs: per stage an interior and two edge launches
+        launches = 3 * K + 1 if world == 1 else 9 * K + 1
         per_launch_ms = ms32 / launches
         trf = MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH["f32"]
         fl = MEASURED_FLOPS_PER_CELL_STEP["f32"]
@@ -294,8 +296,8 @@ def engine_arm(args):
                        "cells_per_gpu": cells,
                        "kernel_variant": {"f32": variants[cfsb.FP32_MIXED], "f64": variants[cfsb.FP64]},
                        "parallelism": "single grid" if world == 1 else
-                       f"{world} slabs of {n}x{n} along x, 3-row halo exchange per stage (NCCL send/recv), "
-                       "global CFL min per step",
+                       f"{world} slabs of {n}x{n} along x, 3-row halo exchange per stage (NCCL send/recv on the "
+                       "engine's stream, overlapping the stage's interior rows), device-side global CFL max per step",
                        "l2": "inputs larger than L2 (3 state buffers of "
                              f"{4 * 4 * cells / 1e6:.0f} MB each)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",

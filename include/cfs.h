@@ -297,6 +297,35 @@ int cfs_set_storage_offsets(cfs_ctx* ctx, const double* off4);
 int cfs_get_step(cfs_ctx* ctx, unsigned int* step, double* cfl_max, double* off4);
 int cfs_set_step(cfs_ctx* ctx, unsigned int step, double cfl_max);
 
+/* Device-ordered stepping, for a grid decomposed over several contexts (the
+ * reference's MPI decomposition, CartesianParallel.cpp:3-60, whose halo
+ * exchange :172-427 posts Irecv/Isend per stage and waits).  Nothing here
+ * waits on the host between begin and end: dt comes from the device (CFL
+ * maximum fused into each step's last stage, as cfs_advance), and every call
+ * only enqueues work on the context's stream, so the caller orders its halo
+ * exchange (cfs_halo_pack/unpack and its own transfers) and the CFL
+ * reduction across contexts on that stream, or on streams it joins to it.
+ *   cfs_steps_begin: starts a run of steps with cfl > 0 (device CFL dt) or a
+ *     fixed dt; reduces the first step's CFL maximum unless one is carried.
+ *   cfs_steps_stage: enqueues the next stage of the running step (the stage
+ *     sequence of cfs_stage), or one part of it: CFS_PART_INTERIOR updates
+ *     rows 3 .. nx-4, which read no ghost row, so it may run while the ghost
+ *     rows of its input are still being exchanged; CFS_PART_EDGES then updates
+ *     rows 0..2 and nx-3..nx-1.  The parts need a throughput form, no viscous
+ *     terms, no immersed boundary and nx >= 6.
+ *   cfs_cfl_export / cfs_cfl_import: between steps, copy the CFL maximum the
+ *     next step will use (8 bytes, FP64 bits of a non-negative value, so an
+ *     integer MAX orders it) to / from caller device memory, ordered on the
+ *     stream: export, a MAX all-reduce over the contexts, import.
+ *   cfs_steps_end: waits for the stream; *t_elapsed and *dt_last as
+ *     cfs_advance; CFS_ERR_NUMERIC on a non-finite step or fluid cell. */
+enum cfs_stage_part { CFS_PART_ALL = 0, CFS_PART_INTERIOR = 1, CFS_PART_EDGES = 2 };
+int cfs_steps_begin(cfs_ctx* ctx, double cfl, double dt);
+int cfs_steps_stage(cfs_ctx* ctx, int part);
+int cfs_cfl_export(cfs_ctx* ctx, void* dev_dst);
+int cfs_cfl_import(cfs_ctx* ctx, const void* dev_src);
+int cfs_steps_end(cfs_ctx* ctx, double* t_elapsed, double* dt_last);
+
 /* Waits for the context's stream. */
 int cfs_synchronize(cfs_ctx* ctx);
 
