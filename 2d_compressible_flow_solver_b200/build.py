@@ -40,7 +40,7 @@ CU_UNITS = [
      [f"-DCFS_MARCH_POL={pol}", f"-DCFS_MARCH_FEAT={feat}", f"-DCFS_MARCH_FN=launch_march_{form}_{feat}"])
     for form, pol in (("f32", "PolF32"), ("f64", "PolF64")) for feat in range(8)
 ]
-CPP_SOURCES = ["cfs_api.cpp", "cfs_batch.cpp", "ib_setup.cpp"]
+CPP_SOURCES = ["cfs_api.cpp", "cfs_batch.cpp", "ib_setup.cpp", "tma_maps.cpp"]
 
 
 def _headers() -> list[Path]:

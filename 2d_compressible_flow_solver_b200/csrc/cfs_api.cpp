@@ -37,6 +37,9 @@ struct cfs_ctx {
     uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
     uint8_t* cflags_d = nullptr;  // [nx+2][ny+2] per-cell flags of the row march (with cell types)
     void* bflux = nullptr;        // boundary-face fluxes of the row march (physical sides)
+    bool has_tmaps = false;       // throughput forms: TMA tensor maps of S0, S1, S2 encoded
+    alignas(64) unsigned char tmaps[3][cfs::kTensorMapBytes] = {};
+    unsigned int* err_d = nullptr;   // device error flags (cfs::kErr* bits)
     unsigned int steps_done = 0;  // completed RK steps: the stochastic-rounding step counter
     // CFL maximum of the current state from the last stage of the last advance
     // (FP64 bits), reused by the next advance while nothing changed the state
@@ -185,7 +188,22 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.lowo = c->cfg.positivity >= CFS_POSITIVITY_BODY && c->has_types ? c->lowo_d : nullptr;
     a.cflags = c->has_types ? c->cflags_d : nullptr;
     a.bflux = c->bflux;
+    a.err = c->err_d;
     return a;
+}
+
+// Device error flags set by bounded waits in the kernels; read (and cleared)
+// at the calls that wait for the stream.
+int check_device_errors(cfs_ctx* c) {
+    unsigned int e = 0;
+    CFS_CUDA(c, cudaMemcpyAsync(&e, c->err_d, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (e != 0) {
+        CFS_CUDA(c, cudaMemsetAsync(c->err_d, 0, sizeof(unsigned int), c->stream));
+        return fail(c, CFS_ERR_CUDA, "a TMA row copy did not complete within its bounded wait (device flag " +
+                                         std::to_string(e) + ")");
+    }
+    return CFS_OK;
 }
 
 cfs::IbArgs ib_args(const cfs_ctx* c, void* U) {
@@ -254,6 +272,11 @@ int enqueue_stage(cfs_ctx* c, int stage, const Roles& r, double dt, bool graph_m
     a.u0 = r.u0 >= 0 ? c->S[r.u0] : nullptr;
     a.u1 = r.u1 >= 0 ? c->S[r.u1] : nullptr;
     a.out = c->S[r.out];
+    if (c->has_tmaps) {
+        a.has_tmaps = 1;
+        std::memcpy(a.tmap_in, c->tmaps[r.in], cfs::kTensorMapBytes);
+        if (r.u0 >= 0) std::memcpy(a.tmap_u0, c->tmaps[r.u0], cfs::kTensorMapBytes);
+    }
     a.rhs = c->cfg.keep_rhs ? c->rhs : nullptr;
     a.stage = stage;
     a.dt = dt;
@@ -460,11 +483,24 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
         cudaMemsetAsync(c->rhs, 0, hb, c->stream);
     }
     if (cudaMalloc(&c->P, sizeof(cfs::DevParams)) != cudaSuccess || cudaMalloc(&c->wmax, sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&c->totals, 4 * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&c->totals, 4 * sizeof(double)) != cudaSuccess || cudaMalloc(&c->err_d, sizeof(unsigned int)) != cudaSuccess) {
         c->err = "device allocation of the reduction slots failed";
         return bail(CFS_ERR_NOMEM);
     }
     cudaMemsetAsync(c->P, 0, sizeof(cfs::DevParams), c->stream);
+    cudaMemsetAsync(c->err_d, 0, sizeof(unsigned int), c->stream);
+    if (c->prec != cfs::kF64Exact) {
+        // tensor maps of the three state buffers (TMA load schedule), encoded
+        // on the host once (the buffers never move) and passed in each
+        // stage's argument block
+        for (int b = 0; b < 3; ++b) {
+            if (cfs::encode_state_map(c->S[b], c->L, c->tmaps[b]) != cudaSuccess) {
+                c->err = "tensor map encoding of the state buffers failed";
+                return bail(CFS_ERR_CUDA);
+            }
+        }
+        c->has_tmaps = true;
+    }
     for (int b = 0; b < 3; ++b) cfs::launch_ghost_fill(c->L.elem_bytes, c->S[b], c->L, c->sides, c->stream);
     // the clears and ghost fills above are checked here, at enqueue and at completion
     cudaError_t ie = cudaStreamSynchronize(c->stream);
@@ -496,6 +532,7 @@ int cfs_destroy(cfs_ctx* c) {
     cudaFree(c->P);
     cudaFree(c->wmax);
     cudaFree(c->totals);
+    cudaFree(c->err_d);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CFS_OK;
@@ -574,7 +611,7 @@ int cfs_get_state(cfs_ctx* c, double* U) {
     CFS_CUDA(c, cfs::launch_unpack(c->L.elem_bytes, c->S[c->cur], c->staging, c->L, c->stream));
     CFS_CUDA(c, cudaMemcpyAsync(U, c->staging, hb, cudaMemcpyDeviceToHost, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
-    return CFS_OK;
+    return check_device_errors(c);
 }
 
 int cfs_get_rhs(cfs_ctx* c, double* R) {
@@ -858,6 +895,7 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     if (t_elapsed) *t_elapsed = out.t;
     if (dt_last) *dt_last = out.dt_last;
     c->steps_done += static_cast<unsigned int>(nsteps);
+    if (const int rc = check_device_errors(c); rc != CFS_OK) return rc;
     if (nsteps > 0) c->wmax_carry = false;
     if (nsteps > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
         return fail(c, CFS_ERR_NUMERIC, "time step became non-finite or non-positive");
@@ -977,6 +1015,7 @@ int cfs_steps_end(cfs_ctx* c, double* t_elapsed, double* dt_last) {
     CFS_CUDA(c, cudaMemcpyAsync(&out, c->P, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
     c->in_steps = false;
+    if (const int rc = check_device_errors(c); rc != CFS_OK) return rc;
     if (t_elapsed) *t_elapsed = out.t;
     if (dt_last) *dt_last = out.dt_last;
     if (out.t > 0 && (!(out.dt_last > 0) || !std::isfinite(out.dt_last)))
@@ -993,30 +1032,26 @@ int cfs_synchronize(cfs_ctx* c) {
     if (!c) return fail(c, CFS_ERR_INVALID, "null context");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
-    return CFS_OK;
+    return check_device_errors(c);
 }
 
 void* cfs_get_stream(cfs_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
 
 int cfs_halo_bytes(cfs_ctx* c, long long* bytes) {
     if (!c || !bytes) return fail(c, CFS_ERR_INVALID, "null argument");
-    *bytes = static_cast<long long>(kVars) * cfs::kGhost * c->L.pitch * c->L.elem_bytes;
+    *bytes = cfs::kGhost * c->L.row_bytes();
     return CFS_OK;
 }
 
-// Rows are contiguous in the padded layout: one side's 3 rows of a plane are
-// 3 * pitch consecutive elements, so a message is 4 plain copies.
+// Rows hold whole cells and are contiguous in the padded layout: one side's 3
+// rows are one block of 3 * row_bytes, so a message is one plain copy.
 int cfs_halo_pack(cfs_ctx* c, int side, void* dst) {
     if (!c || !dst || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo pack arguments");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
-    const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
+    const size_t row_bytes = static_cast<size_t>(c->L.row_bytes());
     const int first = side == 0 ? 0 : c->cfg.nx - cfs::kGhost;
-    for (int v = 0; v < kVars; ++v) {
-        const char* src = static_cast<const char*>(c->S[c->cur]) +
-                          (static_cast<size_t>(v) * c->L.plane + static_cast<size_t>(first + cfs::kGhost) * c->L.pitch) * c->L.elem_bytes;
-        CFS_CUDA(c, cudaMemcpyAsync(static_cast<char*>(dst) + v * cfs::kGhost * row_bytes, src, cfs::kGhost * row_bytes,
-                                    cudaMemcpyDeviceToDevice, c->stream));
-    }
+    const char* src = static_cast<const char*>(c->S[c->cur]) + static_cast<size_t>(first + cfs::kGhost) * row_bytes;
+    CFS_CUDA(c, cudaMemcpyAsync(dst, src, cfs::kGhost * row_bytes, cudaMemcpyDeviceToDevice, c->stream));
     return CFS_OK;
 }
 
@@ -1024,14 +1059,10 @@ int cfs_halo_unpack(cfs_ctx* c, int side, const void* src) {
     if (!c || !src || (side != 0 && side != 1)) return fail(c, CFS_ERR_INVALID, "bad halo unpack arguments");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     c->wmax_carry = false;
-    const size_t row_bytes = static_cast<size_t>(c->L.pitch) * c->L.elem_bytes;
+    const size_t row_bytes = static_cast<size_t>(c->L.row_bytes());
     const int first = side == 0 ? -cfs::kGhost : c->cfg.nx;
-    for (int v = 0; v < kVars; ++v) {
-        char* dst = static_cast<char*>(c->S[c->cur]) +
-                    (static_cast<size_t>(v) * c->L.plane + static_cast<size_t>(first + cfs::kGhost) * c->L.pitch) * c->L.elem_bytes;
-        CFS_CUDA(c, cudaMemcpyAsync(dst, static_cast<const char*>(src) + v * cfs::kGhost * row_bytes, cfs::kGhost * row_bytes,
-                                    cudaMemcpyDeviceToDevice, c->stream));
-    }
+    char* dst = static_cast<char*>(c->S[c->cur]) + static_cast<size_t>(first + cfs::kGhost) * row_bytes;
+    CFS_CUDA(c, cudaMemcpyAsync(dst, src, cfs::kGhost * row_bytes, cudaMemcpyDeviceToDevice, c->stream));
     return CFS_OK;
 }
 

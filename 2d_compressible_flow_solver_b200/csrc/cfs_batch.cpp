@@ -109,7 +109,7 @@ int stages_of(int rk) { return rk == CFS_RK_TVD2 ? 2 : 3; }
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
 
 void* state_buf(const cfs_batch* b, const BatchCase& c, int k) {
-    return b->arena + c.state_off + static_cast<size_t>(k) * static_cast<size_t>(c.L.plane) * kVars * b->elem;
+    return b->arena + c.state_off + static_cast<size_t>(k) * static_cast<size_t>(c.L.bytes());
 }
 
 // Host images of the per-case stage and fill arguments (device copies in

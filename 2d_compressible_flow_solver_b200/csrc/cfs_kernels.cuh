@@ -29,6 +29,36 @@ __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
 __device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrtf(x); }
 __device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
 
+// One cell's four stored variables in vector accesses (one 16-byte access in
+// FP32, two in FP64; cells are 16- / 32-byte aligned in the interleaved layout).
+template <class T>
+__device__ __forceinline__ void ld_cell(const T* U, long long cell, T v[kVars]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(U + Layout::at(cell, 0));
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else {
+        const double2* q = reinterpret_cast<const double2*>(U + Layout::at(cell, 0));
+        const double2 a = q[0], b = q[1];
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+}
+template <class T>
+__device__ __forceinline__ void st_cell(T* U, long long cell, const T v[kVars]) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(U + Layout::at(cell, 0)) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        double2* q = reinterpret_cast<double2*>(U + Layout::at(cell, 0));
+        q[0] = make_double2(v[0], v[1]);
+        q[1] = make_double2(v[2], v[3]);
+    }
+}
+
 // State storage: FP64 holds the value; FP32 holds value - L.off[v].
 template <class T>
 __device__ __forceinline__ double dec(T stored, const Layout& L, int v) {
@@ -388,9 +418,7 @@ __device__ __forceinline__ C wave_sum_fast(C rho, C mx, C my, C E, C g, C inv_dx
 template <class T>
 __device__ __forceinline__ void store_cell4(T* out, const Layout& L, const int bc[4], int i, int j, const T val[kVars]) {
     if (i >= kGhost && i < L.nx - kGhost && j >= kGhost && j < L.ny - kGhost) {  // no ghost copies
-        const long long off = L.offset(i, j);
-#pragma unroll
-        for (int v = 0; v < kVars; ++v) out[v * L.plane + off] = val[v];
+        st_cell<T>(out, L.offset(i, j), val);
         return;
     }
     int xi[4], yj[4];
@@ -406,11 +434,7 @@ __device__ __forceinline__ void store_cell4(T* out, const Layout& L, const int b
     if (bc[2] == kPeriodic && j >= L.ny - kGhost) yj[nyj++] = j - L.ny;
     if (bc[3] == kPeriodic && j < kGhost) yj[nyj++] = j + L.ny;
     for (int a = 0; a < nxi; ++a)
-        for (int b = 0; b < nyj; ++b) {
-            const long long off = L.offset(xi[a], yj[b]);
-#pragma unroll
-            for (int v = 0; v < kVars; ++v) out[v * L.plane + off] = val[v];
-        }
+        for (int b = 0; b < nyj; ++b) st_cell<T>(out, L.offset(xi[a], yj[b]), val);
 }
 
 template <int NT>
@@ -461,9 +485,10 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
         const bool corner = (r < kGhost || r >= TI + kGhost) && (c < kGhost || c >= TJ + kGhost);
         const bool ok = !corner && i < L.nx + kGhost && j < L.ny + kGhost;
         if (ok) {
-            const long long off = L.offset(i, j);
+            T cv[kVars];
+            ld_cell<T>(in, L.offset(i, j), cv);
 #pragma unroll
-            for (int v = 0; v < kVars; ++v) sU[v][r][c] = decc<T, C>(in[v * L.plane + off], L, v);
+            for (int v = 0; v < kVars; ++v) sU[v][r][c] = decc<T, C>(cv[v], L, v);
         } else {
 #pragma unroll
             for (int v = 0; v < kVars; ++v) sU[v][r][c] = C(0);
@@ -536,7 +561,9 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
         const T* u1 = static_cast<const T*>(a.u1);
         T* out = static_cast<T*>(a.out);
         double nv[kVars];
-        T sv[kVars];
+        T sv[kVars], u0c[kVars] = {T(0), T(0), T(0), T(0)}, u1c[kVars] = {T(0), T(0), T(0), T(0)};
+        if (fluid && a.stage >= 1) ld_cell<T>(u0, off, u0c);
+        if (fluid && a.stage == 2 && a.rk == kRkTvd3Ref) ld_cell<T>(u1, off, u1c);
 #pragma unroll
         for (int v = 0; v < kVars; ++v) {
             double rv;
@@ -550,8 +577,8 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(const StageArgs a) {
             const double cur = double(sU[v][ti + kGhost][tj + kGhost]);
             double val = cur;
             if (fluid) {
-                const double u0v = a.stage >= 1 ? dec<T>(u0[v * L.plane + off], L, v) : 0.0;
-                const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
+                const double u0v = a.stage >= 1 ? dec<T>(u0c[v], L, v) : 0.0;
+                const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1c[v], L, v) : 0.0;
                 val = rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv);
             }
             sv[v] = enc<T>(val, L, v);
@@ -627,9 +654,10 @@ __global__ void __launch_bounds__(TI * TJ) viscous_kernel(const ViscArgs a) {
         const int i = i0 - kGhost + r, j = j0 - kGhost + c;
         C u = C(0), v = C(0), Tt = C(0);
         if (i < L.nx + kGhost && j < L.ny + kGhost) {
-            const long long off = L.offset(i, j);
-            const C rho = decc<T, C>(in[off], L, 0), mx = decc<T, C>(in[L.plane + off], L, 1);
-            const C my = decc<T, C>(in[2 * L.plane + off], L, 2), E = decc<T, C>(in[3 * L.plane + off], L, 3);
+            T cv[kVars];
+            ld_cell<T>(in, L.offset(i, j), cv);
+            const C rho = decc<T, C>(cv[0], L, 0), mx = decc<T, C>(cv[1], L, 1);
+            const C my = decc<T, C>(cv[2], L, 2), E = decc<T, C>(cv[3], L, 3);
             const C rinv = rcp_fast(rho);
             u = mx * rinv;
             v = my * rinv;
@@ -793,9 +821,10 @@ __device__ __forceinline__ void ib_fill_one(const IbArgs& a, int g) {
     for (int k = 0; k < 4; ++k) {
         const int d = a.donor[4 * g + k];
         const int i = d / L.ny, j = d - (d / L.ny) * L.ny;
-        const long long off = L.offset(i, j);
+        T cv[kVars];
+        ld_cell<T>(U, L.offset(i, j), cv);
 #pragma unroll
-        for (int v = 0; v < kVars; ++v) f[v][k] = dec<T>(U[v * L.plane + off], L, v);
+        for (int v = 0; v < kVars; ++v) f[v][k] = dec<T>(cv[v], L, v);
     }
     const double* fac = a.fac + 16 * g;
     double val[kVars];
@@ -839,9 +868,10 @@ __device__ __forceinline__ void ib_fill_one(const IbArgs& a, int g) {
         val[2] = val[2] - 2.0 * mn * ny_;
     }
     const int c = a.cell[g];
-    const long long off = L.offset(c / L.ny, c - (c / L.ny) * L.ny);
+    T sv[kVars];
 #pragma unroll
-    for (int v = 0; v < kVars; ++v) U[v * L.plane + off] = enc<T>(val[v], L, v);
+    for (int v = 0; v < kVars; ++v) sv[v] = enc<T>(val[v], L, v);
+    st_cell<T>(U, L.offset(c / L.ny, c - (c / L.ny) * L.ny), sv);
 }
 
 template <class T>
@@ -872,9 +902,10 @@ __global__ void __launch_bounds__(NT) wmax_kernel(const T* U, const Layout L, co
     for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
         if (types && types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
-        const long long off = L.offset(i, j);
-        const double w = cfl_term(wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1),
-                                           dec<T>(U[2 * L.plane + off], L, 2), dec<T>(U[3 * L.plane + off], L, 3), g, dx, dy));
+        T cv[kVars];
+        ld_cell<T>(U, L.offset(i, j), cv);
+        const double w = cfl_term(wave_sum(dec<T>(cv[0], L, 0), dec<T>(cv[1], L, 1), dec<T>(cv[2], L, 2),
+                                           dec<T>(cv[3], L, 3), g, dx, dy));
         if (w > m) m = w;
     }
     m = block_max<NT>(m, red);
@@ -894,10 +925,10 @@ __global__ void __launch_bounds__(NT) batch_wmax_kernel(const StageArgs* __restr
     for (long long k = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; k < n; k += static_cast<long long>(gridDim.x) * NT) {
         if (a.types && a.types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
-        const long long off = L.offset(i, j);
-        const double w = cfl_term(wave_sum(dec<T>(U[off], L, 0), dec<T>(U[L.plane + off], L, 1),
-                                           dec<T>(U[2 * L.plane + off], L, 2), dec<T>(U[3 * L.plane + off], L, 3), a.gamma,
-                                           a.dx, a.dy));
+        T cv[kVars];
+        ld_cell<T>(U, L.offset(i, j), cv);
+        const double w = cfl_term(wave_sum(dec<T>(cv[0], L, 0), dec<T>(cv[1], L, 1), dec<T>(cv[2], L, 2),
+                                           dec<T>(cv[3], L, 3), a.gamma, a.dx, a.dy));
         if (w > m) m = w;
     }
     m = block_max<NT>(m, red);
@@ -919,7 +950,7 @@ __global__ void __launch_bounds__(NT) totals_partial_kernel(const T* U, const La
     for (long long k = static_cast<long long>(blockIdx.x) * NT + threadIdx.x; k < n; k += static_cast<long long>(NB) * NT) {
         if (types && types[k] != 0) continue;
         const int i = static_cast<int>(k / L.ny), j = static_cast<int>(k - (k / L.ny) * L.ny);
-        s += dec<T>(U[v * L.plane + L.offset(i, j)], L, v);
+        s += dec<T>(U[Layout::at(L.offset(i, j), v)], L, v);
     }
     red[threadIdx.x] = s;
     __syncthreads();
@@ -940,7 +971,7 @@ __global__ void pack_kernel(const double* src, T* dst, const Layout L) {
         const int v = static_cast<int>(k / n);
         const long long c = k - v * n;
         const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
-        dst[v * L.plane + L.offset(i, j)] = enc<T>(src[k], L, v);
+        dst[Layout::at(L.offset(i, j), v)] = enc<T>(src[k], L, v);
     }
 }
 
@@ -952,7 +983,7 @@ __global__ void unpack_kernel(const T* src, double* dst, const Layout L) {
         const int v = static_cast<int>(k / n);
         const long long c = k - v * n;
         const int i = static_cast<int>(c / L.ny), j = static_cast<int>(c - (c / L.ny) * L.ny);
-        dst[k] = dec<T>(src[v * L.plane + L.offset(i, j)], L, v);
+        dst[k] = dec<T>(src[Layout::at(L.offset(i, j), v)], L, v);
     }
 }
 
@@ -980,7 +1011,7 @@ __device__ __forceinline__ bool ghost_value(const T* p, const Layout& L, const B
         else if (bc == kPeriodic) j = gj < 0 ? gj + L.ny : gj - L.ny;
         else return false;
     }
-    out = p[L.offset(i, j)];
+    out = p[Layout::at(L.offset(i, j), v)];
     return true;
 }
 
@@ -1019,9 +1050,8 @@ __global__ void ghost_fill_kernel(T* U, const Layout L, BcSides sides) {
             gi = (corner & 1) ? L.nx - 1 + lx : -lx;
             gj = (corner & 2) ? L.ny - 1 + ly : -ly;
         }
-        T* p = U + v * L.plane;
         T val;
-        if (ghost_value<T>(p, L, sides, v, gi, gj, val)) p[L.offset(gi, gj)] = val;
+        if (ghost_value<T>(U, L, sides, v, gi, gj, val)) U[Layout::at(L.offset(gi, gj), v)] = val;
     }
 }
 

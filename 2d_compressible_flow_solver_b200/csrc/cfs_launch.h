@@ -38,16 +38,24 @@ cudaError_t launch_weno_faces(Prec p, int n, const double* st, double* left, dou
 cudaError_t launch_hll_faces(Prec p, int n, int dir, const double* L, const double* R, double* F, double g,
                              int variant, cudaStream_t s);
 
+// TMA load schedule: one tensor map (CUtensorMap, 128 bytes, 64-byte
+// aligned) per state buffer, box of 4 variables x kTmaBoxCells cells x 1 row
+// (tma_maps.cpp; the row march's ring rows are that wide).
+constexpr int kTmaBoxCells = 36;
+constexpr int kTensorMapBytes = 128;
+cudaError_t encode_state_map(const void* base, const Layout& L, void* map);
+
 // Stage-kernel variants of the throughput forms (march_kernel template shapes).
 struct MarchVariant {
     int rows, warps, min_blocks;
     int load;  // load schedule of the row march: 0 at use, 1 early in the iteration, 2 rows ahead,
-               // 3 rows staged in shared memory by cp.async
+               // 3 rows staged in shared memory by cp.async, 4 rows staged by TMA
 };
-constexpr int kNumVariants = 10;
+constexpr int kNumVariants = 13;
 constexpr MarchVariant kVariants[kNumVariants] = {
     {64, 4, 1, 0}, {32, 4, 5, 0}, {64, 8, 2, 0}, {32, 4, 4, 1}, {64, 8, 2, 1},
     {32, 4, 5, 2}, {32, 4, 5, 3}, {32, 4, 4, 3}, {64, 4, 4, 3}, {32, 4, 6, 3},
+    {32, 4, 5, 4}, {32, 4, 4, 4}, {64, 4, 4, 4},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json).

@@ -1,13 +1,16 @@
 // Device grid layout and kernel argument blocks shared by the host code and the
 // kernels.  Plain C++ (no CUDA syntax) so that g++-compiled host files can use it.
 //
-// State: four planes (rho, rho u, rho v, E), each (nx + 6) rows of `pitch`
-// elements.  Row r = i + 3 holds x index i (i = -3 .. nx+2); element j of a
-// row (j = -3 .. ny+2) sits at column joff + j, where joff is one 128-byte block
-// so that every interior row starts 128-byte aligned.  The three ghost layers
-// per side are maintained by the kernels (Neumann copies, periodic wraps) or set
-// once (Dirichlet states), so a stage kernel reads a tile plus its 3-cell halo
-// with no boundary logic in the load path.
+// State: cells interleaved, (nx + 6) rows of `pitch` cells, each cell the four
+// conserved variables (rho, rho u, rho v, E) side by side -- one 16-byte
+// vector per cell in FP32, two in FP64.  Row r = i + 3 holds x index i
+// (i = -3 .. nx+2); cell j of a row (j = -3 .. ny+2) sits at column joff + j,
+// where joff is one 128-byte block so that every interior row starts 128-byte
+// aligned.  A stage reads and writes whole cells, so one vector access (or one
+// TMA box per row of a tile) moves all four variables.  The three ghost
+// layers per side are maintained by the kernels (Neumann copies, periodic
+// wraps) or set once (Dirichlet states), so a stage kernel reads a tile plus
+// its 3-cell halo with no boundary logic in the load path.
 #pragma once
 #include <cstdint>
 
@@ -26,10 +29,10 @@ enum BcKind : int { kNeumann = 0, kDirichlet = 1, kPeriodic = 2, kHalo = 3 };
 
 struct Layout {
     int nx, ny;
-    int pitch;           // elements per row
+    int pitch;           // cells per row
     int joff;            // column of j = 0
-    long long plane;     // elements per variable plane
-    int elem_bytes;      // 8 (FP64) or 4 (FP32)
+    long long cells;     // cells per state buffer ((nx + 6) * pitch)
+    int elem_bytes;      // bytes per variable: 8 (FP64) or 4 (FP32)
     // FP32 storage keeps value - off[v] (off = an FP32 value near the variable's
     // mean), so the rounding step of the stored state scales with the variation
     // of the field rather than its magnitude.  Always 0 for FP64 storage.
@@ -40,16 +43,19 @@ struct Layout {
         L.nx = nx;
         L.ny = ny;
         L.elem_bytes = elem_bytes;
-        const int blk = 128 / elem_bytes;
+        const int blk = 128 / (elem_bytes * kVars);  // cells per 128-byte block
         L.joff = blk;
         const int need = L.joff + ny + kGhost;
         L.pitch = ((need + blk - 1) / blk) * blk;
-        L.plane = static_cast<long long>(nx + 2 * kGhost) * L.pitch;
+        L.cells = static_cast<long long>(nx + 2 * kGhost) * L.pitch;
         for (int v = 0; v < 4; ++v) L.off[v] = 0.0f;
         return L;
     }
+    // cell index of (i, j) and element index of variable v of a cell
     CFS_HD long long offset(int i, int j) const { return static_cast<long long>(i + kGhost) * pitch + joff + j; }
-    long long bytes() const { return plane * kVars * elem_bytes; }
+    CFS_HD static long long at(long long cell, int v) { return cell * kVars + v; }
+    CFS_HD long long row_bytes() const { return static_cast<long long>(pitch) * kVars * elem_bytes; }
+    long long bytes() const { return cells * kVars * elem_bytes; }
 };
 
 // Boundary kinds of the four sides (left, right, bottom, top) and the
@@ -103,7 +109,18 @@ struct StageArgs {
     int row_lo, row_hi;    // throughput forms: the launch updates cells of rows [row_lo, row_hi)
                            // (row_hi 0: up to nx); a decomposed grid updates its interior
                            // rows while the halo exchange is in flight, then its edge rows
+    unsigned int* err;     // device error flags (kErr* bits), set instead of waiting forever
+    int has_tmaps;         // 1: tmap_in (and, stage >= 1, tmap_u0) hold encoded tensor maps
+    // TMA load schedule: tensor maps (CUtensorMap) of the `in` and `u0` buffers,
+    // box of 4 variables x 36 cells x 1 row.  Kernels that read them take the
+    // arguments as a __grid_constant__ parameter, so the copies address the
+    // maps in parameter space.
+    alignas(64) unsigned char tmap_in[128];
+    alignas(64) unsigned char tmap_u0[128];
 };
+
+// Bits of *StageArgs::err.
+constexpr unsigned int kErrTmaTimeout = 1u;  // a TMA copy did not land within its bounded wait
 
 // Rows [lo, hi) a stage launch updates.
 CFS_HD int stage_row_lo(const StageArgs& a) { return a.row_lo; }

@@ -31,17 +31,21 @@ constexpr int kSeg = 30;
 // correction (fewer operations, and in FP32 a rounding error relative to the
 // correction instead of to the value):
 //   beta_k (13/12) d_k^2 + (1/4) e_k^2 with d = (D2-D1, D3-D2, D4-D3),
-//     e = (3 D2 - D1, D2 + D3, D4 - 3 D3); scaled by 12/13 with eps alike, which
-//     leaves the normalised weights unchanged;
+//     e = (3 D2 - D1, D2 + D3, D4 - 3 D3) = (2 D2 + d0, D2 + D3, D4 - 3 D3);
+//     scaled by 12/13 with eps alike, which leaves the normalised weights
+//     unchanged;
 //   candidate p_k = v2 + c_k: c = ((5 D2 - 2 D1)/6, (D2 + 2 D3)/6, (4 D3 - D4)/6),
-//     mirrored c' = ((2 D4 - 5 D3)/6, -(D3 + 2 D2)/6, (D1 - 4 D2)/6);
+//     mirrored c' = ((2 D4 - 5 D3)/6, -(D3 + 2 D2)/6, (D1 - 4 D2)/6); each
+//     mirrored candidate is d/6 minus a left one: c'_0 = d2/6 - c_2,
+//     c'_1 = d1/6 - c_1, c'_2 = d0/6 - c_0, so the left ones are formed
+//     negated (n_k = -c_k) and the right ones take one fused multiply-add;
 //   weights d_k / q_k with q_k = (eps + beta_k)^2, taken as products of the
 //     other two q times (1, 6, 3) (the linear weights 0.1, 0.6, 0.3 times 10).
 template <class C>
 __device__ __forceinline__ void weno5_pair_diff(C v0, C v1, C v2, C v3, C v4, C eps, C& left, C& right) {
     const C D1 = v1 - v0, D2 = v2 - v1, D3 = v3 - v2, D4 = v4 - v3;
     const C d0 = D2 - D1, d1 = D3 - D2, d2 = D4 - D3;
-    const C e0 = fma(C(3), D2, -D1), e1 = D2 + D3, e2 = fma(C(-3), D3, D4);
+    const C e0 = fma(C(2), D2, d0), e1 = D2 + D3, e2 = fma(C(-3), D3, D4);
     const C k = C(3.0 / 13.0);
     C b0 = fma(d0, d0, k * (e0 * e0));
     C b1 = fma(d1, d1, k * (e1 * e1));
@@ -57,13 +61,13 @@ __device__ __forceinline__ void weno5_pair_diff(C v0, C v1, C v2, C v3, C v4, C 
     q2 *= q2;
     const C q01 = q0 * q1, q12 = q1 * q2, a1 = C(6) * (q0 * q2);
     const C a2L = C(3) * q01, a2R = C(3) * q12;
-    const C c0 = fma(C(5.0 / 6.0), D2, C(-1.0 / 3.0) * D1);
-    const C c1 = fma(C(1.0 / 3.0), D3, C(1.0 / 6.0) * D2);
-    const C c2 = fma(C(2.0 / 3.0), D3, C(-1.0 / 6.0) * D4);
-    const C r0 = fma(C(1.0 / 3.0), D4, C(-5.0 / 6.0) * D3);
-    const C r1 = fma(C(-1.0 / 3.0), D2, C(-1.0 / 6.0) * D3);
-    const C r2 = fma(C(1.0 / 6.0), D1, C(-2.0 / 3.0) * D2);
-    left = fma(fma(q12, c0, fma(a1, c1, a2L * c2)), rcp_fast(q12 + a1 + a2L), v2);
+    const C n0 = fma(C(-5.0 / 6.0), D2, C(1.0 / 3.0) * D1);
+    const C n1 = fma(C(-1.0 / 3.0), D3, C(-1.0 / 6.0) * D2);
+    const C n2 = fma(C(-2.0 / 3.0), D3, C(1.0 / 6.0) * D4);
+    const C r0 = fma(C(1.0 / 6.0), d2, n2);
+    const C r1 = fma(C(1.0 / 6.0), d1, n1);
+    const C r2 = fma(C(1.0 / 6.0), d0, n0);
+    left = fma(fma(q12, n0, fma(a1, n1, a2L * n2)), rcp_fast(-(q12 + a1 + a2L)), v2);
     right = fma(fma(q01, r0, fma(a1, r1, a2R * r2)), rcp_fast(q01 + a1 + a2R), v2);
 }
 
@@ -81,7 +85,7 @@ __device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, f
                                               float2& left, float2& right) {
     const float2 D1 = sub2(v1, v0), D2 = sub2(v2, v1), D3 = sub2(v3, v2), D4 = sub2(v4, v3);
     const float2 d0 = sub2(D2, D1), d1 = sub2(D3, D2), d2 = sub2(D4, D3);
-    const float2 e0 = fma2(p2(3.0f), D2, mul2(p2(-1.0f), D1)), e1 = add2(D2, D3), e2 = fma2(p2(-3.0f), D3, D4);
+    const float2 e0 = fma2(p2(2.0f), D2, d0), e1 = add2(D2, D3), e2 = fma2(p2(-3.0f), D3, D4);
     const float2 k = p2(float(3.0 / 13.0));
     float2 b0 = fma2(d0, d0, mul2(k, mul2(e0, e0)));
     float2 b1 = fma2(d1, d1, mul2(k, mul2(e1, e1)));
@@ -96,15 +100,15 @@ __device__ __forceinline__ void weno5_pair_x2(float2 v0, float2 v1, float2 v2, f
     q2 = mul2(q2, q2);
     const float2 q01 = mul2(q0, q1), q12 = mul2(q1, q2), a1 = mul2(p2(6.0f), mul2(q0, q2));
     const float2 a2L = mul2(p2(3.0f), q01), a2R = mul2(p2(3.0f), q12);
-    const float2 c0 = fma2(p2(float(5.0 / 6.0)), D2, mul2(p2(float(-1.0 / 3.0)), D1));
-    const float2 c1 = fma2(p2(float(1.0 / 3.0)), D3, mul2(p2(float(1.0 / 6.0)), D2));
-    const float2 c2 = fma2(p2(float(2.0 / 3.0)), D3, mul2(p2(float(-1.0 / 6.0)), D4));
-    const float2 r0 = fma2(p2(float(1.0 / 3.0)), D4, mul2(p2(float(-5.0 / 6.0)), D3));
-    const float2 r1 = fma2(p2(float(-1.0 / 3.0)), D2, mul2(p2(float(-1.0 / 6.0)), D3));
-    const float2 r2 = fma2(p2(float(1.0 / 6.0)), D1, mul2(p2(float(-2.0 / 3.0)), D2));
+    const float2 n0 = fma2(p2(float(-5.0 / 6.0)), D2, mul2(p2(float(1.0 / 3.0)), D1));
+    const float2 n1 = fma2(p2(float(-1.0 / 3.0)), D3, mul2(p2(float(-1.0 / 6.0)), D2));
+    const float2 n2 = fma2(p2(float(-2.0 / 3.0)), D3, mul2(p2(float(1.0 / 6.0)), D4));
+    const float2 sixth = p2(float(1.0 / 6.0));
+    const float2 r0 = fma2(sixth, d2, n2), r1 = fma2(sixth, d1, n1), r2 = fma2(sixth, d0, n0);
     const float2 sL = add2(add2(q12, a1), a2L), sR = add2(add2(q01, a1), a2R);
-    const float2 iL = make_float2(rcp_fast(sL.x), rcp_fast(sL.y)), iR = make_float2(rcp_fast(sR.x), rcp_fast(sR.y));
-    left = fma2(fma2(q12, c0, fma2(a1, c1, mul2(a2L, c2))), iL, v2);
+    // (the left reciprocals negated: the left sum is over the negated candidates)
+    const float2 iL = make_float2(rcp_fast(-sL.x), rcp_fast(-sL.y)), iR = make_float2(rcp_fast(sR.x), rcp_fast(sR.y));
+    left = fma2(fma2(q12, n0, fma2(a1, n1, mul2(a2L, n2))), iL, v2);
     right = fma2(fma2(q01, r0, fma2(a1, r1, mul2(a2R, r2))), iR, v2);
 }
 
@@ -199,24 +203,19 @@ __device__ __forceinline__ void boundary_face_states(const typename Pol::C c[kVa
     finish_state<Pol>(R, g);
 }
 
-// Asynchronous global -> shared copies (cp.async, sm_80+): 4 bytes each, zero
-// filled without reading when `valid` is false (gmem must still be a valid
-// address); completion per thread in commit groups.
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
+// Asynchronous global -> shared copies (cp.async, sm_80+): 16 bytes each,
+// bypassing L1, zero filled without reading when `valid` is false (gmem must
+// still be a valid address); completion per thread in commit groups.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    const int n = valid ? 4 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
 }
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    const int n = valid ? 8 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
-}
-// one element of the stored state, zero filled when not valid
+// one cell of the stored state (all four variables), zero filled when not valid
 template <class T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem, bool valid) {
-    if constexpr (sizeof(T) == 8) cp_async8(smem, gmem, valid);
-    else cp_async4(smem, gmem, valid);
+__device__ __forceinline__ void cp_async_cell(T* smem, const T* gmem, bool valid) {
+    cp_async16(smem, gmem, valid);
+    if constexpr (sizeof(T) == 8) cp_async16(smem + 2, gmem + 2, valid);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -225,17 +224,68 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Ring of staged rows of the row march (load schedule 3), per warp: kRingRows
-// rows of its 36 columns (the segment and 2 halo columns each side), stored
-// values, and (FP32 storage) the same rows of U^0 for its 32 lanes.  The FP64
-// ring leaves U^0 out (each lane loads it early in the row's iteration): its
-// rows of doubles would otherwise cost a fourth block per SM.
+// Ring of staged rows of the row march (load schedules 3 and 4), per warp:
+// kRingRows rows of its 36 columns (the segment and 2 halo columns each side,
+// whole cells), stored values, and (FP32 storage) the same 36 columns of the
+// rows of U^0 (lane l reads column l + 2).  The FP64 ring leaves U^0 out (each
+// lane loads it early in the row's iteration): its rows of doubles would
+// otherwise cost a fourth block per SM.
 constexpr int kRingRows = 8, kRingDist = 2;
-constexpr int kRingRowWords = 36 * kVars, kRingU0Words = 32 * kVars;
+constexpr int kRingCols = 36;
+constexpr int kRingRowWords = kRingCols * kVars, kRingU0Words = kRingCols * kVars;
 constexpr int kRingWords = kRingRows * (kRingRowWords + kRingU0Words);
 template <class T>
 __host__ __device__ constexpr int ring_words() {
     return sizeof(T) == 4 ? kRingWords : kRingRows * kRingRowWords;
+}
+
+// ---- TMA staging (load schedule 4).  One elected lane of a warp copies a
+// whole ring row -- the 4 variables of 36 cells, one box of the state
+// buffer's 3-D tensor map (variables, columns, rows) -- with one bulk tensor
+// copy that signals an mbarrier of the row's ring slot; the lanes wait on
+// that barrier instead of issuing per-lane copies.  The tensor maps travel in
+// the kernel's __grid_constant__ argument block (StageArgs::tmap_in,
+// tmap_u0) and cover this GPU's own state buffers only; no copy is
+// multicast.  Every wait is bounded: a copy that never lands sets
+// *StageArgs::err and ends the work item.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// try_wait suspends the thread for a system-dependent time per attempt; this
+// many attempts is far beyond any copy's latency (a row lands within a few
+// microseconds); the drain after a failure tries less
+constexpr int kMbarMaxTries = 1 << 20;
+constexpr int kMbarDrainTries = 1 << 14;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, int tries = kMbarMaxTries) {
+    for (int k = 0; k < tries; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// generic-proxy accesses of this thread (and, after a __syncwarp, of its warp)
+// before later async-proxy (TMA) writes to shared memory
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_load_row(unsigned dst, const void* tmap, int col, int row, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(dst), "l"(tmap), "r"(0), "r"(col), "r"(row), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_map(const void* tmap) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(tmap) : "memory");
 }
 
 // One column's 4 variables to / from the shared row buffer in vector accesses.
@@ -327,11 +377,13 @@ __device__ __forceinline__ void boundary_face_flux(const StageArgs& a, int s, in
         gj = s == 2 ? -1 : L.ny;
     }
     C c[kVars], gh[kVars];
-    const long long oc = L.offset(ii, jj), og = L.offset(gi, gj);
+    T cs[kVars], gs[kVars];
+    ld_cell<T>(in, L.offset(ii, jj), cs);
+    ld_cell<T>(in, L.offset(gi, gj), gs);
 #pragma unroll
     for (int v = 0; v < kVars; ++v) {
-        c[v] = decc<T, C>(in[v * L.plane + oc], L, v);
-        gh[v] = decc<T, C>(in[v * L.plane + og], L, v);
+        c[v] = decc<T, C>(cs[v], L, v);
+        gh[v] = decc<T, C>(gs[v], L, v);
     }
     const bool lo = s == 0 || s == 2;
     Face5<C> Lf, Rf;
@@ -399,12 +451,14 @@ __global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArg
 // instruction cache stalls every warp on instruction fetch, whatever the share
 // of the rare code actually executed.
 template <class Pol, int kWarps, int kLoad, int kFeat>
-__device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, int rows,
+__device__ __forceinline__ bool march_item(const StageArgs& a, int bx, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][36][kVars],
-                                           typename Pol::T* ring, int wid) {
+                                           typename Pol::T* ring, int wid, unsigned long long* bars = nullptr,
+                                           unsigned* phase = nullptr) {
     using T = typename Pol::T;
     using C = typename Pol::C;
-    constexpr bool kRing = kLoad == 3;
+    constexpr bool kTma = kLoad == 4;
+    constexpr bool kRing = kLoad >= 3;
     constexpr int kL = kLoad;
     constexpr bool kPos = (kFeat & kFeatPos) != 0;
     constexpr bool kExtra = (kFeat & kFeatExtra) != 0;
@@ -469,9 +523,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 
     auto load_row = [&](int r, C out[kVars]) {
         if (col_ok) {
-            const long long off = L.offset(r, j);
+            T cv[kVars];
+            ld_cell<T>(in, L.offset(r, j), cv);
 #pragma unroll
-            for (int v = 0; v < kVars; ++v) out[v] = decc<T, C>(in[v * L.plane + off], L, v);
+            for (int v = 0; v < kVars; ++v) out[v] = decc<T, C>(cv[v], L, v);
         } else {
 #pragma unroll
             for (int v = 0; v < kVars; ++v) out[v] = C(0);
@@ -482,9 +537,10 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         if (lane < 2 || lane >= 30) {  // halo columns j0-3, j0-2 and j0+31, j0+32
             const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
             if (hc <= L.ny + kGhost - 1) {
-                const long long off = L.offset(r, hc);
+                T cv[kVars];
+                ld_cell<T>(in, L.offset(r, hc), cv);
 #pragma unroll
-                for (int v = 0; v < kVars; ++v) h[v] = decc<T, C>(in[v * L.plane + off], L, v);
+                for (int v = 0; v < kVars; ++v) h[v] = decc<T, C>(cv[v], L, v);
             } else {
 #pragma unroll
                 for (int v = 0; v < kVars; ++v) h[v] = C(0);
@@ -510,11 +566,8 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     T pf_cur[kVars], pf_u0[kVars];
     auto load_update = [&](int i) {
         const long long off = L.offset(i, j);
-#pragma unroll
-        for (int v = 0; v < kVars; ++v) {
-            pf_cur[v] = Pol::kMixed ? in[v * L.plane + off] : T(0);
-            pf_u0[v] = a.stage >= 1 ? static_cast<const T*>(a.u0)[v * L.plane + off] : T(0);
-        }
+        if (Pol::kMixed) ld_cell<T>(in, off, pf_cur);
+        if (a.stage >= 1) ld_cell<T>(static_cast<const T*>(a.u0), off, pf_u0);
     };
 
     // Load schedule 3: this warp's ring (rows, and U^0 rows in FP32; ring_words).
@@ -526,29 +579,57 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     // Issue the copies of row q (the lane's column; halo lanes also their
     // halo column) and, for an updated row, of its U^0; one commit group per
     // row (empty past the last row needed, so group counts stay uniform).
+    // TMA: lane 0 copies the row's 36 cells (and U^0's) as one box each,
+    // completing on the slot's mbarrier.
+    constexpr unsigned kRowBytes = kRingCols * kVars * sizeof(T);
+    const int tcol = L.joff + j0 - 3;  // buffer column of ring column 0 (j0 - 3)
+    int issued = i0 - 4;               // TMA: rows <= issued have been issued
     auto issue_row = [&](int q) {
-        if constexpr (kRing) {
+        if constexpr (kTma) {
+            if (q > i1 + 2) return;
+            issued = q;
+            if (lane == 0) {
+                const bool u0row = kU0Ring && a.stage >= 1 && q >= i0 && q < i1;
+                const unsigned bar = smem_addr(bars + (q & (kRingRows - 1)));
+                fence_proxy_async_smem();
+                mbar_expect_tx(bar, u0row ? 2u * kRowBytes : kRowBytes);
+                tma_load_row(smem_addr(ring_row(q)), a.tmap_in, tcol, q + kGhost, bar);
+                if (u0row) tma_load_row(smem_addr(ring_u0(q)), a.tmap_u0, tcol, q + kGhost, bar);
+            }
+        } else if constexpr (kRing) {
             if (q <= i1 + 2) {
                 T* dst = ring_row(q);
                 const long long off = L.offset(q, col_ok ? j : 0);
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + (lane + 2) * kVars + v, in + v * L.plane + off, col_ok);
+                cp_async_cell<T>(dst + (lane + 2) * kVars, in + Layout::at(off, 0), col_ok);
                 if (lane < 2 || lane >= 30) {
                     const int hc = lane < 2 ? j0 - 3 + lane : j0 + 1 + lane;
                     const bool ok = hc <= L.ny + kGhost - 1;
                     const long long hoff = L.offset(q, ok ? hc : 0);
                     const int slot = lane < 2 ? lane : lane + 4;
-#pragma unroll
-                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(dst + slot * kVars + v, in + v * L.plane + hoff, ok);
+                    cp_async_cell<T>(dst + slot * kVars, in + Layout::at(hoff, 0), ok);
                 }
-                if (kU0Ring && a.stage >= 1 && q >= i0 && q < i1) {  // uniform: every lane fills its slot
-                    T* du = ring_u0(q);
-                    const T* u0p = static_cast<const T*>(a.u0);
-#pragma unroll
-                    for (int v = 0; v < kVars; ++v) cp_async_elem<T>(du + lane * kVars + v, u0p + v * L.plane + off, col_ok);
-                }
+                if (kU0Ring && a.stage >= 1 && q >= i0 && q < i1)  // uniform: every lane fills its slot
+                    cp_async_cell<T>(ring_u0(q) + (lane + 2) * kVars, static_cast<const T*>(a.u0) + Layout::at(off, 0),
+                                     col_ok);
             }
             cp_async_commit();
+        }
+    };
+    // TMA: wait until row q has landed in its slot (each row is waited on
+    // exactly once, in order, so one phase bit per slot tracks its fills)
+    bool tma_ok = true;
+    int waited = i0 - 4;  // rows <= waited have been waited on
+    auto wait_row = [&](int q) {
+        if constexpr (kTma) {
+            if (q > i1 + 2 || !tma_ok) return;
+            const int sl = q & (kRingRows - 1);
+            // warp-uniform outcome: every lane continues or every lane stops
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(smem_addr(bars + sl), (*phase >> sl) & 1u))) {
+                tma_ok = false;
+                return;
+            }
+            *phase ^= 1u << sl;
+            waited = q;
         }
     };
     // full value of a stencil cell (the ring holds stored deviations)
@@ -567,7 +648,11 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
     T rv_cur[3] = {T(0), T(0), T(0)}, rv_pf[3] = {T(0), T(0), T(0)};  // kExtra: viscous RHS of rows r-1, r
     double wloc = 0.0;
     if (active_warp && kRing) {
+        if constexpr (kTma) __syncwarp();  // a previous item's reads of the ring end before lane 0's copies
         for (int q = i0 - 3; q <= i0 + 1 + kRingDist; ++q) issue_row(q);
+        if constexpr (kTma) {
+            for (int q = i0 - 3; q <= i0; ++q) wait_row(q);  // the first iteration waits for row i0 + 1
+        }
     } else if (active_warp) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) load_row(i0 - 3 + k, win[k]);
@@ -581,11 +666,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         const unsigned int f_r = f_next;
         f_next = load_flags(r + 1);
         if constexpr (kRing && !kU0Ring) {  // FP64 ring: U^0 of row r-1, ahead of the x reconstruction
-            if (a.stage >= 1 && owner && r - 1 >= i0) {
-                const long long off = L.offset(r - 1, j);
-#pragma unroll
-                for (int v = 0; v < kVars; ++v) pf_u0[v] = static_cast<const T*>(a.u0)[v * L.plane + off];
-            }
+            if (a.stage >= 1 && owner && r - 1 >= i0) ld_cell<T>(static_cast<const T*>(a.u0), L.offset(r - 1, j), pf_u0);
         }
         if constexpr (kExtra) {  // viscous RHS of row r, a whole iteration ahead of its update
 #pragma unroll
@@ -601,8 +682,13 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             // now refilled held row r+3+kRingDist-kRingRows, last read at r-1
             __syncwarp();
             issue_row(r + 3 + kRingDist);
-            cp_async_wait<kRingDist + 1>();  // this lane's copies of rows <= r+2 have landed
-            __syncwarp();                    // ... and every lane's
+            if constexpr (kTma) {
+                wait_row(r + 2);  // rows <= r+2 have landed
+                if (!tma_ok) break;
+            } else {
+                cp_async_wait<kRingDist + 1>();  // this lane's copies of rows <= r+2 have landed
+                __syncwarp();                    // ... and every lane's
+            }
 #pragma unroll
             for (int k = 0; k < 5; ++k) {  // stored deviations; offsets added after the reconstruction
                 const T* src = ring_row(r - 2 + k) + (lane + 2) * kVars;
@@ -646,7 +732,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) pf_cur[v] = cs[v];
                     if constexpr (kU0Ring) {
-                        const T* us = ring_u0(i) + lane * kVars;
+                        const T* us = ring_u0(i) + (lane + 2) * kVars;
 #pragma unroll
                         for (int v = 0; v < kVars; ++v) pf_u0[v] = a.stage >= 1 ? us[v] : T(0);
                     }
@@ -654,9 +740,9 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                     load_update(i);
                 }
                 const bool fluid = !kEdge || !(f_prev & kCellSolid);
-                const long long off = L.offset(i, j);
-                const T* u1 = static_cast<const T*>(a.u1);
                 T* out = static_cast<T*>(a.out);
+                T u1c[kVars] = {T(0), T(0), T(0), T(0)};  // U^1 (TVD3 as written, stage 2 only)
+                if (a.stage == 2 && a.rk == kRkTvd3Ref) ld_cell<T>(static_cast<const T*>(a.u1), L.offset(i, j), u1c);
                 C nv[kVars];  // new state in the form's arithmetic type, for the CFL maximum
                 T sv[kVars];
                 if constexpr (Pol::kMixed) {
@@ -673,7 +759,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         if (kExtra && rv_in && v >= 1) rvf += rv_cur[v - 1];
                         const float cur = pf_cur[v];
                         const float x0 = a.stage == 0 ? cur : pf_u0[v];
-                        const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1[v * L.plane + off] : cur);
+                        const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1c[v] : cur);
                         float nd;
                         if (sr) {
                             const double tot = fma(cdtd, double(rvf), fma(double(cA), double(x0), double(cB) * double(x1)));
@@ -694,7 +780,7 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
                         if (kExtra && rv_in && v >= 1) rv += double(rv_cur[v - 1]);
                         const double cur = double(win[1][v]);
                         const double u0v = a.stage >= 1 ? dec<T>(pf_u0[v], L, v) : 0.0;
-                        const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1[v * L.plane + off], L, v) : 0.0;
+                        const double u1v = (a.stage == 2 && a.rk == kRkTvd3Ref) ? dec<T>(u1c[v], L, v) : 0.0;
                         const double val = fluid ? rk_update(a.rk, a.stage, dt, cur, u0v, u1v, rv) : cur;
                         sv[v] = enc<T>(val, L, v);
                         nv[v] = C(dec<T>(sv[v], L, v));
@@ -799,7 +885,21 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
             }
         }
     }
-    if constexpr (kRing) cp_async_wait_all();  // no copy into the ring outlives the item
+    if constexpr (kTma) {
+        if (!tma_ok) {
+            // a copy never landed: report it, and wait (bounded) for the
+            // copies still in flight so that none outlives the item
+            if (lane == 0) atomicOr(a.err, kErrTmaTimeout);
+            for (int q = waited + 1; q <= issued; ++q) {
+                const int sl = q & (kRingRows - 1);
+                if (__all_sync(0xffffffffu, mbar_wait_bounded(smem_addr(bars + sl), (*phase >> sl) & 1u, kMbarDrainTries)))
+                    *phase ^= 1u << sl;
+            }
+            return false;
+        }
+    } else if constexpr (kRing) {
+        cp_async_wait_all();  // no copy into the ring outlives the item
+    }
     // CFL maximum: one atomic per warp (no block barrier, so the warps of a
     // block never wait for each other)
     if (do_cfl) {
@@ -808,20 +908,55 @@ __device__ __forceinline__ void march_item(const StageArgs& a, int bx, int by, i
         if (lane == 0 && wloc > 0.0)
             atomicMax(&a.P->wmax[1 - a.parity], static_cast<unsigned long long>(__double_as_longlong(wloc)));
     }
+    return true;
+}
+
+// Per-warp mbarriers of the TMA ring: initialised once per launch by lane 0,
+// made visible to the async proxy before the first copy.
+template <int kWarps>
+__device__ __forceinline__ void init_ring_bars(unsigned long long (&bars)[kWarps][kRingRows], int wid) {
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < kRingRows; ++k) mbar_init(smem_addr(&bars[wid][k]), 1u);
+        mbar_init_fence();
+    }
+    __syncwarp();
 }
 
 template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad, int kFeat>
-__global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const StageArgs a) {
-    __shared__ __align__(16) typename Pol::C rbuf[kWarps][36][kVars];
-    if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
+__global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __grid_constant__ StageArgs a) {
+    // (the ring forms use no row buffer)
+    __shared__ __align__(16) typename Pol::C rbuf[kLoad >= 3 ? 1 : kWarps][36][kVars];
+    using RB = typename Pol::C(&)[kWarps][36][kVars];
+    const int wid = threadIdx.x >> 5;
+    if constexpr (kLoad == 4) {
+        __shared__ __align__(8) unsigned long long bars[kWarps][kRingRows];
+        init_ring_bars<kWarps>(bars, wid);
+        if ((threadIdx.x & 31) == 0) {
+            tma_prefetch_map(a.tmap_in);
+            if (a.stage >= 1 && sizeof(typename Pol::T) == 4) tma_prefetch_map(a.tmap_u0);
+        }
+        unsigned phase = 0u;
+        if constexpr (sizeof(typename Pol::T) == 4) {
+            __shared__ __align__(128) typename Pol::T ring[kWarps * kRingWords];
+            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid,
+                                                  bars[wid], &phase);
+        } else {
+            // FP64 ring: dynamic shared memory, sized at launch
+            extern __shared__ __align__(128) unsigned char march_dyn_smem[];
+            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf),
+                                                  reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid, bars[wid],
+                                                  &phase);
+        }
+    } else if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, ring, threadIdx.x >> 5);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid);
     } else if constexpr (kLoad == 3) {
         // FP64 ring: kWarps * ring_words<double>() doubles (36.9 KB for 4
         // warps); dynamic shared memory, sized at launch
-        extern __shared__ __align__(16) unsigned char march_dyn_smem[];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf,
-                                              reinterpret_cast<typename Pol::T*>(march_dyn_smem), threadIdx.x >> 5);
+        extern __shared__ __align__(128) unsigned char march_dyn_smem[];
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf),
+                                              reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid);
     } else {
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, nullptr, threadIdx.x >> 5);
     }
@@ -843,7 +978,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
     constexpr bool kRing = kLoad == 3;
     constexpr bool kDynRing = kRing && sizeof(typename Pol::T) == 8;  // FP64: ring in dynamic shared memory
     __shared__ __align__(16) typename Pol::T ring_static[kRing && !kDynRing ? kWarps * kRingWords : 1];
-    extern __shared__ __align__(16) unsigned char batch_dyn_smem[];
+    extern __shared__ __align__(128) unsigned char batch_dyn_smem[];
     typename Pol::T* const ring = kDynRing ? reinterpret_cast<typename Pol::T*>(batch_dyn_smem) : ring_static;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     C(&wbuf)[1][36][kVars] = *reinterpret_cast<C(*)[1][36][kVars]>(&rbuf[wid]);

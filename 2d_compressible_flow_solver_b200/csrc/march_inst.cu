@@ -22,7 +22,10 @@ cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
     if (nrows <= 0) return cudaSuccess;
     const dim3 grid((nseg + W - 1) / W, (nrows + R - 1) / R);
     size_t dyn = 0;
-    if constexpr (Ld == 3 && sizeof(typename Pol::T) == 8) {
+    if constexpr (Ld == 4) {
+        if (!a.has_tmaps || !a.err) return cudaErrorInvalidValue;
+    }
+    if constexpr (Ld >= 3 && sizeof(typename Pol::T) == 8) {
         // the FP64 ring lives in dynamic shared memory; allow it once per
         // device (std::call_once: host threads may make their first launches
         // on one device at the same time)
@@ -60,7 +63,7 @@ cudaError_t launch_march_k(const StageArgs& a, cudaStream_t s) {
 cudaError_t CFS_MARCH_FN(const StageArgs& a, int v, cudaStream_t s) {
     using P = CFS_MARCH_POL;
     constexpr int F = CFS_MARCH_FEAT;
-    static_assert(kNumVariants == 10, "variant table and dispatch disagree");
+    static_assert(kNumVariants == 13, "variant table and dispatch disagree");
     switch (v) {
         case 1: return launch_march_k<P, 0, F>(a, s);
         case 2: return launch_march_k<P, 1, F>(a, s);
@@ -72,6 +75,9 @@ cudaError_t CFS_MARCH_FN(const StageArgs& a, int v, cudaStream_t s) {
         case 8: return launch_march_k<P, 7, F>(a, s);
         case 9: return launch_march_k<P, 8, F>(a, s);
         case 10: return launch_march_k<P, 9, F>(a, s);
+        case 11: return launch_march_k<P, 10, F>(a, s);
+        case 12: return launch_march_k<P, 11, F>(a, s);
+        case 13: return launch_march_k<P, 12, F>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
