@@ -36,7 +36,17 @@ struct BatchCase {
     long long bflux_off = -1;     // bytes from the arena start to the boundary-face fluxes
     int ib_n = 0, ib_mode = 0;
     int ib_first = 0;       // first immersed-ghost index in the flattened lists
+    int feat = 0;           // row-march features this case needs (kFeatPos, kFeatEdge)
 };
+
+// Work items of one feature set: one persistent launch per stage runs them
+// with the row march compiled for exactly those features, so a case with
+// neither physical sides nor a body runs no edge code.
+struct FeatureGroup {
+    int feat = 0;
+    int first = 0, count = 0;  // range of the group's items in item_case / item_local
+};
+constexpr int kMaxGroups = 4;  // the feature sets a batch launches: 0, Pos, Edge, Edge | Pos
 
 }  // namespace
 
@@ -52,7 +62,7 @@ struct cfs_batch {
     uint8_t* lowo_d = nullptr;
     uint8_t* cflags_d = nullptr;
     bool any_bflux = false;  // some case has a physical side
-    int feat = 0;            // row-march features of the batch (kFeatPos, kFeatEdge)
+    std::vector<FeatureGroup> groups;  // work items by feature set, largest cases first in each
     int max_edge = 0;        // largest nx or ny of the cases
     int total_ig = 0;
     int* ib_cell = nullptr;
@@ -70,7 +80,7 @@ struct cfs_batch {
     int* item_local = nullptr;
     int* case_rows = nullptr;
     int* case_nseg = nullptr;
-    unsigned int* counters = nullptr;  // [parity][stage]
+    unsigned int* counters = nullptr;  // [parity][stage][group]
     double* staging = nullptr;
     double* sums = nullptr;  // plane sums of an uploaded case state (FP32 storage offsets)
     int grid = 0;
@@ -188,16 +198,20 @@ int enqueue_batch_step(cfs_batch* b, int parity) {
     for (int s = 0; s < S; ++s) {
         const int slot = parity * 3 + s;
         const int in = s;  // stage s reads S_s (S0, S1, S2)
-        CFSB_CUDA(b, cudaMemsetAsync(b->counters + slot, 0, sizeof(unsigned int), b->stream));
+        CFSB_CUDA(b, cudaMemsetAsync(b->counters + slot * kMaxGroups, 0, sizeof(unsigned int) * kMaxGroups, b->stream));
         if (b->total_ig > 0)
             CFSB_CUDA(b, cfs::launch_batch_ib_fill(b->elem, b->dib + static_cast<size_t>(in) * b->n, b->ig_case,
                                                    b->ig_local, b->total_ig, b->stream));
         if (b->any_bflux)
             CFSB_CUDA(b, cfs::launch_batch_boundary_flux(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->n,
                                                          b->max_edge, b->stream));
-        CFSB_CUDA(b, cfs::launch_batch_stage(b->prec, b->dargs + static_cast<size_t>(slot) * b->n, b->item_case,
-                                             b->item_local, b->case_rows, b->case_nseg, b->total_items,
-                                             b->counters + slot, b->grid, b->feat, b->stream));
+        for (size_t g = 0; g < b->groups.size(); ++g) {
+            const FeatureGroup& fg = b->groups[g];
+            CFSB_CUDA(b, cfs::launch_batch_stage(b->prec, b->dargs + static_cast<size_t>(slot) * b->n,
+                                                 b->item_case + fg.first, b->item_local + fg.first, b->case_rows,
+                                                 b->case_nseg, fg.count, b->counters + slot * kMaxGroups + g, b->grid,
+                                                 fg.feat, b->stream));
+        }
     }
     return CFS_OK;
 }
@@ -357,10 +371,19 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     }
     b->total_ig = static_cast<int>(h_cell.size());
 
-    // --- work items, largest cases first
+    // --- features per case: edge code where a case has a physical side or
+    // a body, positivity code as the batch's mode asks
+    for (BatchCase& c : b->cases) {
+        bool physical = false;
+        for (int s = 0; s < 4; ++s)
+            physical = physical || c.desc.bc[s] == CFS_BC_NEUMANN || c.desc.bc[s] == CFS_BC_DIRICHLET;
+        c.feat = (common->positivity ? cfs::kFeatPos : 0) | (physical || c.cflags_off >= 0 ? cfs::kFeatEdge : 0);
+    }
+    // --- work items grouped by feature set, largest cases first in each group
     std::vector<int> order(ncases);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (b->cases[x].feat != b->cases[y].feat) return b->cases[x].feat < b->cases[y].feat;
         return static_cast<long long>(b->cases[x].desc.nx) * b->cases[x].desc.ny >
                static_cast<long long>(b->cases[y].desc.nx) * b->cases[y].desc.ny;
     });
@@ -368,10 +391,17 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     std::vector<int> it_case, it_local, c_rows(ncases), c_ix(ncases);
     for (int ci : order) {
         const BatchCase& c = b->cases[ci];
+        if (b->groups.empty() || b->groups.back().feat != c.feat) {
+            FeatureGroup g;
+            g.feat = c.feat;
+            g.first = static_cast<int>(it_case.size());
+            b->groups.push_back(g);
+        }
         for (int li = 0; li < c.nseg * c.items_y; ++li) {
             it_case.push_back(ci);
             it_local.push_back(li);
         }
+        b->groups.back().count = static_cast<int>(it_case.size()) - b->groups.back().first;
     }
     for (int ci = 0; ci < ncases; ++ci) {
         c_rows[ci] = b->cases[ci].rows;
@@ -399,7 +429,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         !dalloc(reinterpret_cast<void**>(&b->item_local), sizeof(int) * it_local.size()) ||
         !dalloc(reinterpret_cast<void**>(&b->case_rows), sizeof(int) * ncases) ||
         !dalloc(reinterpret_cast<void**>(&b->case_nseg), sizeof(int) * ncases) ||
-        !dalloc(reinterpret_cast<void**>(&b->counters), sizeof(unsigned int) * 6) ||
+        !dalloc(reinterpret_cast<void**>(&b->counters), sizeof(unsigned int) * 6 * kMaxGroups) ||
         !dalloc(reinterpret_cast<void**>(&b->staging), sizeof(double) * kVars * max_cells) ||
         !dalloc(reinterpret_cast<void**>(&b->sums), sizeof(double) * cfs::plane_sums_scratch_doubles()))
         return bail(CFS_ERR_NOMEM, "batch device allocation failed");
@@ -430,9 +460,6 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
             if (cfs::launch_ghost_fill(b->elem, state_buf(b, b->cases[ci], k), b->cases[ci].L, b->cases[ci].sides,
                                        b->stream) != cudaSuccess)
                 return bail(CFS_ERR_CUDA, "ghost fill failed");
-    bool flags = false;
-    for (const BatchCase& c : b->cases) flags = flags || c.cflags_off >= 0;
-    b->feat = (common->positivity ? cfs::kFeatPos : 0) | (b->any_bflux || flags ? cfs::kFeatEdge : 0);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, common->device) != cudaSuccess || sms <= 0)
         return bail(CFS_ERR_CUDA, "SM count query failed");

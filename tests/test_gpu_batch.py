@@ -10,9 +10,21 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+def _mixed_cases(workloads):
+    """Quadrant and cylinder cases (edge code) beside periodic body-free
+    smooth-advection cases (no edge code): the batch runs them as separate
+    feature groups."""
+    cases, states = workloads.batch_cases(8, seed=5, sizes=[48, 64, 96, 112, 160])
+    for n in (64, 96, 150):
+        w = workloads.smooth_advection(n)
+        cases.append({"nx": n, "ny": n, "lx": 1.0, "ly": 1.0, "bc": (2, 2, 2, 2)})
+        states.append(w.U0)
+    return cases, states
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_batch_equals_single_contexts(cfsb, workloads, prec):
-    cases, states = workloads.batch_cases(8, seed=5, sizes=[48, 64, 96, 112, 160])
+    cases, states = _mixed_cases(workloads)
     with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_BODY) as b:
         for k, U in enumerate(states):
             b.set_state(k, U)
