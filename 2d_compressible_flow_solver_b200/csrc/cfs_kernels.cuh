@@ -24,9 +24,24 @@ enum { kHllReference = 0, kHllDavis = 1 };
 // (throughput forms) 1/rho.
 template <class C> struct Face5 { C r, mx, my, E, p, a, ri; };
 
-__device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
+// FP32 reciprocal and reciprocal square root of the throughput forms: the
+// PTX approximations themselves (one MUFU instruction each, maximum error
+// 1 ulp for rcp.approx and 2 ulp for rsqrt.approx per the PTX ISA), with
+// subnormal inputs and results flushed to zero.  The state's magnitudes are
+// far from the subnormal range, and the row march is bound by instruction
+// issue, so no range handling is wrapped around them.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_fast(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
-__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrtf(x); }
+__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrt_fast(x); }
 __device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
 
 // One cell's four stored variables in vector accesses (one 16-byte access in

@@ -128,7 +128,7 @@ __device__ __forceinline__ void finish_pair(Face5<typename Pol::C>& L, Face5<typ
         }
         const float2 p = mul2(p2(float(g - 1)), sub2(E, ke));
         const float2 a2 = mul2(mul2(p2(float(g)), p), ri);
-        const float2 a = mul2(a2, make_float2(rsqrtf(a2.x), rsqrtf(a2.y)));
+        const float2 a = mul2(a2, make_float2(rsqrt_fast(a2.x), rsqrt_fast(a2.y)));
         L.ri = ri.x;
         R.ri = ri.y;
         L.p = p.x;
