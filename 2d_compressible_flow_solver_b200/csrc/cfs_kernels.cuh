@@ -270,8 +270,11 @@ __device__ __forceinline__ void hll_flux(const Face5<typename Pol::C>& L, const 
             SL = min_ref(qL - aL, u_star - a_star_L);
             SR = max_ref(qL + aL, u_star + a_star_R);
         } else {
-            SL = min_ref(uL - aL, uR - aR);
-            SR = max_ref(uL + aL, uR + aR);
+            // Davis bounds have no reference counterpart: fmin / fmax (one
+            // min-max instruction each) instead of the reference's
+            // compare-and-select
+            SL = fmin(uL - aL, uR - aR);
+            SR = fmax(uL + aL, uR + aR);
         }
     }
     if constexpr (Pol::kMixed) {
