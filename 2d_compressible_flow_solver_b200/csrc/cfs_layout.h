@@ -121,6 +121,7 @@ struct StageArgs {
 
 // Bits of *StageArgs::err.
 constexpr unsigned int kErrTmaTimeout = 1u;  // a TMA copy did not land within its bounded wait
+constexpr unsigned int kErrTmaAlign = 2u;    // a TMA copy's shared-memory row was not 128-byte aligned (not issued)
 
 // Rows [lo, hi) a stage launch updates.
 CFS_HD int stage_row_lo(const StageArgs& a) { return a.row_lo; }

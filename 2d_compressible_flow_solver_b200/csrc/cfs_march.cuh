@@ -230,14 +230,24 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // rows of U^0 (lane l reads column l + 2).  The FP64 ring leaves U^0 out (each
 // lane loads it early in the row's iteration): its rows of doubles would
 // otherwise cost a fourth block per SM.
+// A ring row holds 36 cells and starts 128-byte aligned, as a TMA copy's
+// shared-memory destination must: its stride is rounded up to 128 bytes
+// (FP32: 576 bytes of cells in a 640-byte row; FP64: 1,152 bytes, already a
+// multiple).
 constexpr int kRingRows = 8, kRingDist = 2;
 constexpr int kRingCols = 36;
-constexpr int kRingRowWords = kRingCols * kVars, kRingU0Words = kRingCols * kVars;
-constexpr int kRingWords = kRingRows * (kRingRowWords + kRingU0Words);
+template <class T>
+__host__ __device__ constexpr int ring_row_words() {
+    return ((kRingCols * kVars * static_cast<int>(sizeof(T)) + 127) / 128) * 128 / static_cast<int>(sizeof(T));
+}
 template <class T>
 __host__ __device__ constexpr int ring_words() {
-    return sizeof(T) == 4 ? kRingWords : kRingRows * kRingRowWords;
+    return sizeof(T) == 4 ? kRingRows * 2 * ring_row_words<T>() : kRingRows * ring_row_words<T>();
 }
+static_assert(ring_row_words<float>() * 4 % 128 == 0 && ring_row_words<double>() * 8 % 128 == 0,
+              "ring rows start 128-byte aligned");
+static_assert(ring_words<float>() * 4 % 128 == 0 && ring_words<double>() * 8 % 128 == 0,
+              "each warp's ring starts 128-byte aligned");
 
 // ---- TMA staging (load schedule 4).  One elected lane of a warp copies a
 // whole ring row -- the 4 variables of 36 cells, one box of the state
@@ -253,6 +263,9 @@ __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -572,10 +585,11 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int bx, int by, i
 
     // Load schedule 3: this warp's ring (rows, and U^0 rows in FP32; ring_words).
     constexpr bool kU0Ring = kRing && sizeof(T) == 4;
+    constexpr int kRowWords = ring_row_words<T>();
     T* const rw = kRing ? ring + wid * ring_words<T>() : nullptr;
-    T* const ru0 = kU0Ring ? rw + kRingRows * kRingRowWords : nullptr;
-    auto ring_row = [&](int q) -> T* { return rw + (q & (kRingRows - 1)) * kRingRowWords; };
-    auto ring_u0 = [&](int q) -> T* { return ru0 + (q & (kRingRows - 1)) * kRingU0Words; };
+    T* const ru0 = kU0Ring ? rw + kRingRows * kRowWords : nullptr;
+    auto ring_row = [&](int q) -> T* { return rw + (q & (kRingRows - 1)) * kRowWords; };
+    auto ring_u0 = [&](int q) -> T* { return ru0 + (q & (kRingRows - 1)) * kRowWords; };
     // Issue the copies of row q (the lane's column; halo lanes also their
     // halo column) and, for an updated row, of its U^0; one commit group per
     // row (empty past the last row needed, so group counts stay uniform).
@@ -591,10 +605,18 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int bx, int by, i
             if (lane == 0) {
                 const bool u0row = kU0Ring && a.stage >= 1 && q >= i0 && q < i1;
                 const unsigned bar = smem_addr(bars + (q & (kRingRows - 1)));
-                fence_proxy_async_smem();
-                mbar_expect_tx(bar, u0row ? 2u * kRowBytes : kRowBytes);
-                tma_load_row(smem_addr(ring_row(q)), a.tmap_in, tcol, q + kGhost, bar);
-                if (u0row) tma_load_row(smem_addr(ring_u0(q)), a.tmap_u0, tcol, q + kGhost, bar);
+                const unsigned dst = smem_addr(ring_row(q)), dst0 = u0row ? smem_addr(ring_u0(q)) : 0u;
+                if (((dst | dst0) & 127u) != 0u) {
+                    // self-check: never issue a copy to a misaligned row;
+                    // complete the slot's phase without data and flag it
+                    atomicOr(a.err, kErrTmaAlign);
+                    mbar_arrive(bar);
+                } else {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(bar, u0row ? 2u * kRowBytes : kRowBytes);
+                    tma_load_row(dst, a.tmap_in, tcol, q + kGhost, bar);
+                    if (u0row) tma_load_row(dst0, a.tmap_u0, tcol, q + kGhost, bar);
+                }
             }
         } else if constexpr (kRing) {
             if (q <= i1 + 2) {
@@ -938,7 +960,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __
         }
         unsigned phase = 0u;
         if constexpr (sizeof(typename Pol::T) == 4) {
-            __shared__ __align__(128) typename Pol::T ring[kWarps * kRingWords];
+            __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
             march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid,
                                                   bars[wid], &phase);
         } else {
@@ -949,7 +971,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __
                                                   &phase);
         }
     } else if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
-        __shared__ __align__(16) typename Pol::T ring[kWarps * kRingWords];
+        __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
         march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid);
     } else if constexpr (kLoad == 3) {
         // FP64 ring: kWarps * ring_words<double>() doubles (36.9 KB for 4
@@ -977,7 +999,7 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks)
     __shared__ __align__(16) C rbuf[kWarps][36][kVars];
     constexpr bool kRing = kLoad == 3;
     constexpr bool kDynRing = kRing && sizeof(typename Pol::T) == 8;  // FP64: ring in dynamic shared memory
-    __shared__ __align__(16) typename Pol::T ring_static[kRing && !kDynRing ? kWarps * kRingWords : 1];
+    __shared__ __align__(128) typename Pol::T ring_static[kRing && !kDynRing ? kWarps * ring_words<typename Pol::T>() : 1];
     extern __shared__ __align__(128) unsigned char batch_dyn_smem[];
     typename Pol::T* const ring = kDynRing ? reinterpret_cast<typename Pol::T*>(batch_dyn_smem) : ring_static;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
