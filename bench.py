@@ -904,7 +904,7 @@ def modes_arm(args):
     in one mode; the last mode is the periodic Navier-Stokes shear layer (mu =
     1/2000, Pr 0.72) on the same grid.  Each form, each mode: W warm-up steps, K
     timed steps with CUDA events on the engine's stream.  `--mode` runs one mode
-    (FP32 only), for a profiler.  One JSON line."""
+    in one form (`--form`, FP32 by default), for a profiler.  One JSON line."""
     import torch
 
     cfsb = importlib.import_module(PKG)
@@ -935,7 +935,8 @@ def modes_arm(args):
     out = {"workload": f"row-march feature sets, four-quadrant state {n}^2, SSP-RK3, Davis HLL, CFL 0.5",
            "steps": args.steps, "warmup": args.warmup, "unit": UNIT}
     if args.mode:
-        out[args.mode] = {"fp32": rate(cfsb.FP32_MIXED, args.mode)}
+        form = cfsb.FP64 if args.form == "f64" else cfsb.FP32_MIXED
+        out[args.mode] = {args.form: rate(form, args.mode)}
     else:
         for mode in MODES:
             out[mode] = {"fp32": rate(cfsb.FP32_MIXED, mode), "fp64": rate(cfsb.FP64, mode)}
@@ -963,6 +964,7 @@ def main():
     ap.add_argument("--modes-n", type=int, default=2048, help="grid edge of the modes workload")
     ap.add_argument("--mode", choices=list(MODES), default=None, help="modes workload: run this mode only (FP32)")
     ap.add_argument("--variant", type=int, default=0, help="modes workload: stage-kernel variant (0 = default)")
+    ap.add_argument("--form", choices=["f32", "f64"], default="f32", help="modes workload with --mode: the form to run")
     ap.add_argument("--report-parts", default="quadrants,cylinder,shear,batch,convergence",
                     help="report workload: comma-separated parts to run")
     ap.add_argument("--batch-steps", type=int, default=500, help="report workload: steps of the batch comparison")
