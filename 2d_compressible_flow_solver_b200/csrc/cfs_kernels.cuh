@@ -41,6 +41,22 @@ __device__ __forceinline__ float rsqrt_fast(float x) {
     return r;
 }
 __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
+
+// FP64 reciprocal of a positive, finite, normal x (the WENO weight sums,
+// bounded below by eps^2): the hardware approximation refined by two
+// Newton-Raphson steps r <- r + r (1 - x r) (quadratic convergence: the
+// approximation's relative error e becomes about e^4, far below FP64
+// rounding), as fused multiply-adds; no handling of zero, infinite or
+// subnormal inputs, which never reach it.
+__device__ __forceinline__ double rcp_pos(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_pos(float x) { return rcp_fast(x); }
 __device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrt_fast(x); }
 __device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
 

@@ -67,8 +67,9 @@ __device__ __forceinline__ void weno5_pair_diff(C v0, C v1, C v2, C v3, C v4, C 
     const C r0 = fma(C(1.0 / 6.0), d2, n2);
     const C r1 = fma(C(1.0 / 6.0), d1, n1);
     const C r2 = fma(C(1.0 / 6.0), d0, n0);
-    left = fma(fma(q12, n0, fma(a1, n1, a2L * n2)), rcp_fast(-(q12 + a1 + a2L)), v2);
-    right = fma(fma(q01, r0, fma(a1, r1, a2R * r2)), rcp_fast(q01 + a1 + a2R), v2);
+    // (the weight sums are >= eps^2 > 0: rcp_pos; the left one negated after)
+    left = fma(fma(q12, n0, fma(a1, n1, a2L * n2)), -rcp_pos(q12 + a1 + a2L), v2);
+    right = fma(fma(q01, r0, fma(a1, r1, a2R * r2)), rcp_pos(q01 + a1 + a2R), v2);
 }
 
 template <class C>
