@@ -42,12 +42,18 @@ __device__ __forceinline__ float rsqrt_fast(float x) {
 }
 __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
 
-// FP64 reciprocal of a positive, finite, normal x (the WENO weight sums,
-// bounded below by eps^2): the hardware approximation refined by two
-// Newton-Raphson steps r <- r + r (1 - x r) (quadratic convergence: the
-// approximation's relative error e becomes about e^4, far below FP64
-// rounding), as fused multiply-adds; no handling of zero, infinite or
-// subnormal inputs, which never reach it.
+// FP64 reciprocal and square root of the FP64 throughput form, from the
+// hardware approximations refined by Newton-Raphson steps as fused
+// multiply-adds (a published method; quadratic convergence: an initial
+// relative error e becomes about e^2 per step, and two steps take the
+// approximations far below FP64 rounding).  Inputs are finite, nonzero and
+// normal where these are used (WENO weight sums >= eps^2, densities and
+// pressures of physical states); a zero or negative argument yields NaN
+// where the IEEE operation would give an infinity or NaN, which the callers
+// treat alike (non-admissible state, a blow-up the CFL reduction reports).
+//   reciprocal: r <- r + r (1 - x r);
+//   square root: the reciprocal square root y <- y + (y/2)(1 - x y^2),
+//     then s = x y corrected once by s <- s + (y/2)(x - s^2).
 __device__ __forceinline__ double rcp_pos(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -55,6 +61,16 @@ __device__ __forceinline__ double rcp_pos(double x) {
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
+}
+__device__ __forceinline__ double sqrt_pos(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double h = 0.5 * y;
+    y = fma(h, fma(-x * y, y, 1.0), y);
+    h = 0.5 * y;
+    y = fma(h, fma(-x * y, y, 1.0), y);
+    const double sq = x * y;
+    return fma(0.5 * y, fma(-sq, sq, x), sq);
 }
 __device__ __forceinline__ float rcp_pos(float x) { return rcp_fast(x); }
 __device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrt_fast(x); }
@@ -202,10 +218,10 @@ __device__ __forceinline__ void finish_state(Face5<typename Pol::C>& s, double g
             s.a = sqrt_fast(C(g) * s.p * rinv);
         }
     } else {
-        const C rinv = rcp_fast(s.r);
+        const C rinv = rcp_pos(s.r);
         s.ri = rinv;
         s.p = C(g - 1) * (s.E - C(0.5) * (s.mx * s.mx + s.my * s.my) * rinv);
-        s.a = sqrt(C(g) * s.p * rinv);
+        s.a = sqrt_pos(C(g) * s.p * rinv);
     }
 }
 

@@ -58,9 +58,14 @@ constexpr MarchVariant kVariants[kNumVariants] = {
     {32, 4, 5, 4}, {32, 4, 4, 4}, {64, 4, 4, 4},
 };
 // 1-based defaults, the 4096^2 winners of the committed tuning table
-// (2d_compressible_flow_solver_b200/tuning.json).
+// (2d_compressible_flow_solver_b200/tuning.json): FP32 stages its ring rows by
+// per-lane 16-byte cp.async (variant 7: 10,356 Mcell-steps/s against 10,216 for
+// the same shape staged by TMA, whose lane-0 issue and mbarrier waits cost
+// more instructions than the copies they replace once cells are interleaved);
+// FP64 stages them by TMA (variant 12: 4,835 against 4,816 by cp.async, and
+// ahead at 256^2 .. 2048^2 too).
 constexpr int kDefaultVariantF32 = 7;
-constexpr int kDefaultVariantF64 = 8;
+constexpr int kDefaultVariantF64 = 12;
 // FP32 grids with edge code (physical sides, cell types) run the same ring
 // march with 128 registers and 4 blocks per SM: 2048^2 transmissive with floors
 // and a cylinder 5,672 against 5,476 Mcell-steps/s, the 2048 x 1024 Mach-3
