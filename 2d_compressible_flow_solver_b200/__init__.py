@@ -72,7 +72,7 @@ class CfsCase(ctypes.Structure):
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
         ("bc", ctypes.c_int * 4), ("bc_prim", (ctypes.c_double * 4) * 4),
         ("circle", ctypes.c_int), ("radius", ctypes.c_double), ("cx", ctypes.c_double), ("cy", ctypes.c_double),
-        ("npoints", ctypes.c_int), ("ib_mode", ctypes.c_int), ("rows", ctypes.c_int),
+        ("npoints", ctypes.c_int), ("ib_mode", ctypes.c_int), ("rows", ctypes.c_int), ("edge_code", ctypes.c_int),
     ]
 
 
@@ -522,6 +522,7 @@ class Batch:
                 d.npoints = int(c.get("npoints", 400))
                 d.ib_mode = int(c.get("ib_mode", IB_BILINEAR_SLIP))
             d.rows = int(c.get("rows", 0))
+            d.edge_code = int(bool(c.get("edge_code", False)))
             self.shapes.append((d.nx, d.ny))
         self._b = ctypes.c_void_p()
         rc = self._lib.cfs_batch_create(ctypes.byref(cfg), len(cases), ctypes.cast(arr, ctypes.c_void_p),

@@ -377,7 +377,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         bool physical = false;
         for (int s = 0; s < 4; ++s)
             physical = physical || c.desc.bc[s] == CFS_BC_NEUMANN || c.desc.bc[s] == CFS_BC_DIRICHLET;
-        c.feat = (common->positivity ? cfs::kFeatPos : 0) | (physical || c.cflags_off >= 0 ? cfs::kFeatEdge : 0);
+        c.feat = (common->positivity ? cfs::kFeatPos : 0) |
+                 (physical || c.cflags_off >= 0 || c.desc.edge_code ? cfs::kFeatEdge : 0);
     }
     // --- work items grouped by feature set, largest cases first in each group
     std::vector<int> order(ncases);

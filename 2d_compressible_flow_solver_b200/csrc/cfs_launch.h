@@ -62,12 +62,12 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 // per-lane 16-byte cp.async (variant 7: 10,356 Mcell-steps/s against 10,216 for
 // the same shape staged by TMA, whose lane-0 issue and mbarrier waits cost
 // more instructions than the copies they replace once cells are interleaved);
-// FP64 by cp.async too (variant 8: 5,592 against 5,569 for the same shape
-// staged by TMA, and ahead at 256^2 .. 2048^2 as well, since the FP64 sound
-// speed and 1/rho come from Newton-refined hardware approximations; before
-// that TMA led by 0.4 %).
+// FP64 stages them by TMA (variant 12: 5,880 against 5,777 for the same shape
+// by cp.async, and ahead at 1024^2 and 2048^2 too; with the cubically refined
+// reciprocal and square root and the branch-free HLL the cp.async form needs a
+// few more registers than 128 and spills 8 bytes, the TMA form none).
 constexpr int kDefaultVariantF32 = 7;
-constexpr int kDefaultVariantF64 = 8;
+constexpr int kDefaultVariantF64 = 12;
 // FP32 grids with edge code (physical sides, cell types) run the same ring
 // march with 128 registers and 4 blocks per SM: 2048^2 transmissive with floors
 // and a cylinder 5,672 against 5,476 Mcell-steps/s, the 2048 x 1024 Mach-3

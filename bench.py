@@ -265,6 +265,9 @@ def engine_arm(args):
     ms32, t32, dt32, _ = timed_advance(cfsb.FP32_MIXED, K, W)
     clocks = sampler.stop()
     ms64, _, _, _ = timed_advance(cfsb.FP64, K, W)
+    # the multi-GPU slab path at one rank (device-ordered stage launches through
+    # the steps API, no graph, no exchange partner), against the single grid
+    ms_slab1 = timed_advance_slab(cfsb.FP32_MIXED, K, W)[0] if world == 1 else None
     if world > 1:
         t = torch.tensor([ms32, ms64], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -322,6 +325,12 @@ def engine_arm(args):
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        if ms_slab1 is not None:
+            v_slab1 = cells * K / (ms_slab1 / 1e3) / 1e6
+            result["slab_solver_1rank"] = {
+                "fp32": round(v_slab1, 1), "over_single_grid": round(v_slab1 / v32, 4),
+                "how": "parallel.SlabSolver at world size 1 on the same grid: the stages launched one by one "
+                       "through the device-ordered steps API (no CUDA graph), CUDA events on the engine's stream"}
     # like-for-like companion of the reference arm: the reference's own scheme
     # (TVD3rdRK as written, its HLL, transmissive sides, fixed dt) on the same
     # 4096^2 state, FP64 and FP32-mixed
@@ -412,30 +421,37 @@ def engine_arm(args):
 
 
 # ------------------------------------------------------------ batch arm
+def _time_batch(cfsb, torch, cases, states, prec, K: int, W: int, device: int):
+    """(ms for K steps after W warm-up steps, cells, work items per stage) of
+    one persistent batch, timed with CUDA events on the batch's stream (the
+    per-case CFL reductions, graph replays and the final read-back of the
+    per-case times included)."""
+    with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR, device=device) as b:
+        cells, items = b.info()
+        for k, U in enumerate(states):
+            b.set_state(k, U)
+        b.advance(W, cfl=0.5)
+        stream = torch.cuda.ExternalStream(b.stream, device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.advance(K, cfl=0.5)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), cells, items
+
+
 def batch_subresult(cfsb, wl, torch, ncases: int, K: int, W: int, device: int) -> dict:
     """The uneven batch in the default line: every case of `ncases` (seeded,
     nx, ny in 64..768) advanced K steps after W warm-up steps by the persistent
-    batched engine, FP32-mixed and FP64, timed with CUDA events on the batch's
-    stream (the per-case CFL reductions, graph replays and the final read-back
-    of the per-case times included)."""
+    batched engine, FP32-mixed and FP64."""
     cases, states = wl.batch_cases(ncases, seed=1)
     out = {"workload": f"{ncases} uneven cases, nx,ny in 64..768 step 16, half four-quadrant, half Mach 2-3 "
                        "cylinder (slip wall), SSP-RK3, Davis HLL, positivity fallbacks with floors, per-case CFL 0.5",
            "steps": K, "warmup": W}
     for prec, key in ((cfsb.FP32_MIXED, "fp32"), (cfsb.FP64, "fp64")):
-        with cfsb.Batch(cases, precision=prec, positivity=cfsb.POSITIVITY_FLOOR, device=device) as b:
-            cells, items = b.info()
-            for k, U in enumerate(states):
-                b.set_state(k, U)
-            b.advance(W, cfl=0.5)
-            stream = torch.cuda.ExternalStream(b.stream, device=device)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            b.advance(K, cfl=0.5)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            out[key] = round(cells * K / (e0.elapsed_time(e1) / 1e3) / 1e6, 1)
+        ms, cells, items = _time_batch(cfsb, torch, cases, states, prec, K, W, device)
+        out[key] = round(cells * K / (ms / 1e3) / 1e6, 1)
         out["cells"] = cells
         out["work_items_per_stage"] = items
     peak, kind = hbm_peak()
@@ -507,6 +523,22 @@ def batch_arm(args):
     out.update({"cells": cells, "work_items_per_stage": items,
                 "batched_fp32": round(v32, 1), "batched_fp64": round(v64, 1),
                 "create_s_fp32": round(create_s[cfsb.FP32_MIXED], 3)})
+    # Per-case code paths: the same cases with the four-quadrant ones on
+    # periodic sides, which need no edge code, so the batch runs two feature
+    # groups (one persistent launch each per stage); against the same batch
+    # with every case asking for the edge code (one group, one launch).
+    periodic = [c if "circle" in c else dict(c, bc=(2, 2, 2, 2)) for c in cases]
+    fg = {"workload": "the cases above with the four-quadrant cases on periodic sides (no edge code), "
+                      "the cylinders unchanged; per-case code path (two launches per stage) against the edge "
+                      "code for every case (cfs_case.edge_code = 1, one launch per stage); CUDA events on the "
+                      "batch's stream, max over ranks"}
+    for label, cs in (("per_case", periodic), ("edge_code_for_all", [dict(c, edge_code=True) for c in periodic])):
+        for prec, key in ((cfsb.FP32_MIXED, "fp32"), (cfsb.FP64, "fp64")):
+            ms, c_cells, _ = _time_batch(cfsb, torch, cs, states, prec, K, W, local)
+            fg[f"{label}_{key}"] = round(job_sum(c_cells) * K / (job_max(ms) / 1e3) / 1e6, 1)
+    fg["per_case_gain_fp32"] = round(fg["per_case_fp32"] / fg["edge_code_for_all_fp32"], 3)
+    fg["per_case_gain_fp64"] = round(fg["per_case_fp64"] / fg["edge_code_for_all_fp64"], 3)
+    out["feature_groups"] = fg
     solvers = []
     for c, U in zip(cases, states):
         s = cfsb.Solver(c["nx"], c["ny"], c["lx"], c["ly"], precision=cfsb.FP64, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,

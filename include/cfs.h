@@ -354,6 +354,10 @@ typedef struct cfs_case {
     int npoints;
     int ib_mode;             /* enum cfs_ib_mode */
     int rows;                /* row chunk of a work item (0: from the tuning default) */
+    int edge_code;           /* 1: run this case with the row march's edge code even where it
+                                needs none (no physical side, no body): its work items join the
+                                launch of the cases that need it, one launch fewer per stage when
+                                it is the only case without; 0: the code path the case needs */
 } cfs_case;
 
 typedef struct cfs_batch cfs_batch;

@@ -76,3 +76,26 @@ def test_batch_replays_a_dt_sequence_per_case(cfsb, workloads):
         for k in range(len(cases)):
             assert np.array_equal(b.get_state(k), ref[k])
     assert np.array_equal(t, t_ref)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_edge_code_on_request_changes_nothing(cfsb, workloads, prec):
+    """cfs_case.edge_code = 1 puts periodic body-free cases into the edge-code
+    launch (one feature group instead of two); their physics is unchanged --
+    the edge code finds no physical side and no cell flags -- so they end
+    within the instantiation tolerance of the same batch without the request."""
+    cases, states = _mixed_cases(workloads)
+    forced = [dict(c, edge_code=True) for c in cases]
+    out = []
+    for cs in (cases, forced):
+        with cfsb.Batch(cs, precision=prec, positivity=cfsb.POSITIVITY_BODY) as b:
+            for k, U in enumerate(states):
+                b.set_state(k, U)
+            t = b.advance(5, cfl=0.5)
+            out.append(([b.get_state(k) for k in range(len(cs))], t))
+    tol = 1e-12 if prec == cfsb.FP64 else 1e-5
+    for k in range(len(cases)):
+        a, b_ = out[0][0][k], out[1][0][k]
+        assert np.all(np.isfinite(b_))
+        assert np.abs(a - b_).max() / np.abs(a).max() <= tol, k
+        assert abs(out[0][1][k] - out[1][1][k]) <= tol * out[0][1][k]
