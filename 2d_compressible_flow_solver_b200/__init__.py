@@ -61,7 +61,7 @@ class CfsConfig(ctypes.Structure):
         ("viscous", ctypes.c_int),
         ("mu", ctypes.c_double), ("prandtl", ctypes.c_double), ("mach", ctypes.c_double),
         ("keep_rhs", ctypes.c_int), ("device", ctypes.c_int), ("variant", ctypes.c_int),
-        ("positivity", ctypes.c_int), ("rounding", ctypes.c_int),
+        ("positivity", ctypes.c_int), ("rounding", ctypes.c_int), ("march_rows", ctypes.c_int),
     ]
 
 
@@ -271,7 +271,7 @@ class Solver:
                  rk: int = RK_TVD3_REFERENCE, hll: int = HLL_REFERENCE, bc=(BC_NEUMANN,) * 4, bc_prim=None,
                  gamma: float = 1.4, weno_eps: float = 1e-2, viscous: int = VISCOUS_OFF, mu: float = 1e-3,
                  prandtl: float = 0.72, mach: float = 1.0, keep_rhs: bool = False, device: int = 0,
-                 variant: int = 0, positivity: int = 0, rounding: int = ROUND_STOCHASTIC):
+                 variant: int = 0, positivity: int = 0, rounding: int = ROUND_STOCHASTIC, march_rows: int = 0):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
@@ -285,7 +285,7 @@ class Solver:
                     cfg.bc_prim[s][q] = float(bc_prim[s][q])
         cfg.viscous, cfg.mu, cfg.prandtl, cfg.mach = int(viscous), float(mu), float(prandtl), float(mach)
         cfg.keep_rhs, cfg.device, cfg.variant = int(bool(keep_rhs)), int(device), int(variant)
-        cfg.positivity, cfg.rounding = int(positivity), int(rounding)
+        cfg.positivity, cfg.rounding, cfg.march_rows = int(positivity), int(rounding), int(march_rows)
         self.config = cfg
         self.nx, self.ny = int(nx), int(ny)
         self._ctx = ctypes.c_void_p()

@@ -147,6 +147,7 @@ int validate(const cfs_config* g, std::string& msg) {
         }
     if (g->viscous != CFS_VISCOUS_OFF && g->viscous != CFS_VISCOUS_NS) { msg = "unknown viscous mode"; return CFS_ERR_INVALID; }
     if (g->variant < 0 || g->variant > cfs::kNumVariants) { msg = "unknown kernel variant"; return CFS_ERR_INVALID; }
+    if (g->march_rows < 0 || g->march_rows > 4096) { msg = "march_rows out of range 0..4096"; return CFS_ERR_INVALID; }
     if (g->positivity < CFS_POSITIVITY_OFF || g->positivity > CFS_POSITIVITY_FLOOR) {
         msg = "unknown positivity mode";
         return CFS_ERR_INVALID;
@@ -182,6 +183,7 @@ cfs::StageArgs base_args(const cfs_ctx* c) {
     a.mach = c->cfg.mach;
     a.types = c->has_types ? c->types_d : nullptr;
     a.variant = c->cfg.variant;
+    a.rows = c->cfg.march_rows;
     a.positivity = c->cfg.positivity;
     a.rounding = c->cfg.rounding;
     a.seed = c->steps_done;

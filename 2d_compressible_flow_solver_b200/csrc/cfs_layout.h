@@ -109,6 +109,7 @@ struct StageArgs {
     int row_lo, row_hi;    // throughput forms: the launch updates cells of rows [row_lo, row_hi)
                            // (row_hi 0: up to nx); a decomposed grid updates its interior
                            // rows while the halo exchange is in flight, then its edge rows
+    int rows;              // row march: rows of one warp's work item (0: the launcher chooses)
     unsigned int* err;     // device error flags (kErr* bits), set instead of waiting forever
     int has_tmaps;         // 1: tmap_in (and, stage >= 1, tmap_u0) hold encoded tensor maps
     // TMA load schedule: tensor maps (CUtensorMap) of the `in` and `u0` buffers,

@@ -948,6 +948,8 @@ __device__ __forceinline__ void init_ring_bars(unsigned long long (&bars)[kWarps
 
 template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad, int kFeat>
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __grid_constant__ StageArgs a) {
+    // rows of this launch's work items: chosen by the launcher (a.rows), or the variant's
+    const int rows = a.rows > 0 ? a.rows : kRows;
     // (the ring forms use no row buffer)
     __shared__ __align__(16) typename Pol::C rbuf[kLoad >= 3 ? 1 : kWarps][36][kVars];
     using RB = typename Pol::C(&)[kWarps][36][kVars];
@@ -962,26 +964,26 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __
         unsigned phase = 0u;
         if constexpr (sizeof(typename Pol::T) == 4) {
             __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
-            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid,
+            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf), ring, wid,
                                                   bars[wid], &phase);
         } else {
             // FP64 ring: dynamic shared memory, sized at launch
             extern __shared__ __align__(128) unsigned char march_dyn_smem[];
-            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf),
+            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf),
                                                   reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid, bars[wid],
                                                   &phase);
         }
     } else if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf), ring, wid);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf), ring, wid);
     } else if constexpr (kLoad == 3) {
         // FP64 ring: kWarps * ring_words<double>() doubles (36.9 KB for 4
         // warps); dynamic shared memory, sized at launch
         extern __shared__ __align__(128) unsigned char march_dyn_smem[];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, reinterpret_cast<RB>(rbuf),
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf),
                                               reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid);
     } else {
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, kRows, rbuf, nullptr, threadIdx.x >> 5);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, rbuf, nullptr, threadIdx.x >> 5);
     }
 }
 

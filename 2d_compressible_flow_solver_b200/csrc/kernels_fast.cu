@@ -42,10 +42,10 @@ int sm_count() {
 // finishes first (measured with the earlier 3-block ring on the Mach-3
 // cylinder, 2048 x 1024: 2,105 against 1,832 Mcell-steps/s; the 4-block ring
 // now fills that grid in one wave and runs it at 2,376).
-int default_variant_f64(const Layout& L) {
+int default_variant_f64(const Layout& L, int rows) {
     const MarchVariant& d = kVariants[kDefaultVariantF64 - 1];
     const long long nseg = (L.ny + kSeg - 1) / kSeg;
-    const long long blocks = ((nseg + d.warps - 1) / d.warps) * ((L.nx + d.rows - 1) / d.rows);
+    const long long blocks = ((nseg + d.warps - 1) / d.warps) * ((L.nx + rows - 1) / rows);
     const double waves = static_cast<double>(blocks) / (static_cast<double>(sm_count()) * kRingBlocksPerSmF64);
     if (waves > 1.0 && waves < 3.0 && waves - static_cast<double>(static_cast<long long>(waves)) < 0.5)
         return kWindowVariantF64;
@@ -55,7 +55,9 @@ int default_variant_f64(const Layout& L) {
 cudaError_t launch_stage_f64(const StageArgs& a, cudaStream_t s) {
     const cudaError_t e = launch_boundary_flux<PolF64>(a, s);
     if (e != cudaSuccess) return e;
-    const int v = a.variant > 0 ? a.variant : default_variant_f64(a.L);
+    // (with the row chunk chosen per launch to fill whole waves, the ring
+    // variant stays; the fallback serves fixed chunks)
+    const int v = a.variant > 0 ? a.variant : a.rows > 0 ? default_variant_f64(a.L, a.rows) : kDefaultVariantF64;
     switch (march_features(a)) {
         case 0: return launch_march_f64_0(a, v, s);
         case 1: return launch_march_f64_1(a, v, s);

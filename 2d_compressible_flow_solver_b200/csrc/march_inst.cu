@@ -2,6 +2,7 @@
 //   -DCFS_MARCH_POL=PolF32|PolF64  -DCFS_MARCH_FEAT=0..7  -DCFS_MARCH_FN=<launcher name>
 // (the build gives each pair its own object, so the 160 kernels compile in
 // parallel).  The launcher runs the variant `v` of kVariants (1-based).
+#include <climits>
 #include <mutex>
 
 #include "cfs_kernels.cuh"
@@ -15,13 +16,43 @@
 namespace cfs {
 namespace {
 
+constexpr int kMaxDev = 64;
+
+// Row chunk of a launch whose blocks (bx per chunk of rows) run on `slots`
+// resident blocks.  An item costs its R rows plus about 2 more (the x-work of
+// the row above and below the chunk), and the launch ends with a partly
+// filled stretch of about half an item, so the launch lasts about
+// (R + 2) (blocks / slots + 1/2): short chunks pay the per-item rows, long
+// ones the tail.  The minimum lies near R = 2 sqrt(bx nrows / slots): 28 rows
+// at 4096^2, 14 at 2048^2, 7 at 1024^2 (FP32, 740 slots).  Fitted to a sweep of
+// fixed chunks of 8 .. 196 rows at 512^2 .. 4096^2, FP32 and FP64; a
+// whole-wave model that ignored the tail picked 196 rows at 4096^2 and lost
+// 12 % against 32.  Searched over 6 .. 128 rows (the whole range when it is
+// shorter), ties to the longer chunk.
+int choose_rows(int bx, int nrows, long long slots) {
+    if (nrows <= 6 || slots <= 0) return nrows <= 6 ? nrows : 32;
+    int best_r = 32;
+    long long best_cost = LLONG_MAX;
+    const int r_max = nrows < 128 ? nrows : 128;
+    for (int r = 6; r <= r_max; ++r) {
+        const long long blocks = static_cast<long long>(bx) * ((nrows + r - 1) / r);
+        const long long cost = static_cast<long long>(r + 2) * (2 * blocks + slots);
+        if (cost <= best_cost) {
+            best_cost = cost;
+            best_r = r;
+        }
+    }
+    return best_r;
+}
+
 template <class Pol, int R, int W, int B, int Ld, int F>
-cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
-    const int nseg = (a.L.ny + kSeg - 1) / kSeg;
-    const int nrows = stage_row_hi(a) - stage_row_lo(a);
+cudaError_t launch_march(const StageArgs& a_in, cudaStream_t s) {
+    const int nseg = (a_in.L.ny + kSeg - 1) / kSeg;
+    const int nrows = stage_row_hi(a_in) - stage_row_lo(a_in);
     if (nrows <= 0) return cudaSuccess;
-    const dim3 grid((nseg + W - 1) / W, (nrows + R - 1) / R);
+    const int bx = (nseg + W - 1) / W;
     size_t dyn = 0;
+    const StageArgs& a = a_in;
     if constexpr (Ld == 4) {
         if (!a.has_tmaps || !a.err) return cudaErrorInvalidValue;
     }
@@ -29,7 +60,6 @@ cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
         // the FP64 ring lives in dynamic shared memory; allow it once per
         // device (std::call_once: host threads may make their first launches
         // on one device at the same time)
-        constexpr int kMaxDev = 64;
         static std::once_flag once[kMaxDev];
         static cudaError_t allow_err[kMaxDev];
         dyn = static_cast<size_t>(W) * ring_words<double>() * sizeof(double);
@@ -48,7 +78,41 @@ cudaError_t launch_march(const StageArgs& a, cudaStream_t s) {
         }
         if (e != cudaSuccess) return e;
     }
-    march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(a);
+    int rows = a.rows;
+    if (rows <= 0) {
+        // resident blocks of this kernel (SMs x blocks per SM), once per device
+        static std::once_flag once_slots[kMaxDev];
+        static long long slots_of[kMaxDev];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        auto query = [dyn]() -> long long {
+            int per_sm = 0, sms = 0, d = 0;
+            if (cudaGetDevice(&d) != cudaSuccess ||
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march_kernel<Pol, R, W, B, Ld, F>, 32 * W,
+                                                              dyn) != cudaSuccess)
+                return 0;
+            return static_cast<long long>(per_sm) * sms;
+        };
+        long long slots = 0;
+        if (dev < 0 || dev >= kMaxDev) {
+            slots = query();
+        } else {
+            std::call_once(once_slots[dev], [&] { slots_of[dev] = query(); });
+            slots = slots_of[dev];
+        }
+        if (slots <= 0) (void)cudaGetLastError();  // a failed query leaves no error behind; fixed rows then
+        rows = slots > 0 ? choose_rows(bx, nrows, slots) : R;
+    }
+    const dim3 grid(bx, (nrows + rows - 1) / rows);
+    if (rows == a.rows) {
+        march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(a);
+    } else {
+        StageArgs b = a;
+        b.rows = rows;
+        march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(b);
+    }
     return cudaGetLastError();
 }
 

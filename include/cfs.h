@@ -125,6 +125,9 @@ typedef struct cfs_config {
                                 occupancy target, see cfs_variant_info); 0 = the tuned default */
     int positivity;          /* enum cfs_positivity */
     int rounding;            /* enum cfs_rounding (CFS_FP32_MIXED) */
+    int march_rows;          /* throughput forms: rows of one warp's work item in the row march;
+                                0 = chosen at each launch so the blocks fill whole waves of the
+                                GPU's resident blocks (the tuned default), > 0 = fixed (<= 4096) */
 } cfs_config;
 
 typedef struct cfs_ctx cfs_ctx;

@@ -63,3 +63,36 @@ def test_feature_sets_agree(cfsb, workloads, prec, tol):
         got = _run(cfsb, w, prec, 0, bc=per, **kw)
         err = np.abs(got - ref).max() / scale
         assert err <= tol, (kw.keys(), err)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_row_chunk_changes_no_bit(cfsb, workloads, prec):
+    """cfs_config.march_rows (rows of one warp's work item; 0 = chosen per
+    launch to fill whole waves): a chunk boundary only repeats the x-flux of
+    the face between two chunks in both, with the same arithmetic, so every
+    chunk gives the same state bit for bit, on a grid whose rows the chunks do
+    not divide, with transmissive sides and with a cylinder."""
+    quad = workloads.riemann_quadrants(150, 130, seed=9)
+    cyl = workloads.mach3_cylinder(192, 96)
+    for w, circle in ((quad, None), (cyl, cyl.circle)):
+        outs = []
+        for rows in (0, 1, 7, 32, 61, 500):
+            with cfsb.Solver(w.nx, w.ny, w.lx, w.ly, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
+                             bc=w.bc, bc_prim=w.bc_prim, march_rows=rows,
+                             positivity=cfsb.POSITIVITY_BODY if circle else cfsb.POSITIVITY_OFF) as s:
+                if circle:
+                    s.build_circle(*circle, 400, cfsb.IB_BILINEAR_SLIP)
+                s.set_state(w.U0)
+                t, _ = s.advance(4, cfl=0.5)
+                outs.append((s.get_state(), t))
+        assert np.all(np.isfinite(outs[0][0]))
+        for got, t in outs[1:]:
+            assert np.array_equal(got, outs[0][0])
+            assert t == outs[0][1]
+
+
+def test_row_chunk_out_of_range_is_refused(cfsb):
+    with pytest.raises(cfsb.CfsError):
+        cfsb.Solver(64, 64, march_rows=-1)
+    with pytest.raises(cfsb.CfsError):
+        cfsb.Solver(64, 64, march_rows=4097)
