@@ -313,8 +313,7 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
         c.L = cfs::Layout::make(d.nx, d.ny, b->elem);
         c.dx = d.lx / d.nx;
         c.dy = d.ly / d.ny;
-        c.rows = d.rows > 0 ? d.rows : cfs::kVariants[(b->prec == cfs::kF32Mixed ? cfs::kDefaultVariantF32
-                                                                                   : cfs::kDefaultVariantF64) - 1].rows;
+        c.rows = d.rows > 0 ? d.rows : cfs::kBatchRows;
         c.nseg = (d.ny + 29) / 30;
         c.items_y = (d.nx + c.rows - 1) / c.rows;
         c.state_off = arena;

@@ -91,6 +91,12 @@ constexpr int kBatchMinBlocksF64 = 4;
 // SM): the uneven 512-case batch 3,230 against 2,938 Mcell-steps/s without it
 // (the earlier ring that also held U^0 rows allowed 3 blocks and lost, 2,775).
 constexpr int kBatchLoadF64 = 3;
+// Rows of a batch work unit (cfs_case.rows = 0): the persistent warps pull
+// units until none are left, so the launch's tail is one unit per warp and
+// longer units cost less per row (the uneven 512-case batch: FP32 8,408 /
+// 8,651 / 8,763 / 8,838 / 8,854 and FP64 5,019 / 5,217 / 5,294 / 5,340 / 5,341
+// Mcell-steps/s at 16 / 24 / 32 / 48 / 64 rows).
+constexpr int kBatchRows = 64;
 cudaError_t launch_batch_stage(Prec p, const StageArgs* args, const int* item_case, const int* item_local,
                                const int* case_rows, const int* case_nseg, int total, unsigned int* counter,
                                int grid, int feat, cudaStream_t s);  // feat: kFeatPos | kFeatEdge bits

@@ -439,9 +439,9 @@ __global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArg
     boundary_face_flux<Pol>(a, s, k);
 }
 
-// One work item: rows [by*rows, by*rows + rows) of the kWarps segments of
-// block column bx.  Each warp works on its own segment; the warps of a block
-// share nothing but their slices of the row buffer.  kLoad, where global loads
+// One work item: rows [by*rows, by*rows + rows) of segment `seg` (columns
+// seg*30 .. seg*30+29), one warp.  The warps of a block share nothing but their
+// slices of the row buffer and their rings.  kLoad, where global loads
 // are issued (the trade is latency hidden against registers held):
 //   0 at their use;
 //   1 early in the iteration: the next row, the y halo columns and the RK
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(128) batch_boundary_flux_kernel(const StageArg
 // instruction cache stalls every warp on instruction fetch, whatever the share
 // of the rare code actually executed.
 template <class Pol, int kWarps, int kLoad, int kFeat>
-__device__ __forceinline__ bool march_item(const StageArgs& a, int bx, int by, int rows,
+__device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, int rows,
                                            typename Pol::C (&rbuf)[kWarps][36][kVars],
                                            typename Pol::T* ring, int wid, unsigned long long* bars = nullptr,
                                            unsigned* phase = nullptr) {
@@ -479,7 +479,6 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int bx, int by, i
     constexpr bool kEdge = (kFeat & kFeatEdge) != 0;
     const Layout& L = a.L;
     const int lane = threadIdx.x & 31;
-    const int seg = bx * kWarps + wid;
     const int j0 = seg * kSeg;
     const int i0 = stage_row_lo(a) + by * rows;
     const int i1 = min(i0 + rows, stage_row_hi(a));
@@ -950,6 +949,15 @@ template <class Pol, int kRows, int kWarps, int kMinBlocks, int kLoad, int kFeat
 __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __grid_constant__ StageArgs a) {
     // rows of this launch's work items: chosen by the launcher (a.rows), or the variant's
     const int rows = a.rows > 0 ? a.rows : kRows;
+    // warps numbered over (segment, row chunk), segments fastest, so no block
+    // carries idle warps when the segments of a row are not a multiple of its
+    // warps; a warp past the last item runs an empty one
+    const int nseg = (a.L.ny + kSeg - 1) / kSeg;
+    const long long nitems =
+        static_cast<long long>(nseg) * ((stage_row_hi(a) - stage_row_lo(a) + rows - 1) / rows);
+    const long long gw = static_cast<long long>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    const int seg = gw < nitems ? static_cast<int>(gw % nseg) : nseg;
+    const int by = gw < nitems ? static_cast<int>(gw / nseg) : 0;
     // (the ring forms use no row buffer)
     __shared__ __align__(16) typename Pol::C rbuf[kLoad >= 3 ? 1 : kWarps][36][kVars];
     using RB = typename Pol::C(&)[kWarps][36][kVars];
@@ -964,26 +972,26 @@ __global__ void __launch_bounds__(32 * kWarps, kMinBlocks) march_kernel(const __
         unsigned phase = 0u;
         if constexpr (sizeof(typename Pol::T) == 4) {
             __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
-            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf), ring, wid,
+            march_item<Pol, kWarps, kLoad, kFeat>(a, seg, by, rows, reinterpret_cast<RB>(rbuf), ring, wid,
                                                   bars[wid], &phase);
         } else {
             // FP64 ring: dynamic shared memory, sized at launch
             extern __shared__ __align__(128) unsigned char march_dyn_smem[];
-            march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf),
+            march_item<Pol, kWarps, kLoad, kFeat>(a, seg, by, rows, reinterpret_cast<RB>(rbuf),
                                                   reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid, bars[wid],
                                                   &phase);
         }
     } else if constexpr (kLoad == 3 && sizeof(typename Pol::T) == 4) {
         __shared__ __align__(128) typename Pol::T ring[kWarps * ring_words<typename Pol::T>()];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf), ring, wid);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, seg, by, rows, reinterpret_cast<RB>(rbuf), ring, wid);
     } else if constexpr (kLoad == 3) {
         // FP64 ring: kWarps * ring_words<double>() doubles (36.9 KB for 4
         // warps); dynamic shared memory, sized at launch
         extern __shared__ __align__(128) unsigned char march_dyn_smem[];
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, reinterpret_cast<RB>(rbuf),
+        march_item<Pol, kWarps, kLoad, kFeat>(a, seg, by, rows, reinterpret_cast<RB>(rbuf),
                                               reinterpret_cast<typename Pol::T*>(march_dyn_smem), wid);
     } else {
-        march_item<Pol, kWarps, kLoad, kFeat>(a, blockIdx.x, blockIdx.y, rows, rbuf, nullptr, threadIdx.x >> 5);
+        march_item<Pol, kWarps, kLoad, kFeat>(a, seg, by, rows, rbuf, nullptr, threadIdx.x >> 5);
     }
 }
 

@@ -45,7 +45,7 @@ int sm_count() {
 int default_variant_f64(const Layout& L, int rows) {
     const MarchVariant& d = kVariants[kDefaultVariantF64 - 1];
     const long long nseg = (L.ny + kSeg - 1) / kSeg;
-    const long long blocks = ((nseg + d.warps - 1) / d.warps) * ((L.nx + rows - 1) / rows);
+    const long long blocks = (nseg * ((L.nx + rows - 1) / rows) + d.warps - 1) / d.warps;
     const double waves = static_cast<double>(blocks) / (static_cast<double>(sm_count()) * kRingBlocksPerSmF64);
     if (waves > 1.0 && waves < 3.0 && waves - static_cast<double>(static_cast<long long>(waves)) < 0.5)
         return kWindowVariantF64;

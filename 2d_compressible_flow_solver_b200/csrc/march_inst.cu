@@ -18,24 +18,24 @@ namespace {
 
 constexpr int kMaxDev = 64;
 
-// Row chunk of a launch whose blocks (bx per chunk of rows) run on `slots`
-// resident blocks.  An item costs its R rows plus about 2 more (the x-work of
+// Row chunk of a launch whose warps (nseg per chunk of rows, w per block) run
+// on `slots` resident blocks.  An item costs its R rows plus about 2 more (the x-work of
 // the row above and below the chunk), and the launch ends with a partly
 // filled stretch of about half an item, so the launch lasts about
 // (R + 2) (blocks / slots + 1/2): short chunks pay the per-item rows, long
-// ones the tail.  The minimum lies near R = 2 sqrt(bx nrows / slots): 28 rows
+// ones the tail.  The minimum lies near R = 2 sqrt(nseg nrows / (w slots)): 28 rows
 // at 4096^2, 14 at 2048^2, 7 at 1024^2 (FP32, 740 slots).  Fitted to a sweep of
 // fixed chunks of 8 .. 196 rows at 512^2 .. 4096^2, FP32 and FP64; a
 // whole-wave model that ignored the tail picked 196 rows at 4096^2 and lost
 // 12 % against 32.  Searched over 6 .. 128 rows (the whole range when it is
 // shorter), ties to the longer chunk.
-int choose_rows(int bx, int nrows, long long slots) {
+int choose_rows(int nseg, int w, int nrows, long long slots) {
     if (nrows <= 6 || slots <= 0) return nrows <= 6 ? nrows : 32;
     int best_r = 32;
     long long best_cost = LLONG_MAX;
     const int r_max = nrows < 128 ? nrows : 128;
     for (int r = 6; r <= r_max; ++r) {
-        const long long blocks = static_cast<long long>(bx) * ((nrows + r - 1) / r);
+        const long long blocks = (static_cast<long long>(nseg) * ((nrows + r - 1) / r) + w - 1) / w;
         const long long cost = static_cast<long long>(r + 2) * (2 * blocks + slots);
         if (cost <= best_cost) {
             best_cost = cost;
@@ -50,7 +50,6 @@ cudaError_t launch_march(const StageArgs& a_in, cudaStream_t s) {
     const int nseg = (a_in.L.ny + kSeg - 1) / kSeg;
     const int nrows = stage_row_hi(a_in) - stage_row_lo(a_in);
     if (nrows <= 0) return cudaSuccess;
-    const int bx = (nseg + W - 1) / W;
     size_t dyn = 0;
     const StageArgs& a = a_in;
     if constexpr (Ld == 4) {
@@ -103,9 +102,11 @@ cudaError_t launch_march(const StageArgs& a_in, cudaStream_t s) {
             slots = slots_of[dev];
         }
         if (slots <= 0) (void)cudaGetLastError();  // a failed query leaves no error behind; fixed rows then
-        rows = slots > 0 ? choose_rows(bx, nrows, slots) : R;
+        rows = slots > 0 ? choose_rows(nseg, W, nrows, slots) : R;
     }
-    const dim3 grid(bx, (nrows + rows - 1) / rows);
+    // one warp per (segment, row chunk), segments fastest
+    const long long items = static_cast<long long>(nseg) * ((nrows + rows - 1) / rows);
+    const dim3 grid(static_cast<unsigned>((items + W - 1) / W));
     if (rows == a.rows) {
         march_kernel<Pol, R, W, B, Ld, F><<<grid, 32 * W, dyn, s>>>(a);
     } else {

@@ -62,9 +62,11 @@ WORDS_PER_CELL_STEP = 32
 MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
 # Floating-point operations the FP32-mixed march executes per cell-step (its
 # three stage launches; packed FFMA2 = 4, FADD2/FMUL2 = 2, FFMA/DFMA = 2, others
-# 1), from ncu's per-opcode thread-instruction counts (sm__sass_thread_inst_
-# executed_op_*) of a periodic 2048^2 run.  Data-independent on smooth states.
-MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2927.9, "fp64": 27.9}}
+# 1), from ncu's per-opcode instruction counts (sass__inst_executed_per_opcode)
+# of the interleaved-cell march on a periodic 2048^2 run: 906.4 FP32 flops per
+# cell-stage, times 3; the FP64 flops are the step-ending stage's exact sums
+# before stochastic rounding.  Data-independent on smooth states.
+MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2719.3, "fp64": 27.9}}
 # The reference's scheme as its own driver runs it (Run.cpp:41-48 with
 # TVD3rdRK, RiemmanSolverHLL, transmissive sides, fixed dt): what the
 # reference arm times, and the engine's like-for-like companion rate.

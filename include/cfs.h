@@ -356,7 +356,7 @@ typedef struct cfs_case {
     double radius, cx, cy;
     int npoints;
     int ib_mode;             /* enum cfs_ib_mode */
-    int rows;                /* row chunk of a work item (0: from the tuning default) */
+    int rows;                /* row chunk of a work item (0: the default, 64 rows) */
     int edge_code;           /* 1: run this case with the row march's edge code even where it
                                 needs none (no physical side, no body): its work items join the
                                 launch of the cases that need it, one launch fewer per stage when
