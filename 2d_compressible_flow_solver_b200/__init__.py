@@ -26,7 +26,7 @@ __all__ = [
     "HLL_REFERENCE", "HLL_DAVIS", "BC_NEUMANN", "BC_DIRICHLET", "BC_PERIODIC", "BC_HALO",
     "CELL_FLUID", "CELL_SOLID", "CELL_IMMERSED_GHOST", "IB_REFERENCE", "IB_BILINEAR_SLIP",
     "VISCOUS_OFF", "VISCOUS_NS", "POSITIVITY_OFF", "POSITIVITY_FACE", "POSITIVITY_BODY", "POSITIVITY_FLOOR", "ROUND_STOCHASTIC",
-    "ROUND_NEAREST", "PART_ALL", "PART_INTERIOR", "PART_EDGES", "variants", "fp_peaks",
+    "ROUND_NEAREST", "ROUND_STOCHASTIC_ALL", "PART_ALL", "PART_INTERIOR", "PART_EDGES", "variants", "fp_peaks",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -41,7 +41,7 @@ CELL_FLUID, CELL_SOLID, CELL_IMMERSED_GHOST = 0, 1, 2
 IB_REFERENCE, IB_BILINEAR_SLIP = 0, 1
 VISCOUS_OFF, VISCOUS_NS = 0, 1
 POSITIVITY_OFF, POSITIVITY_FACE, POSITIVITY_BODY, POSITIVITY_FLOOR = 0, 1, 2, 3
-ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
+ROUND_STOCHASTIC, ROUND_NEAREST, ROUND_STOCHASTIC_ALL = 0, 1, 2
 PART_ALL, PART_INTERIOR, PART_EDGES = 0, 1, 2
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)

@@ -152,7 +152,8 @@ int validate(const cfs_config* g, std::string& msg) {
         msg = "unknown positivity mode";
         return CFS_ERR_INVALID;
     }
-    if (g->rounding != CFS_ROUND_STOCHASTIC && g->rounding != CFS_ROUND_NEAREST) {
+    if (g->rounding != CFS_ROUND_STOCHASTIC && g->rounding != CFS_ROUND_NEAREST &&
+        g->rounding != CFS_ROUND_STOCHASTIC_ALL) {
         msg = "unknown rounding mode";
         return CFS_ERR_INVALID;
     }

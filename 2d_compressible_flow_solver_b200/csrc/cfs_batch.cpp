@@ -264,7 +264,8 @@ int cfs_batch_create(const cfs_config* common, int ncases, const cfs_case* cases
     if (common->viscous != CFS_VISCOUS_OFF) return bfail(nullptr, CFS_ERR_INVALID, "batches are inviscid");
     if (common->positivity < CFS_POSITIVITY_OFF || common->positivity > CFS_POSITIVITY_FLOOR)
         return bfail(nullptr, CFS_ERR_INVALID, "unknown positivity mode");
-    if (common->rounding != CFS_ROUND_STOCHASTIC && common->rounding != CFS_ROUND_NEAREST)
+    if (common->rounding != CFS_ROUND_STOCHASTIC && common->rounding != CFS_ROUND_NEAREST &&
+        common->rounding != CFS_ROUND_STOCHASTIC_ALL)
         return bfail(nullptr, CFS_ERR_INVALID, "unknown rounding mode");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

@@ -516,7 +516,7 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, 
     // gain in accuracy (smooth advection, 128^2 to t = 0.5: density L1 error
     // against FP64 6.4e-8 either way, 2.8e-7 with round-to-nearest throughout).
     const bool last_of_step = a.rk == kRkTvd2 ? a.stage == 1 : a.stage == 2;
-    const bool sr = Pol::kMixed && a.rounding == 0 && last_of_step;
+    const bool sr = Pol::kMixed && ((a.rounding == 0 && last_of_step) || a.rounding == 2);
     const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
     // physical boundary faces: fluxes precomputed (boundary_flux_kernel)
     const bool lo_x = kEdge && physical_side(a, 0), hi_x = kEdge && physical_side(a, 1);

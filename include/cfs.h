@@ -104,7 +104,8 @@ enum cfs_rounding {
                                   to one of its two neighbouring floats with probability by nearness
                                   (random bits hashed from cell and step): an unbiased error that does
                                   not build up; intermediate stage states round to nearest */
-    CFS_ROUND_NEAREST = 1      /* FP32 FMA update, round to nearest */
+    CFS_ROUND_NEAREST = 1,     /* FP32 FMA update, round to nearest */
+    CFS_ROUND_STOCHASTIC_ALL = 2 /* as CFS_ROUND_STOCHASTIC in every stage, intermediate ones included */
 };
 
 typedef struct cfs_config {
