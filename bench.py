@@ -770,8 +770,9 @@ def _report_convergence(cfsb, wl, nmax: int) -> dict:
         dt = w.t_end / nsteps
         exact = wl.smooth_advection_exact(n, w.t_end)
         res = {}
-        for prec, key in ((cfsb.FP64, "fp64"), (cfsb.FP32_MIXED, "fp32")):
-            with cfsb.Solver(n, n, precision=prec, **kw) as s:
+        for prec, key, rnd in ((cfsb.FP64, "fp64", cfsb.ROUND_STOCHASTIC), (cfsb.FP32_MIXED, "fp32", cfsb.ROUND_STOCHASTIC),
+                               (cfsb.FP32_MIXED, "fp32_sr_all", cfsb.ROUND_STOCHASTIC_ALL)):
+            with cfsb.Solver(n, n, precision=prec, rounding=rnd, **kw) as s:
                 s.set_state(w.U0)
                 m0 = s.totals()
                 s.advance(nsteps, dt=dt)
@@ -782,7 +783,9 @@ def _report_convergence(cfsb, wl, nmax: int) -> dict:
                "rho_L1_fp64_vs_exact": res["fp64"][1], "rho_L1_fp32_vs_exact": res["fp32"][1],
                "rho_L1_fp32_vs_fp64": float(np.abs(res["fp32"][0][0] - res["fp64"][0][0]).mean()),
                "rho_Linf_fp32_vs_fp64": float(np.abs(res["fp32"][0][0] - res["fp64"][0][0]).max()),
-               "mass_drift_fp64": res["fp64"][2], "mass_drift_fp32": res["fp32"][2]}
+               "mass_drift_fp64": res["fp64"][2], "mass_drift_fp32": res["fp32"][2],
+               "rho_L1_fp32_sr_all_vs_fp64": float(np.abs(res["fp32_sr_all"][0][0] - res["fp64"][0][0]).mean()),
+               "mass_drift_fp32_sr_all": res["fp32_sr_all"][2]}
         if prev is not None:
             row["order_fp64"] = math.log2(prev["rho_L1_fp64_vs_exact"] / row["rho_L1_fp64_vs_exact"])
             row["order_fp32"] = math.log2(prev["rho_L1_fp32_vs_exact"] / row["rho_L1_fp32_vs_exact"])
