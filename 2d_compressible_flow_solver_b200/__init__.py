@@ -271,7 +271,7 @@ class Solver:
                  rk: int = RK_TVD3_REFERENCE, hll: int = HLL_REFERENCE, bc=(BC_NEUMANN,) * 4, bc_prim=None,
                  gamma: float = 1.4, weno_eps: float = 1e-2, viscous: int = VISCOUS_OFF, mu: float = 1e-3,
                  prandtl: float = 0.72, mach: float = 1.0, keep_rhs: bool = False, device: int = 0,
-                 variant: int = 0, positivity: int = 0, rounding: int = ROUND_STOCHASTIC, march_rows: int = 0):
+                 variant: int = 0, positivity: int = 0, rounding: int = ROUND_STOCHASTIC_ALL, march_rows: int = 0):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
@@ -498,7 +498,7 @@ class Batch:
 
     def __init__(self, cases, *, precision: int = FP32_MIXED, rk: int = RK_SSP3, hll: int = HLL_DAVIS,
                  gamma: float = 1.4, weno_eps: float = 1e-2, device: int = 0, positivity: int = POSITIVITY_OFF,
-                 rounding: int = ROUND_STOCHASTIC):
+                 rounding: int = ROUND_STOCHASTIC_ALL):
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))

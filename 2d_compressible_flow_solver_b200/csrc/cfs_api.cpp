@@ -419,6 +419,7 @@ void cfs_config_default(cfs_config* g) {
     g->mu = 1e-3;
     g->prandtl = 0.72;
     g->mach = 1.0;
+    g->rounding = CFS_ROUND_STOCHASTIC_ALL;
 }
 
 const char* cfs_last_error(const cfs_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }

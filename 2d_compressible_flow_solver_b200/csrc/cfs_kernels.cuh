@@ -409,19 +409,19 @@ __device__ __forceinline__ unsigned int cell_hash(int i, int j, unsigned int ste
                   step_seed * 0xc2b2ae3du);
 }
 
-// x rounded to float stochastically with the 8 random bits u8: round to
-// nearest of x + (u - 1/2) g, with u = (u8 + 1/2)/256 and g the float spacing
-// of the binade of RN(x).  For x between neighbouring floats f < x < f + g this
-// picks f + g with probability (x - f)/g.  Just below a power of two the
-// spacing halves, so there the choice is only approximately unbiased; tiny and
-// non-finite values round to nearest.
-__device__ __forceinline__ float round_stochastic(double x, unsigned int u8) {
-    const float f = __double2float_rn(x);
-    const unsigned int eb = __float_as_uint(f) & 0x7f800000u;
-    if (eb <= (24u << 23) || eb == 0x7f800000u) return f;
-    const float g = __uint_as_float(eb - (23u << 23));
-    const float noise = (static_cast<float>(u8) - 127.5f) * (1.0f / 256.0f) * g;
-    return __double2float_rn(x + static_cast<double>(noise));
+// Dither of stochastic rounding for a result near f: uniform over one float
+// spacing g of f's binade, (u + 1/2)/256 - 1/2 times g for the 8 random bits u
+// (the low byte of `bits`), built by placing u in the mantissa of a float in
+// [1, 2).  Added to a value x between neighbouring floats lo < x < lo + g
+// before one round-to-nearest, it picks lo + g with probability (x - lo)/g (to
+// 1/256).  Just below a power of two the spacing halves, so there the choice
+// is only approximately unbiased; for |f| below 2^-103 the dither is 0 (round
+// to nearest).
+__device__ __forceinline__ float sr_dither(float f, unsigned int bits) {
+    const int eb = static_cast<int>(__float_as_uint(f) & 0x7f800000u);
+    const float g = __int_as_float(max(eb - (23 << 23), 0));
+    const float m = __uint_as_float(0x3f800000u | ((bits & 255u) << 15) | (1u << 14));
+    return fmaf(m, g, -1.5f * g);
 }
 
 // Positivity floors of CFS_POSITIVITY_FLOOR (no reference counterpart): a new

@@ -57,17 +57,17 @@ constexpr MarchVariant kVariants[kNumVariants] = {
     {32, 4, 5, 2}, {32, 4, 5, 3}, {32, 4, 4, 3}, {64, 4, 4, 3}, {32, 4, 6, 3},
     {32, 4, 5, 4}, {32, 4, 4, 4}, {64, 4, 4, 4},
 };
-// 1-based defaults, the 4096^2 winners of the committed tuning table
+// 1-based defaults, from the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json): FP32 stages its ring rows by
 // per-lane 16-byte cp.async (variant 7: 10,356 Mcell-steps/s against 10,216 for
 // the same shape staged by TMA, whose lane-0 issue and mbarrier waits cost
 // more instructions than the copies they replace once cells are interleaved);
-// FP64 stages them by TMA (variant 12: 5,880 against 5,777 for the same shape
-// by cp.async, and ahead at 1024^2 and 2048^2 too; with the cubically refined
-// reciprocal and square root and the branch-free HLL the cp.async form needs a
-// few more registers than 128 and spills 8 bytes, the TMA form none).
+// FP64 by cp.async too (variant 8): with the row chunk chosen per launch it
+// matches the TMA ring on periodic grids (4096^2: 5,987 against 5,999
+// Mcell-steps/s) and wins with edge code (2048^2 transmissive 5,186 against
+// 5,120, with floors and a cylinder 4,734 against 4,448).
 constexpr int kDefaultVariantF32 = 7;
-constexpr int kDefaultVariantF64 = 12;
+constexpr int kDefaultVariantF64 = 8;
 // FP32 grids with edge code (physical sides, cell types) run the same ring
 // march with 128 registers and 4 blocks per SM: 2048^2 transmissive with floors
 // and a cylinder 5,672 against 5,476 Mcell-steps/s, the 2048 x 1024 Mach-3

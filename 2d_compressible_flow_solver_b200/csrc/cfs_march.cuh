@@ -510,11 +510,11 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, 
         x1_u1 = a.rk == kRkTvd3Ref;
     }
     const float cdt = float(cdtd);
-    // Stochastic rounding of the state that ends each step (the last stage);
-    // the intermediate stage states are rounded to nearest: they are
-    // temporaries, and rounding them stochastically too gives no measurable
-    // gain in accuracy (smooth advection, 128^2 to t = 0.5: density L1 error
-    // against FP64 6.4e-8 either way, 2.8e-7 with round-to-nearest throughout).
+    // Stochastic rounding of the state that ends each step (the last stage), or
+    // of every stage (CFS_ROUND_STOCHASTIC_ALL); otherwise round to nearest.
+    // Rounding an intermediate stage to nearest leaves a small mass bias: its
+    // increments are dt times differences of FP32 fluxes, a coarse lattice on
+    // the stored grid, so the rounding errors do not average out.
     const bool last_of_step = a.rk == kRkTvd2 ? a.stage == 1 : a.stage == 2;
     const bool sr = Pol::kMixed && ((a.rounding == 0 && last_of_step) || a.rounding == 2);
     const unsigned int step_seed = (a.P ? a.P->seed[a.parity] : a.seed) * 4u + static_cast<unsigned int>(a.stage);
@@ -770,30 +770,47 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, 
                 if constexpr (Pol::kMixed) {
                     // FP32 update of the stored deviations (value - off): the RK
                     // coefficients of a stage sum to 1, so the offsets cancel and
-                    // the rounding step is that of the deviation.  Stochastic
-                    // rounding forms the new deviation exactly in FP64 (float
-                    // products are exact there) and rounds it once.
+                    // the rounding step is that of the deviation.
                     // (formed for every cell and selected: a non-fluid cell keeps its state)
-                    const unsigned int h = sr ? cell_hash(i, j, step_seed) : 0u;
+                    float rvf[kVars], x0[kVars], x1[kVars], ndv[kVars];
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) {
-                        float rvf = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
-                        if (kExtra && rv_in && v >= 1) rvf += rv_cur[v - 1];
-                        const float cur = pf_cur[v];
-                        const float x0 = a.stage == 0 ? cur : pf_u0[v];
-                        const float x1 = a.stage == 0 ? 0.0f : (x1_u1 ? u1c[v] : cur);
-                        float nd;
-                        if (sr) {
-                            const double tot = fma(cdtd, double(rvf), fma(double(cA), double(x0), double(cB) * double(x1)));
-                            nd = round_stochastic(tot, (h >> (8 * v)) & 255u);
-                        } else {
-                            nd = fmaf(cdt, rvf, fmaf(cA, x0, cB * x1));
+                        rvf[v] = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
+                        if (kExtra && rv_in && v >= 1) rvf[v] += rv_cur[v - 1];
+                        x0[v] = a.stage == 0 ? pf_cur[v] : pf_u0[v];
+                        x1[v] = a.stage == 0 ? 0.0f : (x1_u1 ? u1c[v] : pf_cur[v]);
+                    }
+                    if (sr) {
+                        // Stochastic rounding of x0 + cB (x1 - x0) + cdt R (cA = 1 - cB
+                        // exactly): the increment is formed first, at its own
+                        // spacing (roundings near 1e-12 of the state, far below the
+                        // stored spacing), gets a dither uniform over one stored
+                        // spacing of the result's binade, and is added to x0 with
+                        // one rounding; two variables per packed instruction.
+                        const unsigned int h = cell_hash(i, j, step_seed);
+#pragma unroll
+                        for (int v = 0; v < kVars; v += 2) {
+                            const float2 a0 = make_float2(x0[v], x0[v + 1]);
+                            const float2 inc = fma2(p2(cB), sub2(make_float2(x1[v], x1[v + 1]), a0),
+                                                    mul2(p2(cdt), make_float2(rvf[v], rvf[v + 1])));
+                            const float2 f = add2(a0, inc);
+                            const float2 dz = make_float2(sr_dither(f.x, h >> (8 * v)), sr_dither(f.y, h >> (8 * v + 8)));
+                            const float2 r = add2(a0, add2(inc, dz));
+                            ndv[v] = r.x;
+                            ndv[v + 1] = r.y;
                         }
-                        nd = fluid ? nd : cur;
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < kVars; ++v) ndv[v] = fmaf(cdt, rvf[v], fmaf(cA, x0[v], cB * x1[v]));
+                    }
+#pragma unroll
+                    for (int v = 0; v < kVars; ++v) {
+                        const float cur = pf_cur[v];
+                        const float nd = fluid ? ndv[v] : cur;
                         sv[v] = nd;
                         nv[v] = nd + L.off[v];
                         if (kExtra && rhs_out)
-                            rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf) : 0.0;
+                            rhs_out[static_cast<long long>(v) * L.nx * L.ny + static_cast<long long>(i) * L.ny + j] = fluid ? double(rvf[v]) : 0.0;
                     }
                 } else {
 #pragma unroll

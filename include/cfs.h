@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CFS_ABI_VERSION 2
+#define CFS_ABI_VERSION 3
 
 enum cfs_status {
     CFS_OK = 0,
@@ -98,14 +98,18 @@ enum cfs_positivity {
 };
 
 /* Rounding of the FP32 state storage of CFS_FP32_MIXED (no reference
- * counterpart; the FP64 forms round to nearest). */
+ * counterpart; the FP64 forms round to nearest).  cfs_config_default selects
+ * CFS_ROUND_STOCHASTIC_ALL. */
 enum cfs_rounding {
-    CFS_ROUND_STOCHASTIC = 0,  /* the state that ends each RK step is formed exactly in FP64 and rounded
-                                  to one of its two neighbouring floats with probability by nearness
-                                  (random bits hashed from cell and step): an unbiased error that does
-                                  not build up; intermediate stage states round to nearest */
+    CFS_ROUND_STOCHASTIC = 0,  /* the state that ends each RK step is rounded to one of its two
+                                  neighbouring floats with probability by nearness (random bits
+                                  hashed from cell and step): an unbiased error that does not build
+                                  up; intermediate stage states round to nearest */
     CFS_ROUND_NEAREST = 1,     /* FP32 FMA update, round to nearest */
-    CFS_ROUND_STOCHASTIC_ALL = 2 /* as CFS_ROUND_STOCHASTIC in every stage, intermediate ones included */
+    CFS_ROUND_STOCHASTIC_ALL = 2 /* as CFS_ROUND_STOCHASTIC in every stage, intermediate ones included:
+                                    rounding an intermediate stage to nearest leaves a small mass bias
+                                    per step (its increments lie on a coarse lattice of the stored
+                                    grid); stochastically, the mass error stays a random walk */
 };
 
 typedef struct cfs_config {

@@ -25,13 +25,14 @@ def test_every_declared_entry_point_is_exported_and_bound(cfsb):
 
 def test_abi_version_and_defaults(cfsb):
     lib = cfsb.load_library()
-    assert lib.cfs_abi_version() == 2
+    assert lib.cfs_abi_version() == 3
     import ctypes
     cfg = cfsb.CfsConfig()
     lib.cfs_config_default(ctypes.byref(cfg))
     assert cfg.gamma == 1.4 and cfg.weno_eps == 1e-2
     assert cfg.rk == cfsb.RK_TVD3_REFERENCE and cfg.hll == cfsb.HLL_REFERENCE
     assert list(cfg.bc) == [cfsb.BC_NEUMANN] * 4
+    assert cfg.rounding == cfsb.ROUND_STOCHASTIC_ALL and cfg.march_rows == 0
 
 
 @pytest.mark.parametrize("kw,msg", [
