@@ -61,12 +61,12 @@ WORDS_PER_CELL_STEP = 32
 # per launch, the three stage launches of one warm step).
 MEASURED_TRAFFIC_BYTES_PER_CELL_LAUNCH = {"f32": 41.6, "f64": None}
 # Floating-point operations the FP32-mixed march executes per cell-step (its
-# three stage launches; packed FFMA2 = 4, FADD2/FMUL2 = 2, FFMA/DFMA = 2, others
-# 1), from ncu's per-opcode instruction counts (sass__inst_executed_per_opcode)
-# of the interleaved-cell march on a periodic 2048^2 run: 906.4 FP32 flops per
-# cell-stage, times 3; the FP64 flops are the step-ending stage's exact sums
-# before stochastic rounding.  Data-independent on smooth states.
-MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2719.3, "fp64": 27.9}}
+# three stage launches; packed FFMA2 = 4, FADD2/FMUL2/FFMA/DFMA = 2, others 1),
+# from ncu's per-opcode instruction counts (sass__inst_executed_per_opcode) of
+# the three stage launches of one step on a periodic 2048^2 run with 32-row
+# work items, as at 4096^2, and stochastic rounding in every stage (the
+# defaults).  Data-independent on smooth states.
+MEASURED_FLOPS_PER_CELL_STEP = {"f32": {"fp32": 2814.1, "fp64": 3.8}}
 # The reference's scheme as its own driver runs it (Run.cpp:41-48 with
 # TVD3rdRK, RiemmanSolverHLL, transmissive sides, fixed dt): what the
 # reference arm times, and the engine's like-for-like companion rate.
@@ -955,7 +955,7 @@ def modes_arm(args):
         extra = dict(viscous=cfsb.VISCOUS_NS, mu=w.meta["mu"], prandtl=0.72, mach=1.0) if ns else {}
         with cfsb.Solver(n, n, 1.0, 1.0, precision=prec, rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS,
                          bc=(getattr(cfsb, side),) * 4, positivity=getattr(cfsb, pos), variant=args.variant,
-                         **extra) as s:
+                         march_rows=args.march_rows, **extra) as s:
             if cyl:
                 s.build_circle(0.1, 0.5, 0.5, 400, cfsb.IB_BILINEAR_SLIP)
             s.set_state(w.U0)
@@ -1002,6 +1002,8 @@ def main():
     ap.add_argument("--mode", choices=list(MODES), default=None, help="modes workload: run this mode only (FP32)")
     ap.add_argument("--variant", type=int, default=0, help="modes workload: stage-kernel variant (0 = default)")
     ap.add_argument("--form", choices=["f32", "f64"], default="f32", help="modes workload with --mode: the form to run")
+    ap.add_argument("--march-rows", type=int, default=0,
+                    help="modes workload: rows of a row-march work item (0 = chosen per launch)")
     ap.add_argument("--report-parts", default="quadrants,cylinder,shear,batch,convergence",
                     help="report workload: comma-separated parts to run")
     ap.add_argument("--batch-steps", type=int, default=500, help="report workload: steps of the batch comparison")
