@@ -754,9 +754,10 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, 
 #pragma unroll
                     for (int v = 0; v < kVars; ++v) pf_cur[v] = cs[v];
                     if constexpr (kU0Ring) {
-                        const T* us = ring_u0(i) + (lane + 2) * kVars;
+                        // U^0 (stage 0: the current state, the update's x0 then)
+                        const T* us = (a.stage >= 1 ? ring_u0(i) : ring_row(i)) + (lane + 2) * kVars;
 #pragma unroll
-                        for (int v = 0; v < kVars; ++v) pf_u0[v] = a.stage >= 1 ? us[v] : T(0);
+                        for (int v = 0; v < kVars; ++v) pf_u0[v] = us[v];
                     }
                 } else if constexpr (kL == 0) {
                     load_update(i);
@@ -777,8 +778,9 @@ __device__ __forceinline__ bool march_item(const StageArgs& a, int seg, int by, 
                     for (int v = 0; v < kVars; ++v) {
                         rvf[v] = -(FX[v] - FXp[v]) * inv_dxf + RY[v];
                         if (kExtra && rv_in && v >= 1) rvf[v] += rv_cur[v - 1];
-                        x0[v] = a.stage == 0 ? pf_cur[v] : pf_u0[v];
-                        x1[v] = a.stage == 0 ? 0.0f : (x1_u1 ? u1c[v] : pf_cur[v]);
+                        x0[v] = (kU0Ring || a.stage >= 1) ? pf_u0[v] : pf_cur[v];
+                        // (stage 0: cB = 0 and x1 - x0 = 0, so x1 adds nothing)
+                        x1[v] = x1_u1 ? u1c[v] : pf_cur[v];
                     }
                     if (sr) {
                         // Stochastic rounding of x0 + cB (x1 - x0) + cdt R (cA = 1 - cB
