@@ -30,6 +30,7 @@
 //     m_interpolation = std::make_shared<cfs_plugins::GpuInterpolation>();
 //     m_riemmansolver = std::make_shared<cfs_plugins::GpuRiemannSolver>();
 //     m_timeadvance = std::make_shared<cfs_plugins::GpuExplicit>(gpu);
+//     gradient = std::make_shared<cfs_plugins::GpuGradient>();  // Run.cpp:8, if used
 // and gpu->sync_to_host() before the final Output::WriteToHDF5 (Run.cpp:235).
 #pragma once
 
@@ -40,6 +41,7 @@
 // so it is reached only through the guarded RiemmanSolverHLL.h, as the
 // reference's own sources do.
 #include "flux/RiemmanSolverHLL.h"
+#include "gradient/FourthOrderCS.h"
 #include "interpolation/Interpolation.h"
 #include "meshes/Cell.h"
 #include "model/EulerMod.h"
@@ -118,6 +120,17 @@ public:
 
 private:
     std::shared_ptr<Flux> zero_ = std::make_shared<EulerFlux>(0.0, Flux::Coord(0.0, 0.0), 0.0);
+};
+
+// Gradient plugin (ForthOrderCS, FourthOrderCS.h:15-16): the viscous
+// derivatives and face fluxes are computed inside the GPU stage when the
+// session's config selects CFS_VISCOUS_NS (cfg.mu, cfg.prandtl, cfg.mach), so
+// the per-face and per-cell calls, which the reference's loop makes only if its
+// commented-out gradient calls (Run.cpp:175-179, 188) are restored, do nothing.
+class GpuGradient : public ForthOrderCS {
+public:
+    void comviscousfluxForcellinterface(CellInterface*, std::list<Cell*>&, Direction) override {}
+    void comprimitivederivativeForcell(Cell*, std::vector<Cell*>&, Direction) override {}
 };
 
 // Explicit (time-advance) plugin: one GPU stage per loop iteration.

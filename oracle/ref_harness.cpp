@@ -515,6 +515,7 @@ int ref_gpu_run(const ref_config* c, const double* U_in, int nstages, int precis
         model = std::make_shared<cfs_plugins::GpuModel>();
         interpolation = std::make_shared<cfs_plugins::GpuInterpolation>();
         riemmansolver = std::make_shared<cfs_plugins::GpuRiemannSolver>();
+        gradient = std::make_shared<cfs_plugins::GpuGradient>();
         s.rk = std::make_shared<cfs_plugins::GpuExplicit>(gpu);
         preloop(s, c->dt);
         for (int i = 1; i <= nstages; ++i) stage(s, i);
