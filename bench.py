@@ -375,11 +375,13 @@ def engine_arm(args):
             "rho_L1_fp64_vs_exact": float(np.abs(U64[0] - exact).mean()),
         }
     # end to end through the C ABI with pinned host buffers: initial state up,
-    # K steps each reading back its dt and time, final state down
-    if rank == 0:
-        pin = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
-        pin.numpy()[:] = w.U0
-        out = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
+    # K steps each reading back its dt and time, final state down; at N GPUs
+    # every rank does this for its slab through parallel.SlabSolver (halo
+    # exchange and the global CFL step included), wall time maxed over ranks
+    pin = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
+    pin.numpy()[:] = w.U0
+    out = torch.empty((4, n, n), dtype=torch.float64, pin_memory=True)
+    if world == 1:
         with cfsb.Solver(n, n, precision=cfsb.FP32_MIXED, variant=variants[cfsb.FP32_MIXED], **kw) as s:
             s.set_state(pin.numpy())
             s.advance(2, cfl=w.cfl)
@@ -390,13 +392,34 @@ def engine_arm(args):
                 s.advance(1, cfl=w.cfl)
             s.get_state(out.numpy())
             wall = time.perf_counter() - t0
+    else:
+        par = importlib.import_module(f"{PKG}.parallel")
+        s = par.SlabSolver(n * world, n, float(world), 1.0, dist=dist, rank=rank, world=world, device=local,
+                           bc=(cfsb.BC_PERIODIC,) * 4, precision=cfsb.FP32_MIXED,
+                           variant=variants[cfsb.FP32_MIXED], rk=cfsb.RK_SSP3, hll=cfsb.HLL_DAVIS)
+        s.set_state(pin.numpy())
+        s.advance(2, w.cfl)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        s.set_state(pin.numpy())
+        for _ in range(K):
+            s.advance(1, w.cfl)
+        s.solver.get_state(out.numpy())
+        wall_t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(wall_t, op=dist.ReduceOp.MAX)
+        wall = float(wall_t.item())
+        s.close()
+    if rank == 0:
         state_bytes = 4 * cells * 8
-        result["e2e"] = {"value": round(cells * K / wall / 1e6, 1), "unit": UNIT, "steps": K,
+        result["e2e"] = {"value": round(cells * world * K / wall / 1e6, 1), "unit": UNIT, "steps": K,
                          "h2d_bytes_per_step": int(state_bytes / K + 40),
                          "d2h_bytes_per_step": int(state_bytes / K + 48),
-                         "how": "cfs_set_state from pinned host, K x cfs_advance(1) with dt/t read back, "
-                                "cfs_get_state to pinned host; host wall clock.  One FP64 state (537 MB) goes "
-                                "up and one comes down per run, so the rate depends on K (the steps field)"}
+                         "how": "per GPU: cfs_set_state from pinned host, K x cfs_advance(1) with dt/t read back "
+                                "(at N GPUs through parallel.SlabSolver: halo exchange and global CFL step), "
+                                "cfs_get_state to pinned host; host wall clock, max over ranks.  One FP64 state "
+                                "(537 MB) per GPU goes up and one comes down per run, so the rate depends on K "
+                                "(the steps field)"}
     # the uneven 512-case batch (persistent batched engine), bounded: K steps
     # per form, device-timed with CUDA events on the batch's stream
     if rank == 0 and world == 1 and args.batch_cases > 0:
