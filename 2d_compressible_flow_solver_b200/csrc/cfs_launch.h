@@ -59,13 +59,14 @@ constexpr MarchVariant kVariants[kNumVariants] = {
 };
 // 1-based defaults, from the committed tuning table
 // (2d_compressible_flow_solver_b200/tuning.json): FP32 stages its ring rows by
-// per-lane 16-byte cp.async (variant 7: 10,356 Mcell-steps/s against 10,216 for
-// the same shape staged by TMA, whose lane-0 issue and mbarrier waits cost
-// more instructions than the copies they replace once cells are interleaved);
-// FP64 by cp.async too (variant 8): with the row chunk chosen per launch it
-// matches the TMA ring on periodic grids (4096^2: 5,987 against 5,999
-// Mcell-steps/s) and wins with edge code (2048^2 transmissive 5,186 against
-// 5,120, with floors and a cylinder 4,734 against 4,448).
+// per-lane 16-byte cp.async (variant 7: 10,937 Mcell-steps/s at 4096^2 against
+// 10,552 for the same shape staged by TMA, whose lane-0 issue and mbarrier
+// waits cost more instructions than the copies they replace once cells are
+// interleaved); FP64 by cp.async too (variant 8): with the row chunk chosen per
+// launch it matches the TMA ring on periodic grids (4096^2: 5,986 against
+// 5,999; 2048^2: 5,527 against 5,523) and wins with edge code (2048^2
+// transmissive 5,186 against 5,120, with floors and a cylinder 4,734 against
+// 4,448).
 constexpr int kDefaultVariantF32 = 7;
 constexpr int kDefaultVariantF64 = 8;
 // FP32 grids with edge code (physical sides, cell types) run the same ring
