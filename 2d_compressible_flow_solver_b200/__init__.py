@@ -494,11 +494,15 @@ class Solver:
 
 class Batch:
     """Many independent grids advanced together (a ``cfs_batch``): one
-    persistent launch per stage for all cases, per-case CFL dt on the device."""
+    persistent launch per stage for all cases, per-case CFL dt on the device.
+    A case without ``rows`` takes the work-unit rows the autotuner measured
+    best for its size (``tuning.json`` ``batch_rows``; ``tuned_rows=False``:
+    the library default)."""
 
     def __init__(self, cases, *, precision: int = FP32_MIXED, rk: int = RK_SSP3, hll: int = HLL_DAVIS,
                  gamma: float = 1.4, weno_eps: float = 1e-2, device: int = 0, positivity: int = POSITIVITY_OFF,
-                 rounding: int = ROUND_STOCHASTIC_ALL):
+                 rounding: int = ROUND_STOCHASTIC_ALL, tuned_rows: bool = True):
+        from . import autotune as _autotune
         self._lib = load_library()
         cfg = CfsConfig()
         self._lib.cfs_config_default(ctypes.byref(cfg))
@@ -522,6 +526,8 @@ class Batch:
                 d.npoints = int(c.get("npoints", 400))
                 d.ib_mode = int(c.get("ib_mode", IB_BILINEAR_SLIP))
             d.rows = int(c.get("rows", 0))
+            if d.rows == 0 and tuned_rows:
+                d.rows = _autotune.batch_rows_for("f32" if precision == FP32_MIXED else "f64", d.nx, d.ny)
             d.edge_code = int(bool(c.get("edge_code", False)))
             self.shapes.append((d.nx, d.ny))
         self._b = ctypes.c_void_p()
