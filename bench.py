@@ -90,19 +90,52 @@ def hbm_peak():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples (every 200 ms) of the GPU's clocks and throttle reasons."""
+    """Samples of the GPU's SM clock and throttle reasons while the timed
+    region runs: read-only NVML queries every 2 ms from a thread (nvidia-smi
+    every 200 ms where NVML is missing).  open() and close() bracket the timed
+    region; stop() reports the samples taken inside it (all samples if none
+    fell inside, with "window": false)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event (throttle) reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.samples = []  # (time, sm MHz, max sm MHz, reason names)
         self.t = None
+        self.stop_flag = threading.Event()
+        self.window = [None, None]
+
+    def _handle(self, nv):
+        # the CUDA device's NVML handle, by UUID (CUDA and NVML may number devices differently)
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:  # noqa: BLE001
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._handle(nv)
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.nvml = (nv, h, smax, get_reasons)
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            return
+        except Exception:  # noqa: BLE001
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                                           "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
@@ -110,38 +143,59 @@ class ClockSampler:
         except OSError:
             self.proc = None
             return
-        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t = threading.Thread(target=self._read_smi, daemon=True)
         self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def open(self):
+        self.window[0] = time.perf_counter()
 
-    def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
+    def close(self):
+        self.window[1] = time.perf_counter()
+
+    def _poll_nvml(self):
+        nv, h, smax, get_reasons = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                bits = int(get_reasons(h))
+                names = [n for n, b in self.REASON_BITS.items() if bits & b]
+                self.samples.append((time.perf_counter(), sm, smax, names))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.002)
+
+    def _read_smi(self):
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.strip().split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                sm, smax = float(f[1]), float(f[2])
             except ValueError:
                 continue
-            for k, name in enumerate(names):
-                if f[5 + k].lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+            self.samples.append((time.perf_counter(), sm, smax, [n for k, n in enumerate(names)
+                                                                 if f[5 + k].lower() == "active"]))
+
+    def stop(self):
+        if self.nvml is None and self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.t.join(timeout=2)
+        t0, t1 = self.window
+        inside = [x for x in self.samples if t0 is not None and t1 is not None and t0 <= x[0] <= t1]
+        use = inside or self.samples
+        sm = [x[1] for x in use]
+        reasons = sorted({n for x in use for n in x[3]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(x[2] for x in use) if use else None,
+                "reasons": reasons, "samples": len(use), "window": bool(inside),
+                "source": "nvml (2 ms)" if self.nvml is not None else "nvidia-smi (200 ms)"}
 
 
 # -------------------------------------------------- CPU reference timing
@@ -209,7 +263,7 @@ def engine_arm(args):
     autotune = importlib.import_module(f"{PKG}.autotune")
     variants = {cfsb.FP32_MIXED: autotune.best_variant("f32", n * n), cfsb.FP64: autotune.best_variant("f64", n * n)}
 
-    def timed_advance_slab(prec, steps, warm):
+    def timed_advance_slab(prec, steps, warm, window=None):
         par = importlib.import_module(f"{PKG}.parallel")
         s = par.SlabSolver(n * world, n, float(world), 1.0, dist=dist, rank=rank, world=world, device=local,
                            bc=(cfsb.BC_PERIODIC,) * 4, precision=prec, variant=variants[prec], rk=cfsb.RK_SSP3,
@@ -225,19 +279,23 @@ def engine_arm(args):
         e1 = torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
+        if window:
+            window.open()
         e0.record(stream)
         t_sim = s.advance(steps, w.cfl)
         e1.record(stream)
         torch.cuda.synchronize()
+        if window:
+            window.close()
         barrier()
         ms = e0.elapsed_time(e1)
         totals = s.solver.totals()
         s.close()
         return ms, t_sim, None, totals
 
-    def timed_advance(prec, steps, warm, scheme=None):
+    def timed_advance(prec, steps, warm, scheme=None, window=None):
         if world > 1:
-            return timed_advance_slab(prec, steps, warm)
+            return timed_advance_slab(prec, steps, warm, window)
         skw, adv = dict(kw), dict(cfl=w.cfl)
         if scheme == "reference":
             skw.update(rk=cfsb.RK_TVD3_REFERENCE, hll=cfsb.HLL_REFERENCE, bc=(cfsb.BC_NEUMANN,) * 4)
@@ -252,10 +310,14 @@ def engine_arm(args):
         e1 = torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
+        if window:
+            window.open()
         e0.record(stream)
         t_sim, dt_last = s.advance(steps, **adv)
         e1.record(stream)
         torch.cuda.synchronize()
+        if window:
+            window.close()
         barrier()
         ms = e0.elapsed_time(e1)
         totals = s.totals()
@@ -264,7 +326,7 @@ def engine_arm(args):
 
     sampler = ClockSampler(local)
     sampler.start()
-    ms32, t32, dt32, _ = timed_advance(cfsb.FP32_MIXED, K, W)
+    ms32, t32, dt32, _ = timed_advance(cfsb.FP32_MIXED, K, W, window=sampler)
     clocks = sampler.stop()
     ms64, _, _, _ = timed_advance(cfsb.FP64, K, W)
     # the multi-GPU slab path at one rank (device-ordered stage launches through
