@@ -25,6 +25,28 @@ def test_cylinder_full_size_matches_reference_fixture(cfsb):
     assert np.allclose(np.hypot(normals[:, 0], normals[:, 1]), 1.0, rtol=1e-14)
 
 
+def test_cylinder_full_size_is_mirror_symmetric(cfsb):
+    """The Mach-3 cylinder grid (2048 x 1024 on [0,2]x[0,1], body centred on
+    y = 1/2): cell types are mirror images about that line exactly, every
+    immersed ghost's mirror is a ghost whose donors are the mirrored donors,
+    and the image points mirror to round-off (the polygon's vertices come from
+    sin and cos, so they mirror to about one ulp; a normal is the unit vector
+    from a ghost to its image point, whose length can be far below a cell, so
+    its mirror error is that ulp over the length).  The FP64 flow's own mirror
+    symmetry (tests/test_gpu_full_size.py) rests on this."""
+    nx, ny = 2048, 1024
+    types, cells, donors, images, normals = cfsb.circle_setup(nx, ny, 2.0, 1.0, 0.05, 0.4, 0.5, 400)
+    assert np.array_equal(types, types[:, ::-1])
+    i, j = cells // ny, cells % ny
+    pos = {int(c): k for k, c in enumerate(cells)}
+    mk = np.array([pos[int(c)] for c in i * ny + (ny - 1 - j)])
+    mirrored = (donors[mk] // ny) * ny + (ny - 1 - donors[mk] % ny)
+    assert np.array_equal(np.sort(donors, axis=1), np.sort(mirrored, axis=1))
+    assert np.abs(images[:, 0] - images[mk, 0]).max() <= 4e-15
+    assert np.abs(images[:, 1] - (1.0 - images[mk, 1])).max() <= 4e-15
+    assert np.abs(normals[:, 1] + normals[mk, 1]).max() <= 1e-10
+
+
 def test_small_circle_matches_reference_fixture(cfsb):
     g = dict(np.load(GOLD / "circle_64x64_lists.npz"))
     r, cx, cy = g["circle"]
