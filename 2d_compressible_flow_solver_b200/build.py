@@ -40,7 +40,7 @@ CU_UNITS = [
      [f"-DCFS_MARCH_POL={pol}", f"-DCFS_MARCH_FEAT={feat}", f"-DCFS_MARCH_FN=launch_march_{form}_{feat}"])
     for form, pol in (("f32", "PolF32"), ("f64", "PolF64")) for feat in range(8)
 ]
-CPP_SOURCES = ["cfs_api.cpp", "cfs_batch.cpp", "ib_setup.cpp", "tma_maps.cpp"]
+CPP_SOURCES = ["cfs_api.cpp", "cfs_batch.cpp", "ib_setup.cpp", "tma_maps.cpp", "host_stage.cpp"]
 
 
 def _headers() -> list[Path]:
@@ -77,14 +77,14 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
         src, obj = CSRC / name, OUT_DIR / (name + ".o")
         objs.append(obj)
         if force or _stale(src, obj, deps):
-            jobs.append(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra",
+            jobs.append(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-pthread", "-Wall", "-Wextra",
                          f"-I{CSRC}", f"-I{INCLUDE}", f"-I{CUDA_HOME / 'include'}", "-c", str(src), "-o", str(obj)])
     relink = force or not LIB.exists() or bool(jobs)
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         for f in [ex.submit(_run, cmd) for cmd in jobs]:
             f.result()
     if relink:
-        _run([NVCC, "-shared", *ARCH, "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(LIB)])
+        _run([NVCC, "-shared", *ARCH, "-Xcompiler", "-fPIC", *map(str, objs), "-lpthread", "-o", str(LIB)])
     return LIB
 
 

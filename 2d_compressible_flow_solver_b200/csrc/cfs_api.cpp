@@ -12,6 +12,7 @@
 
 #include "cfs_launch.h"
 #include "cfs_layout.h"
+#include "host_stage.h"
 #include "ib_setup.h"
 
 using cfs::kGhost;
@@ -32,6 +33,8 @@ struct cfs_ctx {
     double* rhs = nullptr;
     double* staging = nullptr;
     double* sums = nullptr;  // plane sums of an uploaded state (FP32 storage offsets)
+    void* host_stage = nullptr;   // pinned host buffer of the staged copies of large pageable arrays
+    size_t host_stage_bytes = 0;
     void* rv = nullptr;   // viscous RHS [3][nx][ny] (Navier-Stokes form only)
     uint8_t* types_d = nullptr;
     uint8_t* lowo_d = nullptr;  // [nx+1][ny+1] face flags of CFS_POSITIVITY_BODY
@@ -523,6 +526,7 @@ int cfs_destroy(cfs_ctx* c) {
     cudaFree(c->rhs);
     cudaFree(c->staging);
     cudaFree(c->sums);
+    if (c->host_stage) cudaFreeHost(c->host_stage);
     cudaFree(c->rv);
     cudaFree(c->types_d);
     cudaFree(c->lowo_d);
@@ -542,12 +546,45 @@ int cfs_destroy(cfs_ctx* c) {
     return CFS_OK;
 }
 
+// Copies of caller arrays: pinned arrays and small copies go straight to the
+// DMA engine; large pageable ones through the chunked pipeline of a pinned
+// staging buffer (allocated on first use; without it, the plain copy).
+static bool ensure_host_stage(cfs_ctx* c, size_t bytes) {
+    if (c->host_stage_bytes >= bytes) return true;
+    if (c->host_stage) cudaFreeHost(c->host_stage);
+    c->host_stage = nullptr;
+    c->host_stage_bytes = 0;
+    if (cudaHostAlloc(&c->host_stage, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        (void)cudaGetLastError();
+        c->host_stage = nullptr;
+        return false;
+    }
+    c->host_stage_bytes = bytes;
+    return true;
+}
+
+static bool staged(cfs_ctx* c, const void* host, size_t bytes) {
+    return bytes >= cfs::kStagedCopyMinBytes && !cfs::host_is_pinned(host) && ensure_host_stage(c, bytes);
+}
+
+static cudaError_t copy_in(cfs_ctx* c, void* dst, const void* src, size_t bytes) {
+    if (staged(c, src, bytes)) return cfs::upload_staged(dst, src, bytes, c->host_stage, c->stream, c->cfg.device);
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+}
+
+// (returns once dst holds the data)
+static cudaError_t copy_out(cfs_ctx* c, void* dst, const void* src, size_t bytes) {
+    if (staged(c, dst, bytes)) return cfs::download_staged(dst, src, bytes, c->host_stage, c->stream, c->cfg.device);
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(c->stream);
+}
+
 int cfs_set_state(cfs_ctx* c, const double* U) {
     if (!c || !U) return fail(c, CFS_ERR_INVALID, "null argument");
     c->wmax_carry = false;
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
-    CFS_CUDA(c, cudaMemcpyAsync(c->staging, U, hb, cudaMemcpyHostToDevice, c->stream));
+    CFS_CUDA(c, copy_in(c, c->staging, U, hb));
     if (c->L.elem_bytes == 4) {
         // FP32 storage offsets: the FP32-rounded mean of each variable, summed
         // on the device from the uploaded state (a fixed summation order)
@@ -613,8 +650,7 @@ int cfs_get_state(cfs_ctx* c, double* U) {
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
     CFS_CUDA(c, cfs::launch_unpack(c->L.elem_bytes, c->S[c->cur], c->staging, c->L, c->stream));
-    CFS_CUDA(c, cudaMemcpyAsync(U, c->staging, hb, cudaMemcpyDeviceToHost, c->stream));
-    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    CFS_CUDA(c, copy_out(c, U, c->staging, hb));
     return check_device_errors(c);
 }
 
@@ -623,8 +659,7 @@ int cfs_get_rhs(cfs_ctx* c, double* R) {
     if (!c->cfg.keep_rhs) return fail(c, CFS_ERR_STATE, "context created without keep_rhs");
     CFS_CUDA(c, cudaSetDevice(c->cfg.device));
     const size_t hb = sizeof(double) * kVars * static_cast<size_t>(c->cfg.nx) * c->cfg.ny;
-    CFS_CUDA(c, cudaMemcpyAsync(R, c->rhs, hb, cudaMemcpyDeviceToHost, c->stream));
-    CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    CFS_CUDA(c, copy_out(c, R, c->rhs, hb));
     return CFS_OK;
 }
 

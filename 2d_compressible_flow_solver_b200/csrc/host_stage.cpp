@@ -1,0 +1,138 @@
+// Chunked, threaded copies between pageable host arrays and device memory
+// through a pinned staging buffer (host_stage.h).
+#include "host_stage.h"
+
+#include <sched.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace cfs {
+
+namespace {
+
+constexpr int kChunks = 16;       // DMA chunks per copy
+constexpr int kMaxWorkers = 16;   // host copy threads (memory-bound past this)
+
+size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
+size_t round_up(size_t a, size_t b) { return ceil_div(a, b) * b; }
+
+int worker_count() {
+    cpu_set_t set;
+    int n = 1;
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) n = CPU_COUNT(&set);
+    return std::max(1, std::min(n, kMaxWorkers));
+}
+
+// Byte range [a0, a1) of worker t's stripe of chunk c.
+struct Plan {
+    size_t bytes, chunk;
+    int nch, workers;
+    Plan(size_t b, int w) : bytes(b), chunk(round_up(ceil_div(b, kChunks), 4096)), nch(0), workers(w) {
+        nch = static_cast<int>(ceil_div(bytes, chunk));
+    }
+    void chunk_range(int c, size_t& c0, size_t& c1) const {
+        c0 = static_cast<size_t>(c) * chunk;
+        c1 = std::min(bytes, c0 + chunk);
+    }
+    void stripe(int c, int t, size_t& a0, size_t& a1) const {
+        size_t c0, c1;
+        chunk_range(c, c0, c1);
+        const size_t per = round_up(ceil_div(c1 - c0, static_cast<size_t>(workers)), 64);
+        a0 = std::min(c1, c0 + static_cast<size_t>(t) * per);
+        a1 = std::min(c1, a0 + per);
+    }
+};
+
+}  // namespace
+
+bool host_is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();  // this query's own error only
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+cudaError_t upload_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t stream, int device) {
+    (void)device;
+    const Plan P(bytes, worker_count());
+    std::vector<std::atomic<int>> done(static_cast<size_t>(P.nch));
+    for (auto& d : done) d.store(0, std::memory_order_relaxed);
+    auto work = [&](int t) {
+        for (int c = 0; c < P.nch; ++c) {
+            size_t a0, a1;
+            P.stripe(c, t, a0, a1);
+            if (a1 > a0) std::memcpy(static_cast<char*>(stage) + a0, static_cast<const char*>(src) + a0, a1 - a0);
+            done[static_cast<size_t>(c)].fetch_add(1, std::memory_order_release);
+        }
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(static_cast<size_t>(P.workers));
+    for (int t = 0; t < P.workers; ++t) pool.emplace_back(work, t);
+    // this thread issues each chunk's copy once every worker has staged its
+    // stripe of it (the workers always finish: plain host copies)
+    cudaError_t err = cudaSuccess;
+    for (int c = 0; c < P.nch; ++c) {
+        while (done[static_cast<size_t>(c)].load(std::memory_order_acquire) < P.workers) std::this_thread::yield();
+        if (err != cudaSuccess) continue;
+        size_t c0, c1;
+        P.chunk_range(c, c0, c1);
+        err = cudaMemcpyAsync(static_cast<char*>(dst) + c0, static_cast<const char*>(stage) + c0, c1 - c0,
+                              cudaMemcpyHostToDevice, stream);
+    }
+    for (auto& th : pool) th.join();
+    return err;
+}
+
+cudaError_t download_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t stream, int device) {
+    const Plan P(bytes, worker_count());
+    std::vector<cudaEvent_t> ev(static_cast<size_t>(P.nch), nullptr);
+    cudaError_t err = cudaSuccess;
+    for (auto& e : ev)
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (int c = 0; c < P.nch && err == cudaSuccess; ++c) {
+        size_t c0, c1;
+        P.chunk_range(c, c0, c1);
+        err = cudaMemcpyAsync(static_cast<char*>(stage) + c0, static_cast<const char*>(src) + c0, c1 - c0,
+                              cudaMemcpyDeviceToHost, stream);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[static_cast<size_t>(c)], stream);
+    }
+    if (err == cudaSuccess) {
+        // each worker waits for a chunk's copy, then moves its stripe of it
+        std::atomic<int> werr{static_cast<int>(cudaSuccess)};
+        auto work = [&](int t) {
+            if (cudaSetDevice(device) != cudaSuccess) {
+                werr.store(static_cast<int>(cudaErrorInvalidDevice));
+                return;
+            }
+            for (int c = 0; c < P.nch; ++c) {
+                const cudaError_t e = cudaEventSynchronize(ev[static_cast<size_t>(c)]);
+                if (e != cudaSuccess) {
+                    werr.store(static_cast<int>(e));
+                    return;
+                }
+                size_t a0, a1;
+                P.stripe(c, t, a0, a1);
+                if (a1 > a0) std::memcpy(static_cast<char*>(dst) + a0, static_cast<const char*>(stage) + a0, a1 - a0);
+            }
+        };
+        std::vector<std::thread> pool;
+        pool.reserve(static_cast<size_t>(P.workers));
+        for (int t = 0; t < P.workers; ++t) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+        err = static_cast<cudaError_t>(werr.load());
+    } else {
+        (void)cudaStreamSynchronize(stream);  // the staging buffer is free again before an error returns
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    return err;
+}
+
+}  // namespace cfs

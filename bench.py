@@ -454,6 +454,20 @@ def engine_arm(args):
                 s.advance(1, cfl=w.cfl)
             s.get_state(out.numpy())
             wall = time.perf_counter() - t0
+            # the same with pageable host arrays, as a C++ caller's std::vector
+            # (the library stages large pageable copies through pinned memory)
+            # (warm: the staging buffer is pinned once per context, and the
+            # output array's pages are touched once)
+            host_out = np.empty((4, n, n))
+            s.set_state(w.U0)
+            s.get_state(host_out)
+            s.synchronize()
+            t0 = time.perf_counter()
+            s.set_state(w.U0)
+            for _ in range(K):
+                s.advance(1, cfl=w.cfl)
+            s.get_state(host_out)
+            wall_pageable = time.perf_counter() - t0
     else:
         par = importlib.import_module(f"{PKG}.parallel")
         s = par.SlabSolver(n * world, n, float(world), 1.0, dist=dist, rank=rank, world=world, device=local,
@@ -482,6 +496,12 @@ def engine_arm(args):
                                 "cfs_get_state to pinned host; host wall clock, max over ranks.  One FP64 state "
                                 "(537 MB) per GPU goes up and one comes down per run, so the rate depends on K "
                                 "(the steps field)"}
+        if world == 1:
+            result["e2e_pageable"] = {
+                "value": round(cells * K / wall_pageable / 1e6, 1), "unit": UNIT, "steps": K,
+                "how": "as e2e, with pageable host arrays (numpy) in place of pinned ones: cfs_set_state and "
+                       "cfs_get_state copy them in 16 chunks through a pinned staging buffer, host threads "
+                       "moving each chunk while the DMA engine moves the one before (after) it"}
     # the uneven 512-case batch (persistent batched engine), bounded: K steps
     # per form, device-timed with CUDA events on the batch's stream
     if rank == 0 and world == 1 and args.batch_cases > 0:

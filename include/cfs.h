@@ -162,7 +162,12 @@ int cfs_abi_version(void);
  * set: Initialcondition::fillIn (Initialcondition.h:11) over all cells, then
  *      the physical-boundary ghost fill (CartesianMesh::ApplyBoundaryCondition,
  *      CartesianMesh.cpp:280-305, called at Run.cpp:128).
- * get: the cell phases Output::WriteToHDF5 reads (Output.cpp:58-75). */
+ * get: the cell phases Output::WriteToHDF5 reads (Output.cpp:58-75).
+ * U may be pinned or pageable host memory.  A pageable array of 32 MB or more
+ * is copied in 16 chunks through a pinned staging buffer of the state's size,
+ * allocated by the first such call and kept until cfs_destroy, with host
+ * threads (up to 16) moving each chunk while the DMA engine moves the one
+ * before (after) it; the bytes are the same as a direct copy's. */
 int cfs_set_state(cfs_ctx* ctx, const double* U);
 int cfs_get_state(cfs_ctx* ctx, double* U);
 
