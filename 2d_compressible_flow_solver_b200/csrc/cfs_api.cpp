@@ -564,7 +564,7 @@ static bool ensure_host_stage(cfs_ctx* c, size_t bytes) {
 }
 
 static bool staged(cfs_ctx* c, const void* host, size_t bytes) {
-    return bytes >= cfs::kStagedCopyMinBytes && !cfs::host_is_pinned(host) && ensure_host_stage(c, bytes);
+    return bytes >= cfs::kStagedCopyMinBytes && cfs::host_is_pageable(host) && ensure_host_stage(c, bytes);
 }
 
 static cudaError_t copy_in(cfs_ctx* c, void* dst, const void* src, size_t bytes) {

@@ -84,14 +84,14 @@ void stream_copy(void* dst, const void* src, size_t n) {
 
 }  // namespace
 
-bool host_is_pinned(const void* p) {
+bool host_is_pageable(const void* p) {
     cudaPointerAttributes at{};
     const cudaError_t e = cudaPointerGetAttributes(&at, p);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();  // this query's own error only
         return false;
     }
-    return at.type == cudaMemoryTypeHost;
+    return at.type == cudaMemoryTypeUnregistered;
 }
 
 cudaError_t upload_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t stream, int device) {

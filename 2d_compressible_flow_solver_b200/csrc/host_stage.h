@@ -13,9 +13,9 @@
 
 namespace cfs {
 
-// Whether `p` is page-locked host memory the DMA engine reads directly
-// (cudaHostAlloc / cudaHostRegister); false for ordinary pageable memory.
-bool host_is_pinned(const void* p);
+// Whether `p` is ordinary pageable host memory (not page-locked, not device
+// or managed memory): only such arrays take the staged copies.
+bool host_is_pageable(const void* p);
 
 // Smallest copy worth the pipeline (smaller ones go through cudaMemcpyAsync).
 constexpr size_t kStagedCopyMinBytes = size_t(32) << 20;
