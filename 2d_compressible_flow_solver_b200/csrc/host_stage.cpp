@@ -8,6 +8,7 @@
 #endif
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -82,6 +83,20 @@ void stream_copy(void* dst, const void* src, size_t n) {
 #endif
 }
 
+// Starts work(t) on a thread for t = 0..n-1 and returns how many started; a
+// thread the system refuses has its share run by the caller (nothing here
+// throws past the C ABI).
+template <class F>
+int spawn(std::vector<std::thread>& pool, int n, F& work) {
+    int made = 0;
+    try {
+        pool.reserve(static_cast<size_t>(n));
+        for (; made < n; ++made) pool.emplace_back(work, made);
+    } catch (...) {
+    }
+    return made;
+}
+
 }  // namespace
 
 bool host_is_pageable(const void* p) {
@@ -97,7 +112,7 @@ bool host_is_pageable(const void* p) {
 cudaError_t upload_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t stream, int device) {
     (void)device;
     const Plan P(bytes, worker_count());
-    std::vector<std::atomic<int>> done(static_cast<size_t>(P.nch));
+    std::array<std::atomic<int>, kChunks> done;
     for (auto& d : done) d.store(0, std::memory_order_relaxed);
     auto work = [&](int t) {
         for (int c = 0; c < P.nch; ++c) {
@@ -108,8 +123,7 @@ cudaError_t upload_staged(void* dst, const void* src, size_t bytes, void* stage,
         }
     };
     std::vector<std::thread> pool;
-    pool.reserve(static_cast<size_t>(P.workers));
-    for (int t = 0; t < P.workers; ++t) pool.emplace_back(work, t);
+    for (int t = spawn(pool, P.workers, work); t < P.workers; ++t) work(t);
     // this thread issues each chunk's copy once every worker has staged its
     // stripe of it (the workers always finish: plain host copies)
     cudaError_t err = cudaSuccess;
@@ -127,10 +141,10 @@ cudaError_t upload_staged(void* dst, const void* src, size_t bytes, void* stage,
 
 cudaError_t download_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t stream, int device) {
     const Plan P(bytes, worker_count());
-    std::vector<cudaEvent_t> ev(static_cast<size_t>(P.nch), nullptr);
+    std::array<cudaEvent_t, kChunks> ev{};
     cudaError_t err = cudaSuccess;
-    for (auto& e : ev)
-        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (int c = 0; c < P.nch && err == cudaSuccess; ++c)
+        err = cudaEventCreateWithFlags(&ev[static_cast<size_t>(c)], cudaEventDisableTiming);
     for (int c = 0; c < P.nch && err == cudaSuccess; ++c) {
         size_t c0, c1;
         P.chunk_range(c, c0, c1);
@@ -158,8 +172,7 @@ cudaError_t download_staged(void* dst, const void* src, size_t bytes, void* stag
             }
         };
         std::vector<std::thread> pool;
-        pool.reserve(static_cast<size_t>(P.workers));
-        for (int t = 0; t < P.workers; ++t) pool.emplace_back(work, t);
+        for (int t = spawn(pool, P.workers, work); t < P.workers; ++t) work(t);
         for (auto& th : pool) th.join();
         err = static_cast<cudaError_t>(werr.load());
     } else {
