@@ -112,7 +112,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_slab_exchange_matches_single_domain(workloads, world):
     import oracle_bind as ob
 
