@@ -66,6 +66,8 @@ struct cfs_ctx {
     unsigned long long* wmax = nullptr;
     double* totals = nullptr;
     cudaGraphExec_t graph2 = nullptr;  // two full steps (parity 0 then 1)
+    cudaGraphExec_t graph1 = nullptr;  // one full step (parity 0): an odd step count's last step
+    cfs::DevParams* hp_pin = nullptr;  // pinned host copies of cfs_advance's parameters in [0] and results in [1]
     // device-ordered stepping (cfs_steps_*): between begin and end
     bool in_steps = false;
     bool steps_cfl = false;
@@ -122,6 +124,10 @@ void release_graph(cfs_ctx* c) {
     if (c->graph2) {
         cudaGraphExecDestroy(c->graph2);
         c->graph2 = nullptr;
+    }
+    if (c->graph1) {
+        cudaGraphExecDestroy(c->graph1);
+        c->graph1 = nullptr;
     }
 }
 
@@ -496,6 +502,11 @@ int cfs_create(const cfs_config* cfg, cfs_ctx** out) {
     }
     cudaMemsetAsync(c->P, 0, sizeof(cfs::DevParams), c->stream);
     cudaMemsetAsync(c->err_d, 0, sizeof(unsigned int), c->stream);
+    // (without it, cfs_advance copies its parameters through pageable memory)
+    if (cudaHostAlloc(&c->hp_pin, 2 * sizeof(cfs::DevParams), cudaHostAllocDefault) != cudaSuccess) {
+        (void)cudaGetLastError();
+        c->hp_pin = nullptr;
+    }
     if (c->prec != cfs::kF64Exact) {
         // tensor maps of the three state buffers (TMA load schedule), encoded
         // on the host once (the buffers never move) and passed in each
@@ -538,6 +549,7 @@ int cfs_destroy(cfs_ctx* c) {
     cudaFree(c->ib_img);
     cudaFree(c->ib_fac);
     cudaFree(c->P);
+    if (c->hp_pin) cudaFreeHost(c->hp_pin);
     cudaFree(c->wmax);
     cudaFree(c->totals);
     cudaFree(c->err_d);
@@ -886,7 +898,14 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
     // one call of K steps takes), else reduced now
     const bool carry = hp.use_cfl && c->wmax_carry;
     if (carry) hp.wmax[0] = c->wmax_bits;
-    CFS_CUDA(c, cudaMemcpyAsync(c->P, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+    // (the previous advance ended with a stream synchronisation, so the pinned
+    // slot is free)
+    const cfs::DevParams* hp_src = &hp;
+    if (c->hp_pin) {
+        c->hp_pin[0] = hp;
+        hp_src = c->hp_pin;
+    }
+    CFS_CUDA(c, cudaMemcpyAsync(c->P, hp_src, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
     if (hp.use_cfl && !carry) {
         if (c->ib_n > 0) CFS_CUDA(c, cfs::launch_ib_fill(c->L.elem_bytes, ib_args(c, c->S[0]), c->stream));
         CFS_CUDA(c, cfs::launch_wmax(c->L.elem_bytes, c->S[0], c->L, c->has_types ? c->types_d : nullptr, c->cfg.gamma,
@@ -905,32 +924,37 @@ int cfs_advance(cfs_ctx* c, int nsteps, double cfl, double dt, double* t_elapsed
         }
         return CFS_OK;
     };
-    if (nsteps >= 2 && !c->graph2) {
+    // CUDA graphs of two steps (parities 0, 1) and of one step (parity 0),
+    // captured at first use; every launch reads dt and the CFL slots from P
+    auto capture = [&](int steps, cudaGraphExec_t* exec) -> int {
         cudaGraph_t g = nullptr;
         CFS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(0);
-        if (rc == CFS_OK) rc = enqueue_step(1);
+        int rc = CFS_OK;
+        for (int k = 0; k < steps && rc == CFS_OK; ++k) rc = enqueue_step(k);
         const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
         if (rc != CFS_OK) {
             if (g) cudaGraphDestroy(g);
             return rc;
         }
         if (ec != cudaSuccess) return fail(c, CFS_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(ec));
-        const cudaError_t ei = cudaGraphInstantiate(&c->graph2, g, 0);
+        const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
         cudaGraphDestroy(g);
         if (ei != cudaSuccess) {
-            c->graph2 = nullptr;
+            *exec = nullptr;
             return fail(c, CFS_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(ei));
         }
-    }
+        return CFS_OK;
+    };
+    if (nsteps >= 2 && !c->graph2)
+        if (const int rc = capture(2, &c->graph2); rc != CFS_OK) return rc;
+    if (nsteps % 2 == 1 && !c->graph1)
+        if (const int rc = capture(1, &c->graph1); rc != CFS_OK) return rc;
     for (int k = 0; k + 1 < nsteps; k += 2) CFS_CUDA(c, cudaGraphLaunch(c->graph2, c->stream));
-    if (nsteps % 2 == 1) {
-        const int rc = enqueue_step(0);
-        if (rc != CFS_OK) return rc;
-    }
+    if (nsteps % 2 == 1) CFS_CUDA(c, cudaGraphLaunch(c->graph1, c->stream));
     cfs::DevParams out{};
-    CFS_CUDA(c, cudaMemcpyAsync(&out, c->P, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CFS_CUDA(c, cudaMemcpyAsync(c->hp_pin ? c->hp_pin + 1 : &out, c->P, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
     CFS_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->hp_pin) out = c->hp_pin[1];
     if (t_elapsed) *t_elapsed = out.t;
     if (dt_last) *dt_last = out.dt_last;
     c->steps_done += static_cast<unsigned int>(nsteps);
